@@ -1,0 +1,112 @@
+"""Regenerate the golden fixtures of this directory from the eT source tree.
+
+Run in a container that has the eT sources mounted (read-only is fine):
+
+    python tests/golden/make_fixtures.py /path/to/eT
+
+It writes
+
+* ``basis_cc-pvdz.json`` - the cc-pVDZ shells of H, He and O, taken from
+  ``ao_basis/cc-pvdz.g94`` (published Dunning basis data), so the oracle's
+  integral front end can rebuild eT's test molecules without the eT tree;
+* ``et_reference_values.json`` - numbers parsed from eT's committed
+  regression outputs (``tests/*/result/*.out``): geometries, HF energies,
+  the (E, |Omega|) history of the DIIS ground-state solver, final CCSD
+  energies, the number of Cholesky vectors and EOM-CCSD excitation energies.
+
+Nothing here is executed by the tests; they only read the two JSON files.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _geometry(inp: str):
+    m = re.search(r"geometry\s*\n\s*basis:\s*(\S+)\s*\n(.*?)end geometry", inp, re.S | re.I)
+    atoms = []
+    for line in m.group(2).strip().splitlines():
+        tok = line.split()
+        atoms.append([tok[0], float(tok[1]), float(tok[2]), float(tok[3])])
+    return m.group(1).lower(), atoms
+
+
+def _gs_history(out: str):
+    block = out.split("Iteration    Energy (a.u.)        |omega|")[1].split("Convergence criterion")[0]
+    hist = []
+    for line in block.splitlines():
+        tok = line.split()
+        if len(tok) == 4 and tok[0].isdigit():
+            hist.append([float(tok[1]), float(tok[2])])
+    return hist
+
+
+def _scf_energy(out: str):
+    return float(re.search(r"Total energy:\s+(-?\d+\.\d+)", out).group(1))
+
+
+def _final_cc(out: str):
+    return float(re.search(r"Final ground state energy \(a\.u\.\):\s+(-?\d+\.\d+)", out).group(1))
+
+
+def _n_cholesky(out: str):
+    return int(re.search(r"Final number of Cholesky vectors:\s+(\d+)", out).group(1))
+
+
+def _cd_threshold(inp: str):
+    m = re.search(r"solver cholesky\s*\n\s*threshold:\s*(\S+)", inp, re.I)
+    return float(m.group(1).replace("d", "e").replace("D", "e"))
+
+
+def _excitations(out: str):
+    block = out.split("CCSD excitation energies:")[1].split("eV/Hartree")[0]
+    vals = []
+    for line in block.splitlines():
+        tok = line.split()
+        if len(tok) == 3 and tok[0].isdigit():
+            vals.append(float(tok[1]))
+    return vals
+
+
+def _test(root, name):
+    d = os.path.join(root, "tests", name)
+    inp = open(os.path.join(d, name + ".inp")).read()
+    out = open(os.path.join(d, "result", name + ".out")).read()
+    return inp, out
+
+
+def main(root: str) -> None:
+    values = {}
+    for name in ("ccsd_gs_energy", "ccsd_lr_polarizability"):
+        inp, out = _test(root, name)
+        basis, atoms = _geometry(inp)
+        values[name] = dict(
+            source=f"tests/{name}/result/{name}.out",
+            basis=basis, atoms=atoms, cd_threshold=_cd_threshold(inp),
+            e_hf=_scf_energy(out), e_ccsd=_final_cc(out), n_cholesky=_n_cholesky(out),
+            gs_history=_gs_history(out),
+        )
+    for name in ("ccsd_right_es_energies", "ccsd_left_es_energies"):
+        inp, out = _test(root, name)
+        basis, atoms = _geometry(inp)
+        values[name] = dict(source=f"tests/{name}/result/{name}.out", basis=basis, atoms=atoms,
+                            cd_threshold=_cd_threshold(inp), e_ccsd=_final_cc(out),
+                            excitation_energies=_excitations(out))
+    with open(os.path.join(HERE, "et_reference_values.json"), "w") as f:
+        json.dump(values, f, indent=1)
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.frontend import parse_g94
+    text = open(os.path.join(root, "ao_basis", "cc-pvdz.g94")).read()
+    basis = parse_g94(text, {"H", "He", "O"})
+    with open(os.path.join(HERE, "basis_cc-pvdz.json"), "w") as f:
+        json.dump({"source": "ao_basis/cc-pvdz.g94", "shells": basis}, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
