@@ -1,0 +1,279 @@
+"""Benchmark of the CCSD ground-state iteration on B200 (one JSON line on rank 0).
+
+Workload: the synthetic Cholesky-factored CCSD system o=32, v=320, N_J=1200
+(seeded generator in et_b200/synthetic.py), MP2 start, quasi-Newton + DIIS(8).
+A step is one ground-state iteration: T1-transformed Cholesky vectors, T1 Fock
+matrix, energy, Omega, quasi-Newton update and DIIS extrapolation.
+
+value = algorithmic TFLOP/s of the step (eT's own BLAS call-site flop count of
+one iteration divided by its device time), summed over ranks; ms_per_step is
+the per-iteration time.  Multi-GPU runs are independent replicas (one system
+per rank, no collective on the data path) timed as the max over ranks.
+
+--impl reference times the CPU restatement of eT's algorithm (oracle/ccsd.py,
+numpy + threaded BLAS) on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CCSD Omega+Jacobian s/iter & TFLOP/s, mixed vs FP64 on 1 B200 at |dE|<=1e-8 Eh"
+
+
+def iteration_flops(n_o, n_v, n_J):
+    """Algorithmic flops of one ground-state iteration: Omega (eT call sites) + energy + T1 + Fock."""
+    o, v, J = float(n_o), float(n_v), float(n_J)
+    ov = o * v
+    nop, nom, nvp, nvm = o * (o + 1) / 2, o * (o - 1) / 2, v * (v + 1) / 2, v * (v - 1) / 2
+    f = 0.0
+    f += 2 * J * ov * ov + 2 * v * o * J * v
+    f += 2 * ov * o * o * J + 2 * v * o * o * o * v
+    f += 2 * ov * ov
+    f += 2 * ov * ov * J + 2 * v * v * v * o * o * 2 + 2 * o * o * o * v * v * 2
+    f += 2 * ov * ov * J * 2 + 2 * o ** 4 * J + 2 * o ** 4 * v * v * 2
+    f += 2 * v * v * o * o * J + 2 * ov * ov * J * 2 + 8 * ov ** 3
+    f += v * v * (v * v + 1) * J + 2 * nop * nvp * nvp + 2 * nom * nvm * nvm
+    omega = f
+    energy = 2 * ov * ov * J                                     # g_ovov for calculate_energy
+    t1 = 2 * J * o * o * v * 2 + 2 * J * v * v * o * 2 + 2 * J * o * v * o   # construct_t1_cholesky
+    nmo = o + v
+    fock = 2 * J * nmo * nmo + 2 * J * o * nmo * nmo + 4 * nmo * nmo * o   # Coulomb, exchange, h~
+    return omega + energy + t1 + fock, omega
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        if not getattr(self, "lines", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            tok = [x.strip() for x in ln.split(",")]
+            try:
+                sm.append(float(tok[1]))
+                mx = float(tok[2])
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, tok[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, local, world
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_gpu(args):
+    import torch
+    from et_b200 import CCSD, FP64, MIXED
+    from et_b200.synthetic import make_system
+
+    rank, local, world = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    n_o, n_v, n_J = args.n_o, args.n_v, args.n_J
+    sysd = make_system(n_o, n_v, n_J, seed=2026 + rank)
+    prec = MIXED if args.precision == "mixed" else FP64
+    gpu = CCSD(n_o, n_v, n_J, precision=prec, device=local)
+    stream = torch.cuda.current_stream()
+    gpu.set_stream(stream.cuda_stream)
+    gpu.set_system(sysd.L_mo, sysd.h_mo, sysd.eps, sysd.e_hf)
+    flops_iter, flops_omega = iteration_flops(n_o, n_v, n_J)
+
+    # warm-up: W iterations from the MP2 start
+    gpu.set_initial_amplitudes_guess()
+    gpu.solve_ground_state(max_iterations=args.warmup, omega_threshold=1e-30, energy_threshold=-1.0,
+                           refine_threshold=args.refine, raise_on_failure=False)
+    # timed: K iterations from the MP2 start (inputs are > L2: t 419 MB, L 1.19 GB)
+    gpu.set_initial_amplitudes_guess()
+    launches0, _ = gpu.stats()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        e, it, hist, rc = gpu.solve_ground_state(max_iterations=args.steps, omega_threshold=1e-30,
+                                                 energy_threshold=-1.0, refine_threshold=args.refine,
+                                                 raise_on_failure=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, world)
+    launches1, _ = gpu.stats()
+    ms_step = ms / max(it, 1)
+    value = world * flops_iter * it / (ms * 1e-3) / 1e12
+
+    # end to end through the public API with host buffers (eT's per-iteration calls):
+    # set_amplitudes(host t) -> calculate_energy -> construct_omega(host Omega)
+    t_host = gpu.get_amplitudes()
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        gpu.set_amplitudes(t_host)
+        gpu.calculate_energy()
+        om = gpu.construct_omega()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_s = max_over_ranks(e2e_s, world)
+    e2e_value = world * (flops_omega + iteration_flops(n_o, n_v, n_J)[0] - flops_omega) / e2e_s / 1e12
+
+    result = {
+        "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": it,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "s_per_iter": round(ms_step / 1e3, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16x3+f64" if prec == MIXED else "f64", "data": "synthetic",
+        "config": {"workload": f"CCSD ground-state iteration, synthetic Cholesky system o={n_o} v={n_v} N_J={n_J}",
+                   "n_o": n_o, "n_v": n_v, "n_J": n_J, "precision": args.precision,
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (t2 419 MB, L 1.19 GB at full size)",
+                   "flops_per_iter": flops_iter},
+        "clocks": clk.summary(),
+        "e2e": {"value": round(e2e_value, 3), "unit": "TFLOP/s", "s_per_iter": round(e2e_s, 5),
+                "h2d_bytes_per_step": int(8 * gpu.n_amp), "d2h_bytes_per_step": int(8 * gpu.n_amp + 8)},
+        "gpu_launches": int(launches1 - launches0),
+        "energy_after_steps": e, "omega_norm_after_steps": float(hist[-1, 1]) if len(hist) else None,
+    }
+    gpu.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        if args.cpu_baseline and world == 1:
+            result["cpu_baseline"] = cpu_sample(args)
+        print(json.dumps(result), flush=True)
+
+
+def cpu_sample(args):
+    """The CPU oracle (numpy + threaded BLAS) on a bounded sample: GS iterations at a reduced size."""
+    from oracle import ccsd as oc
+    from et_b200.synthetic import make_system
+    n_o, n_v, n_J = args.cpu_o, args.cpu_v, args.cpu_J
+    s = make_system(n_o, n_v, n_J, seed=2026)
+    sy = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o, s.e_hf)
+    sy.mp2_start()
+    t0 = time.perf_counter()
+    n_it = 0
+    while time.perf_counter() - t0 < args.cpu_seconds or n_it == 0:
+        oc.solve_gs(sy, max_iterations=1, omega_threshold=0.0, energy_threshold=-1.0)
+        n_it += 1
+    dt = (time.perf_counter() - t0) / n_it
+    fl, _ = iteration_flops(n_o, n_v, n_J)
+    return {"value": round(fl / dt / 1e12, 5), "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "port",
+            "s_per_iter": round(dt, 4),
+            "sample": f"{n_it} ground-state iterations of the numpy oracle at o={n_o} v={n_v} N_J={n_J}"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_sample(args)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "TFLOP/s", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(cb["s_per_iter"] * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"CCSD ground-state iteration, synthetic Cholesky system "
+                                   f"o={args.n_o} v={args.n_v} N_J={args.n_J} (CPU sample at "
+                                   f"o={args.cpu_o} v={args.cpu_v} N_J={args.cpu_J})"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--refine", type=float, default=1e-5)
+    p.add_argument("--n-o", dest="n_o", type=int, default=32)
+    p.add_argument("--n-v", dest="n_v", type=int, default=320)
+    p.add_argument("--n-J", dest="n_J", type=int, default=1200)
+    p.add_argument("--cpu-o", dest="cpu_o", type=int, default=10)
+    p.add_argument("--cpu-v", dest="cpu_v", type=int, default=100)
+    p.add_argument("--cpu-J", dest="cpu_J", type=int, default=375)
+    p.add_argument("--cpu-seconds", dest="cpu_seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = p.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

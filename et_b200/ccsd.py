@@ -1,0 +1,247 @@
+"""Host-side mirror of eT's CCSD wavefunction entry points over the C ABI (include/ccsd_gpu.h).
+
+``CCSD`` exposes the type-bound procedures of eT's ``class(ccsd)`` that the
+ground-state DIIS solver and the Davidson excited-state solver call
+(src/wavefunctions/ccsd/ccsd_class.F90:99-253): ``construct_omega``,
+``jacobian_transformation``, ``jacobian_transpose_transformation``,
+``calculate_energy``, ``construct_fock``/``construct_t1_cholesky`` (run by
+``set_amplitudes``), plus the device-resident ground-state solver.
+
+The compute runs in ``libccsd_gpu.so`` (sm_100a); there is no CPU fallback: if
+the library cannot be loaded, or no sm_100 device is present, every call
+raises ``CCSDGPUError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libccsd_gpu.so")
+
+FP64 = 0
+MIXED = 1
+
+STATUS = {
+    0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
+    -4: "missing input", -5: "not converged", -6: "non-finite value", -7: "singular system",
+    -8: "no sm_100 device",
+}
+
+
+class CCSDGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("ladder_batch", ctypes.c_int64),
+                ("mixed_min_flops", ctypes.c_int64), ("reserved", ctypes.c_int64 * 5)]
+
+
+class SolverOptions(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_int32), ("diis_dimension", ctypes.c_int32),
+                ("omega_threshold", ctypes.c_double), ("energy_threshold", ctypes.c_double),
+                ("refine_threshold", ctypes.c_double), ("reserved", ctypes.c_int32 * 8)]
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_VP = ctypes.c_void_p
+_DP = ctypes.POINTER(ctypes.c_double)
+_I64 = ctypes.c_int64
+SIGNATURES = {
+    "ccsd_gpu_create": (ctypes.c_int, [_I64, _I64, _I64, ctypes.POINTER(Options), ctypes.POINTER(_VP)]),
+    "ccsd_gpu_destroy": (None, [_VP]),
+    "ccsd_gpu_last_error": (ctypes.c_char_p, [_VP]),
+    "ccsd_gpu_set_precision": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "ccsd_gpu_set_stream": (ctypes.c_int, [_VP, _VP]),
+    "ccsd_gpu_synchronize": (ctypes.c_int, [_VP]),
+    "ccsd_gpu_set_cholesky_mo": (ctypes.c_int, [_VP, _DP]),
+    "ccsd_gpu_set_cholesky_mo_blocks": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
+    "ccsd_gpu_set_h_mo": (ctypes.c_int, [_VP, _DP, _DP, ctypes.c_double]),
+    "ccsd_gpu_set_amplitudes": (ctypes.c_int, [_VP, _DP]),
+    "ccsd_gpu_get_amplitudes": (ctypes.c_int, [_VP, _DP]),
+    "ccsd_gpu_mp2_guess": (ctypes.c_int, [_VP]),
+    "ccsd_gpu_get_fock": (ctypes.c_int, [_VP, _DP]),
+    "ccsd_gpu_energy": (ctypes.c_int, [_VP, _DP]),
+    "ccsd_gpu_omega": (ctypes.c_int, [_VP, _DP]),
+    "ccsd_gpu_omega_device": (ctypes.c_int, [_VP, _VP]),
+    "ccsd_gpu_jacobian": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
+    "ccsd_gpu_jacobian_transpose": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
+    "ccsd_gpu_solve_gs": (ctypes.c_int, [_VP, ctypes.POINTER(SolverOptions), _DP,
+                                         ctypes.POINTER(ctypes.c_int32), _DP]),
+    "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
+    "ccsd_gpu_omega_flops": (ctypes.c_double, [_VP]),
+}
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libccsd_gpu.so (built by et_b200/build.py); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise CCSDGPUError(-8, f"{path} not built; run `python et_b200/build.py`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, order="F") if np.ndim(a) > 1 else a,
+                             dtype=np.float64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+class CCSD:
+    """One Cholesky-factored closed-shell CCSD system resident on one GPU."""
+
+    def __init__(self, n_o, n_v, n_J, *, precision=FP64, device=0, ladder_batch=0, mixed_min_flops=0):
+        self.lib = load_library()
+        self.n_o, self.n_v, self.n_J = int(n_o), int(n_v), int(n_J)
+        self.n_mo = self.n_o + self.n_v
+        self.n_t1 = self.n_o * self.n_v
+        self.n_t2 = self.n_t1 * (self.n_t1 + 1) // 2
+        self.n_amp = self.n_t1 + self.n_t2
+        opt = Options(device=device, precision=precision, ladder_batch=ladder_batch,
+                      mixed_min_flops=mixed_min_flops)
+        ctx = _VP()
+        rc = self.lib.ccsd_gpu_create(self.n_o, self.n_v, self.n_J, ctypes.byref(opt), ctypes.byref(ctx))
+        if rc != 0:
+            raise CCSDGPUError(rc, self.lib.ccsd_gpu_last_error(None).decode())
+        self.ctx = ctx
+
+    # -- plumbing --
+    def _check(self, rc):
+        if rc != 0:
+            raise CCSDGPUError(rc, self.lib.ccsd_gpu_last_error(self.ctx).decode())
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.ccsd_gpu_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_precision(self, precision):
+        self._check(self.lib.ccsd_gpu_set_precision(self.ctx, precision))
+
+    def set_stream(self, stream_handle: int):
+        self._check(self.lib.ccsd_gpu_set_stream(self.ctx, _VP(stream_handle)))
+
+    def synchronize(self):
+        self._check(self.lib.ccsd_gpu_synchronize(self.ctx))
+
+    # -- inputs --
+    def set_cholesky_mo(self, L):
+        """L[J, p, q] (numpy, any memory order) over the full MO range."""
+        L = np.asarray(L, dtype=np.float64)
+        assert L.shape == (self.n_J, self.n_mo, self.n_mo)
+        flat = np.ascontiguousarray(L.reshape(-1, order="F") if not L.flags.f_contiguous else L.ravel(order="K"))
+        self._check(self.lib.ccsd_gpu_set_cholesky_mo(self.ctx, _dp(flat)))
+
+    def set_h_mo(self, h, eps, e_hf=0.0):
+        h = _f64(np.asarray(h, dtype=np.float64).reshape(-1, order="F"), self.n_mo * self.n_mo)
+        eps = _f64(eps, self.n_mo)
+        self._check(self.lib.ccsd_gpu_set_h_mo(self.ctx, _dp(h), _dp(eps), float(e_hf)))
+
+    def set_system(self, L, h, eps, e_hf=0.0):
+        self.set_cholesky_mo(L)
+        self.set_h_mo(h, eps, e_hf)
+
+    # -- eT wavefunction entry points --
+    def set_amplitudes(self, t):
+        t = _f64(t, self.n_amp)
+        self._check(self.lib.ccsd_gpu_set_amplitudes(self.ctx, _dp(t)))
+
+    def get_amplitudes(self):
+        out = np.empty(self.n_amp)
+        self._check(self.lib.ccsd_gpu_get_amplitudes(self.ctx, _dp(out)))
+        return out
+
+    def set_initial_amplitudes_guess(self):
+        self._check(self.lib.ccsd_gpu_mp2_guess(self.ctx))
+
+    def get_fock(self):
+        out = np.empty(self.n_mo * self.n_mo)
+        self._check(self.lib.ccsd_gpu_get_fock(self.ctx, _dp(out)))
+        return out.reshape(self.n_mo, self.n_mo, order="F")
+
+    def calculate_energy(self) -> float:
+        e = ctypes.c_double()
+        self._check(self.lib.ccsd_gpu_energy(self.ctx, ctypes.byref(e)))
+        return e.value
+
+    def construct_omega(self):
+        out = np.empty(self.n_amp)
+        self._check(self.lib.ccsd_gpu_omega(self.ctx, _dp(out)))
+        return out
+
+    def construct_omega_device(self, d_ptr: int):
+        self._check(self.lib.ccsd_gpu_omega_device(self.ctx, _VP(d_ptr)))
+
+    def jacobian_transformation(self, c):
+        c = np.asarray(c, dtype=np.float64)
+        n_vec = 1 if c.ndim == 1 else c.shape[1]
+        flat = np.ascontiguousarray(c.reshape(-1, order="F"))
+        out = np.empty(self.n_amp * n_vec)
+        self._check(self.lib.ccsd_gpu_jacobian(self.ctx, n_vec, _dp(flat), _dp(out)))
+        return out if c.ndim == 1 else out.reshape(self.n_amp, n_vec, order="F")
+
+    def jacobian_transpose_transformation(self, b):
+        b = np.asarray(b, dtype=np.float64)
+        n_vec = 1 if b.ndim == 1 else b.shape[1]
+        flat = np.ascontiguousarray(b.reshape(-1, order="F"))
+        out = np.empty(self.n_amp * n_vec)
+        self._check(self.lib.ccsd_gpu_jacobian_transpose(self.ctx, n_vec, _dp(flat), _dp(out)))
+        return out if b.ndim == 1 else out.reshape(self.n_amp, n_vec, order="F")
+
+    def solve_ground_state(self, *, max_iterations=100, diis_dimension=8, omega_threshold=1e-5,
+                           energy_threshold=1e-5, refine_threshold=1e-4, raise_on_failure=True):
+        """run_diis_cc_gs on the device; returns (energy, iterations, history[(E, |Omega|)], status)."""
+        opt = SolverOptions(max_iterations=max_iterations, diis_dimension=diis_dimension,
+                            omega_threshold=omega_threshold, energy_threshold=energy_threshold,
+                            refine_threshold=refine_threshold)
+        e = ctypes.c_double()
+        it = ctypes.c_int32()
+        hist = np.zeros(2 * max_iterations)
+        rc = self.lib.ccsd_gpu_solve_gs(self.ctx, ctypes.byref(opt), ctypes.byref(e), ctypes.byref(it), _dp(hist))
+        if rc != 0 and (raise_on_failure or rc != -5):
+            self._check(rc)
+        return e.value, it.value, hist[: 2 * it.value].reshape(-1, 2), rc
+
+    def stats(self):
+        """(kernel launches of this library, GEMM flops issued) since creation."""
+        n = ctypes.c_int64()
+        f = ctypes.c_double()
+        self._check(self.lib.ccsd_gpu_stats(self.ctx, ctypes.byref(n), ctypes.byref(f)))
+        return n.value, f.value
+
+    def omega_flops(self) -> float:
+        return float(self.lib.ccsd_gpu_omega_flops(self.ctx))

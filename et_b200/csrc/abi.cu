@@ -1,0 +1,228 @@
+// extern "C" entry points (include/ccsd_gpu.h): argument checks, host<->device staging,
+// and conversion of exceptions into status codes.
+#include <cstring>
+#include <new>
+
+#include "ccsd.cuh"
+#include "ccsd_kernels.cuh"
+#include "tensor_ops.cuh"
+
+using ccsd::Context;
+using ccsd::Error;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(void *ctx, F &&f) {
+    if (!ctx) return CCSD_GPU_EINVAL;
+    Context *c = static_cast<Context *>(ctx);
+    try {
+        CU_CHECK(cudaSetDevice(c->device));
+        f(*c);
+        c->err.clear();
+        return CCSD_GPU_OK;
+    } catch (const Error &e) {
+        c->err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        c->err = "host allocation failed";
+        return CCSD_GPU_ENOMEM;
+    } catch (const std::exception &e) {
+        c->err = e.what();
+        return CCSD_GPU_ECUDA;
+    }
+}
+
+void h2d(Context &c, double *dst, const double *src, int64_t n) {
+    REQUIRE(src != nullptr, CCSD_GPU_EINVAL, "null input pointer");
+    CU_CHECK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, c.ex.stream));
+}
+
+void d2h(Context &c, double *dst, const double *src, int64_t n) {
+    REQUIRE(dst != nullptr, CCSD_GPU_EINVAL, "null output pointer");
+    CU_CHECK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, c.ex.stream));
+    CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int ccsd_gpu_create(int64_t n_o, int64_t n_v, int64_t n_J, const ccsd_gpu_options *opt, void **ctx) {
+    if (!ctx) return CCSD_GPU_EINVAL;
+    *ctx = nullptr;
+    try {
+        if (n_o <= 0 || n_v <= 0 || n_J <= 0) throw Error(CCSD_GPU_EINVAL, "dimensions must be positive");
+        if (opt && opt->precision != CCSD_GPU_FP64 && opt->precision != CCSD_GPU_MIXED)
+            throw Error(CCSD_GPU_EINVAL, "unknown precision");
+        *ctx = new Context(n_o, n_v, n_J, opt);
+        return CCSD_GPU_OK;
+    } catch (const Error &e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return CCSD_GPU_ECUDA;
+    }
+}
+
+void ccsd_gpu_destroy(void *ctx) {
+    if (!ctx) return;
+    Context *c = static_cast<Context *>(ctx);
+    cudaSetDevice(c->device);
+    delete c;
+}
+
+const char *ccsd_gpu_last_error(void *ctx) {
+    if (!ctx) return g_create_error.c_str();
+    return static_cast<Context *>(ctx)->err.c_str();
+}
+
+int ccsd_gpu_set_precision(void *ctx, int32_t precision) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(precision == CCSD_GPU_FP64 || precision == CCSD_GPU_MIXED, CCSD_GPU_EINVAL, "unknown precision");
+        c.ex.prec = precision == CCSD_GPU_MIXED ? ccsd::Prec::MIXED : ccsd::Prec::FP64;
+    });
+}
+
+int ccsd_gpu_set_stream(void *ctx, void *stream) {
+    return guarded(ctx, [&](Context &c) {
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        c.set_stream(static_cast<cudaStream_t>(stream));
+    });
+}
+
+int ccsd_gpu_synchronize(void *ctx) {
+    return guarded(ctx, [&](Context &c) { CU_CHECK(cudaStreamSynchronize(c.ex.stream)); });
+}
+
+int ccsd_gpu_set_cholesky_mo(void *ctx, const double *L) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(L != nullptr, CCSD_GPU_EINVAL, "null L");
+        // split (J, n_mo, n_mo) into the four blocks with strided 2-D copies per q
+        const int64_t J = c.nJ, nmo = c.nmo, no = c.no, nv = c.nv;
+        auto blk = [&](ccsd::DBuf &dst, int64_t p0, int64_t np, int64_t q0, int64_t nq) {
+            // dst[J, p, q] <- L[J, p0+p, q0+q]: for each q a contiguous run of J*np
+            CU_CHECK(cudaMemcpy2DAsync(dst.d(), sizeof(double) * J * np, L + J * (p0 + nmo * q0),
+                                       sizeof(double) * J * nmo, sizeof(double) * J * np, nq,
+                                       cudaMemcpyHostToDevice, c.ex.stream));
+        };
+        blk(c.L_oo, 0, no, 0, no);
+        blk(c.L_ov, 0, no, no, nv);
+        blk(c.L_vo, no, nv, 0, no);
+        blk(c.L_vv, no, nv, no, nv);
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        c.have_L = true;
+        if (c.have_h) c.refresh();
+    });
+}
+
+int ccsd_gpu_set_cholesky_mo_blocks(void *ctx, const double *L_oo, const double *L_ov, const double *L_vo,
+                                    const double *L_vv) {
+    return guarded(ctx, [&](Context &c) {
+        h2d(c, c.L_oo.d(), L_oo, c.nJ * c.no * c.no);
+        h2d(c, c.L_ov.d(), L_ov, c.nJ * c.no * c.nv);
+        h2d(c, c.L_vo.d(), L_vo, c.nJ * c.nv * c.no);
+        h2d(c, c.L_vv.d(), L_vv, c.nJ * c.nv * c.nv);
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        c.have_L = true;
+        if (c.have_h) c.refresh();
+    });
+}
+
+int ccsd_gpu_set_h_mo(void *ctx, const double *h, const double *eps, double e_hf) {
+    return guarded(ctx, [&](Context &c) {
+        h2d(c, c.h.d(), h, c.nmo * c.nmo);
+        h2d(c, c.eps.d(), eps, c.nmo);
+        c.e_hf = e_hf;
+        ccsd::orbital_differences(c.ex, c.eps.d(), c.no, c.nv, c.epsdiff.d());
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        c.have_h = true;
+        if (c.have_L) c.refresh();
+    });
+}
+
+int ccsd_gpu_set_amplitudes(void *ctx, const double *t) {
+    return guarded(ctx, [&](Context &c) {
+        h2d(c, c.t.d(), t, c.namp);
+        c.have_t = true;
+        c.refresh();
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+    });
+}
+
+int ccsd_gpu_get_amplitudes(void *ctx, double *t) {
+    return guarded(ctx, [&](Context &c) { d2h(c, t, c.t.d(), c.namp); });
+}
+
+int ccsd_gpu_mp2_guess(void *ctx) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(c.have_L && c.have_h, CCSD_GPU_ESTATE, "Cholesky vectors and h must be set first");
+        c.mp2_guess();
+        c.refresh();
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+    });
+}
+
+int ccsd_gpu_get_fock(void *ctx, double *F) {
+    return guarded(ctx, [&](Context &c) { d2h(c, F, c.F.d(), c.nmo * c.nmo); });
+}
+
+int ccsd_gpu_energy(void *ctx, double *energy) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(energy != nullptr, CCSD_GPU_EINVAL, "null output");
+        REQUIRE(c.have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+        *energy = c.energy();
+    });
+}
+
+int ccsd_gpu_omega(void *ctx, double *omega) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(omega != nullptr, CCSD_GPU_EINVAL, "null output");
+        ccsd::DBuf om = ccsd::dalloc(c.namp, c.ex.stream);
+        c.omega(om.d());
+        d2h(c, omega, om.d(), c.namp);
+    });
+}
+
+int ccsd_gpu_omega_device(void *ctx, double *d_omega) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(d_omega != nullptr, CCSD_GPU_EINVAL, "null output");
+        c.omega(d_omega);
+    });
+}
+
+int ccsd_gpu_jacobian(void *ctx, int64_t, const double *, double *) {
+    return guarded(ctx, [&](Context &) { throw Error(CCSD_GPU_EINVAL, "jacobian transformation not available"); });
+}
+
+int ccsd_gpu_jacobian_transpose(void *ctx, int64_t, const double *, double *) {
+    return guarded(ctx, [&](Context &) {
+        throw Error(CCSD_GPU_EINVAL, "transpose jacobian transformation not available");
+    });
+}
+
+int ccsd_gpu_solve_gs(void *ctx, const ccsd_gpu_solver_options *opt, double *energy, int32_t *iterations,
+                      double *history) {
+    int status = CCSD_GPU_OK;
+    int rc = guarded(ctx, [&](Context &c) { status = c.solve_gs(opt, energy, iterations, history); });
+    if (rc != CCSD_GPU_OK) return rc;
+    if (status != CCSD_GPU_OK) static_cast<Context *>(ctx)->err = "ground state did not converge";
+    return status;
+}
+
+int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops) {
+    return guarded(ctx, [&](Context &c) {
+        if (kernel_launches) *kernel_launches = c.ex.launches;
+        if (gemm_flops) *gemm_flops = c.ex.flops;
+    });
+}
+
+double ccsd_gpu_omega_flops(void *ctx) {
+    if (!ctx) return 0.0;
+    return static_cast<Context *>(ctx)->omega_flops();
+}
+
+}  // extern "C"

@@ -1,0 +1,491 @@
+// CCSD hot path on one B200: T1-transformed Cholesky vectors, T1 Fock matrix, energy,
+// the residual Omega(t), and the device-resident quasi-Newton + DIIS ground-state solver.
+// Each step restates one eT routine (paths relative to the eT source tree).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "ccsd.cuh"
+#include "ccsd_kernels.cuh"
+#include "tensor_ops.cuh"
+
+namespace ccsd {
+
+Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *opt)
+    : no(no_), nv(nv_), nJ(nJ_) {
+    REQUIRE(no > 0 && nv > 0 && nJ > 0, CCSD_GPU_EINVAL, "dimensions must be positive");
+    nmo = no + nv;
+    nov = no * nv;
+    nt1 = nov;
+    nt2 = nov * (nov + 1) / 2;
+    namp = nt1 + nt2;
+    device = opt ? opt->device : 0;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Error(CCSD_GPU_ENODEV, "no CUDA device available");
+    REQUIRE(device >= 0 && device < ndev, CCSD_GPU_EINVAL, "device ordinal out of range");
+    CU_CHECK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CU_CHECK(cudaGetDeviceProperties(&prop, device));
+    REQUIRE(prop.major == 10, CCSD_GPU_ENODEV,
+            std::string("this library is built for sm_100a; device is sm_") + std::to_string(prop.major) +
+                std::to_string(prop.minor));
+    cudaMemPool_t pool;
+    CU_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;
+    CU_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    CU_CHECK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    BLAS_CHECK(cublasCreate(&blas));
+    set_stream(nullptr);
+    ex.blas = blas;
+    ex.prec = (opt && opt->precision == CCSD_GPU_MIXED) ? Prec::MIXED : Prec::FP64;
+    if (opt && opt->mixed_min_flops > 0) ex.mixed_min_flops = (double)opt->mixed_min_flops;
+    ladder_batch = opt ? opt->ladder_batch : 0;
+    cudaStream_t s = ex.stream;
+    for (auto *b : {&L_oo, &Lt_oo}) *b = dalloc(nJ * no * no, s);
+    for (auto *b : {&L_ov, &Lt_ov}) *b = dalloc(nJ * no * nv, s);
+    for (auto *b : {&L_vo, &Lt_vo}) *b = dalloc(nJ * nv * no, s);
+    for (auto *b : {&L_vv, &Lt_vv}) *b = dalloc(nJ * nv * nv, s);
+    h = dalloc(nmo * nmo, s);
+    eps = dalloc(nmo, s);
+    F = dalloc(nmo * nmo, s);
+    t = dalloc(namp, s);
+    epsdiff = dalloc(namp, s);
+    scal = dalloc(64, s);
+    fill(ex, t.d(), namp, 0.0);
+    CU_CHECK(cudaStreamSynchronize(s));
+}
+
+Context::~Context() {
+    if (own_stream) cudaStreamSynchronize(own_stream);
+    if (ex.stream && ex.stream != own_stream) cudaStreamSynchronize(ex.stream);
+    // buffers are freed (stream-ordered) by their destructors before the stream goes away
+    L_oo.release(); L_ov.release(); L_vo.release(); L_vv.release();
+    Lt_oo.release(); Lt_ov.release(); Lt_vo.release(); Lt_vv.release();
+    h.release(); eps.release(); F.release(); t.release(); epsdiff.release(); scal.release();
+    if (blas) cublasDestroy(blas);
+    if (own_stream) {
+        cudaStreamSynchronize(own_stream);
+        cudaStreamDestroy(own_stream);
+    }
+}
+
+void Context::set_stream(cudaStream_t s) {
+    ex.stream = s ? s : own_stream;
+    BLAS_CHECK(cublasSetStream(blas, ex.stream));
+}
+
+// ---------------------------------------------------------------------------
+// T1 transformation of the Cholesky vectors (src/wavefunctions/ccs/t1_ccs.F90:208-499)
+// ---------------------------------------------------------------------------
+void Context::t1_transform_cholesky() {
+    const double *t1 = t.d();
+    TV T1 = tv(t1, {nv, no});
+    cudaStream_t s = ex.stream;
+    // ov block unchanged
+    CU_CHECK(cudaMemcpyAsync(Lt_ov.d(), L_ov.d(), sizeof(double) * nJ * no * nv, cudaMemcpyDeviceToDevice, s));
+    // oo: L_ij + sum_a L_ia t_aj                                   (:251-290)
+    CU_CHECK(cudaMemcpyAsync(Lt_oo.d(), L_oo.d(), sizeof(double) * nJ * no * no, cudaMemcpyDeviceToDevice, s));
+    contract(ex, "Jia,aj->Jij", 1.0, tv(L_ov.d(), {nJ, no, nv}), T1, 1.0, tv(Lt_oo.d(), {nJ, no, no}));
+    // vo: L_ai + sum_b L_ab t_bi - sum_j t_aj (L_ji + sum_b L_jb t_bi) (:293-440); the bracket is Lt_oo
+    CU_CHECK(cudaMemcpyAsync(Lt_vo.d(), L_vo.d(), sizeof(double) * nJ * nv * no, cudaMemcpyDeviceToDevice, s));
+    contract(ex, "Jab,bi->Jai", 1.0, tv(L_vv.d(), {nJ, nv, nv}), T1, 1.0, tv(Lt_vo.d(), {nJ, nv, no}));
+    contract(ex, "aj,Jji->Jai", -1.0, T1, tv(Lt_oo.d(), {nJ, no, no}), 1.0, tv(Lt_vo.d(), {nJ, nv, no}));
+    // vv: L_ab - sum_j t_aj L_jb                                  (:443-499)
+    CU_CHECK(cudaMemcpyAsync(Lt_vv.d(), L_vv.d(), sizeof(double) * nJ * nv * nv, cudaMemcpyDeviceToDevice, s));
+    contract(ex, "aj,Jjb->Jab", -1.0, T1, tv(L_ov.d(), {nJ, no, nv}), 1.0, tv(Lt_vv.d(), {nJ, nv, nv}));
+}
+
+// ---------------------------------------------------------------------------
+// T1 Fock matrix F_pq = h~_pq + sum_k (2 g~_pqkk - g~_pkkq)
+// (src/wavefunctions/ccsd/fock_ccsd.F90:34-78, src/wavefunctions/ccs/fock_ccs.F90:242-1107)
+// ---------------------------------------------------------------------------
+void Context::construct_fock() {
+    cudaStream_t s = ex.stream;
+    double *Fm = F.d();
+    TV T1 = tv(t.d(), {nv, no});
+    // h~ = X h Y^T, X = 1 - t1, Y = 1 + t1^T (t1_ccs.F90:34-95)
+    CU_CHECK(cudaMemcpyAsync(Fm, h.d(), sizeof(double) * nmo * nmo, cudaMemcpyDeviceToDevice, s));
+    auto blk = [&](double *base, int64_t r0, int64_t c0, int64_t nr, int64_t nc) {
+        TV v;
+        v.p = base + r0 + nmo * c0;
+        v.nd = 2;
+        v.n[0] = nr;
+        v.n[1] = nc;
+        v.s[0] = 1;
+        v.s[1] = nmo;
+        return v;
+    };
+    // rows v: W_aq -= sum_i t_ai h_iq
+    contract(ex, "ai,iq->aq", -1.0, T1, blk(h.d(), 0, 0, no, nmo), 1.0, blk(Fm, no, 0, nv, nmo));
+    // cols o: W_pi += sum_a W_pa t_ai
+    contract(ex, "pa,ai->pi", 1.0, blk(Fm, 0, no, nmo, nv), T1, 1.0, blk(Fm, 0, 0, nmo, no));
+    // Coulomb: 2 sum_J L~_pq X_J with X_J = sum_k L~_kk
+    DBuf X = dalloc(nJ, s);
+    trace_oo(ex, Lt_oo.d(), nJ, no, X.d());
+    TV XJ = tv(X.d(), {nJ});
+    contract(ex, "Jpq,J->pq", 2.0, tv(Lt_oo.d(), {nJ, no, no}), XJ, 1.0, blk(Fm, 0, 0, no, no));
+    contract(ex, "Jpq,J->pq", 2.0, tv(Lt_ov.d(), {nJ, no, nv}), XJ, 1.0, blk(Fm, 0, no, no, nv));
+    contract(ex, "Jpq,J->pq", 2.0, tv(Lt_vo.d(), {nJ, nv, no}), XJ, 1.0, blk(Fm, no, 0, nv, no));
+    contract(ex, "Jpq,J->pq", 2.0, tv(Lt_vv.d(), {nJ, nv, nv}), XJ, 1.0, blk(Fm, no, no, nv, nv));
+    // exchange: - sum_{J,k} L~_pk L~_kq
+    contract(ex, "Jpk,Jkq->pq", -1.0, tv(Lt_oo.d(), {nJ, no, no}), tv(Lt_oo.d(), {nJ, no, no}), 1.0,
+             blk(Fm, 0, 0, no, no));
+    contract(ex, "Jpk,Jkq->pq", -1.0, tv(Lt_oo.d(), {nJ, no, no}), tv(Lt_ov.d(), {nJ, no, nv}), 1.0,
+             blk(Fm, 0, no, no, nv));
+    contract(ex, "Jpk,Jkq->pq", -1.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_oo.d(), {nJ, no, no}), 1.0,
+             blk(Fm, no, 0, nv, no));
+    contract(ex, "Jpk,Jkq->pq", -1.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_ov.d(), {nJ, no, nv}), 1.0,
+             blk(Fm, no, no, nv, nv));
+}
+
+void Context::refresh() {
+    REQUIRE(have_L && have_h, CCSD_GPU_ESTATE, "Cholesky vectors and h must be set first");
+    Prec keep = ex.prec;
+    ex.prec = Prec::FP64;      // the T1 transformation and the Fock matrix stay FP64
+    t1_transform_cholesky();
+    construct_fock();
+    ex.prec = keep;
+}
+
+// g_ovov[i,a,j,b] = sum_J L_ia L_jb  (eri_t1%get('ovov'))
+DBuf Context::g_ovov() {
+    DBuf g = dalloc(nov * nov, ex.stream);
+    contract(ex, "Jia,Jjb->iajb", 1.0, tv(Lt_ov.d(), {nJ, no, nv}), tv(Lt_ov.d(), {nJ, no, nv}), 0.0,
+             tv(g.d(), {no, nv, no, nv}));
+    return g;
+}
+
+// calculate_energy_ccsd (src/wavefunctions/ccsd/mean_value_ccsd.F90:36-99), FP64
+double Context::energy() {
+    Prec keep = ex.prec;
+    ex.prec = Prec::FP64;
+    DBuf g = g_ovov();
+    energy_reduce(ex, t.d(), t.d() + nt1, g.d(), no, nv, e_hf, scal.d());
+    ex.prec = keep;
+    double e;
+    CU_CHECK(cudaMemcpyAsync(&e, scal.d(), sizeof(double), cudaMemcpyDeviceToHost, ex.stream));
+    CU_CHECK(cudaStreamSynchronize(ex.stream));
+    return e;
+}
+
+// set_t2_to_cc2_guess (src/wavefunctions/ccsd/ccsd_class.F90:478-533) at t1 = 0
+void Context::mp2_guess() {
+    fill(ex, t.d(), namp, 0.0);
+    refresh();
+    orbital_differences(ex, eps.d(), no, nv, epsdiff.d());
+    DBuf g = dalloc(nov * nov, ex.stream);
+    Prec keep = ex.prec;
+    ex.prec = Prec::FP64;
+    contract(ex, "Jai,Jbj->aibj", 1.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_vo.d(), {nJ, nv, no}), 0.0,
+             tv(g.d(), {nv, no, nv, no}));
+    ex.prec = keep;
+    mp2_amplitudes(ex, g.d(), epsdiff.d(), nov, t.d() + nt1);
+    have_t = true;
+}
+
+// ---------------------------------------------------------------------------
+// A2 ladder: Omega^ab_ij += sum_cd g_acbd t^cd_ij with the +/- symmetrisation of
+// omega_ccsd_a2 (src/wavefunctions/ccsd/omega_ccsd.F90:113-480), batched over a.
+// ---------------------------------------------------------------------------
+void Context::ladder(const double *t2, double *om2) {
+    cudaStream_t s = ex.stream;
+    const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
+    const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
+    DBuf tp = dalloc(nop * nvp, s), tm = dalloc(std::max<int64_t>(nom * nvm, 1), s);
+    build_tpm(ex, t2, tp.d(), tm.d(), no, nv);
+    // L~_vv as (J, c, a): columns (c, a) of one a-block are contiguous
+    DBuf LT = dalloc(nJ * nv * nv, s);
+    {
+        TV src = tv(Lt_vv.d(), {nJ, nv, nv});   // [J, a, c]
+        TV dst;
+        dst.p = LT.d();
+        dst.nd = 3;
+        dst.n[0] = nJ;
+        dst.n[1] = nv;
+        dst.n[2] = nv;
+        dst.s[0] = 1;
+        dst.s[1] = nJ * nv;   // a
+        dst.s[2] = nJ;        // c
+        permute_add(ex, 1.0, src, 0.0, dst);
+    }
+    // batch length over a: keep G + g+- within the budget
+    int64_t nA = ladder_batch;
+    if (nA <= 0) {
+        const double budget = 6.0e9;   // bytes
+        double per_a = 8.0 * (double)nv * nv * nv + 16.0 * (double)nvp * nv;
+        nA = std::max<int64_t>(1, std::min<int64_t>(nv, (int64_t)(budget / per_a)));
+    }
+    int64_t maxab = 0;
+    for (int64_t a0 = 0; a0 < nv; a0 += nA) {
+        int64_t a1 = std::min(nv, a0 + nA);
+        maxab = std::max(maxab, a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2);
+    }
+    DBuf G = dalloc(nv * nA * nv * nv, s);
+    DBuf gp = dalloc(nvp * maxab, s), gm = dalloc(std::max<int64_t>(nvm * maxab, 1), s);
+    DBuf wp = dalloc(nop * maxab, s), wm = dalloc(std::max<int64_t>(nom * maxab, 1), s);
+    for (int64_t a0 = 0; a0 < nv; a0 += nA) {
+        int64_t a1 = std::min(nv, a0 + nA);
+        int64_t M = nv * (a1 - a0), N = nv * a1;
+        // G[(c,a),(d,b)] = sum_J L_ac L_bd   (eri_t1%get('vvvv') / get_packed('vv'))
+        gemm(ex, true, false, M, N, nJ, 1.0, LT.d() + nJ * nv * a0, nJ, LT.d(), nJ, 0.0, G.d(), M);
+        form_gpm(ex, G.d(), M, gp.d(), gm.d(), nv, a0, a1);
+        int64_t nabp = a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2;
+        int64_t nabm = a1 * (a1 - 1) / 2 - a0 * (a0 - 1) / 2;
+        gemm(ex, false, false, nop, nabp, nvp, 0.5, tp.d(), nop, gp.d(), nvp, 0.0, wp.d(), nop);
+        if (nom > 0 && nabm > 0)
+            gemm(ex, false, false, nom, nabm, nvm, 0.5, tm.d(), nom, gm.d(), nvm, 0.0, wm.d(), nom);
+        add_omega_pm(ex, om2, wp.d(), wm.d(), no, nv, a0, a1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// construct_omega_ccsd (src/wavefunctions/ccsd/omega_ccsd.F90:39-110)
+// ---------------------------------------------------------------------------
+void Context::omega(double *om_out) {
+    REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+    cudaStream_t s = ex.stream;
+    const double *t1 = t.d(), *t2 = t.d() + nt1;
+    double *om1 = om_out, *om2 = om_out + nt1;
+    const int64_t N4 = nov * nov;
+    auto V4 = [&](const double *p) { return tv(p, {nv, no, nv, no}); };
+    // view of x[a,i,b,j] as y[a,i,b,j] = x[P(a,i,b,j)] for the permutation given by strides
+    auto V4s = [&](const double *p, int64_t sa, int64_t si, int64_t sb, int64_t sj) {
+        TV v = tv(p, {nv, no, nv, no});
+        v.s[0] = sa;
+        v.s[1] = si;
+        v.s[2] = sb;
+        v.s[3] = sj;
+        return v;
+    };
+    const int64_t Sa = 1, Si = nv, Sb = nov, Sj = nov * nv;   // strides of a (v,o,v,o) array
+
+    // omega_ccs_a1 (src/wavefunctions/ccs/omega_ccs.F90:62): Omega_ai = F_ai
+    {
+        TV Fvo;
+        Fvo.p = F.d() + no;
+        Fvo.nd = 2;
+        Fvo.n[0] = nv;
+        Fvo.n[1] = no;
+        Fvo.s[0] = 1;
+        Fvo.s[1] = nmo;
+        permute_add(ex, 1.0, Fvo, 0.0, tv(om1, {nv, no}));
+    }
+    DBuf tf = dalloc(N4, s), u = dalloc(N4, s);
+    squareup(ex, t2, tf.d(), nov);
+    // u_aibj = 2 t_aibj - t_ajbi (construct_u_aibj_ccsd, omega_ccsd.F90:881-914)
+    permute_add(ex, 2.0, V4(tf.d()), 0.0, V4(u.d()));
+    permute_add(ex, -1.0, V4s(tf.d(), Sa, Sj, Sb, Si), 1.0, V4(u.d()));
+
+    TV OM1 = tv(om1, {nv, no});
+    // omega_doubles_a1 (src/wavefunctions/doubles/omega_doubles.F90:36-138)
+    {
+        DBuf X = dalloc(nJ * nov, s);
+        contract(ex, "Jcj,cjbi->Jbi", 1.0, tv(L_vo.d(), {nJ, nv, no}), V4(u.d()), 0.0, tv(X.d(), {nJ, nv, no}));
+        contract(ex, "Jab,Jbi->ai", 1.0, tv(Lt_vv.d(), {nJ, nv, nv}), tv(X.d(), {nJ, nv, no}), 1.0, OM1);
+    }
+    // omega_doubles_b1 (:141-204): - sum_jbk u_ajbk g_kbji
+    {
+        DBuf g = dalloc(nov * no * no, s);
+        contract(ex, "Jkb,Jji->kbji", 1.0, tv(Lt_ov.d(), {nJ, no, nv}), tv(Lt_oo.d(), {nJ, no, no}), 0.0,
+                 tv(g.d(), {no, nv, no, no}));
+        contract(ex, "ajbk,kbji->ai", -1.0, V4(u.d()), tv(g.d(), {no, nv, no, no}), 1.0, OM1);
+    }
+    // omega_doubles_c1 (:207-258): sum_bj u_aibj F_jb
+    {
+        TV Fov;
+        Fov.p = F.d() + nmo * no;
+        Fov.nd = 2;
+        Fov.n[0] = no;
+        Fov.n[1] = nv;
+        Fov.s[0] = 1;
+        Fov.s[1] = nmo;
+        contract(ex, "aibj,jb->ai", 1.0, V4(u.d()), Fov, 1.0, OM1);
+    }
+
+    DBuf gov = g_ovov();                 // g[l,d,k,c] = g_ldkc, shared by E2, B2, C2/D2
+    TV G4 = tv(gov.d(), {no, nv, no, nv});
+    DBuf om = dalloc(N4, s), omS = dalloc(N4, s);
+    // omega_ccsd_e2 (omega_ccsd.F90:712-878)
+    {
+        DBuf X = dalloc(nv * nv, s), Y = dalloc(no * no, s);
+        TV Fvv, Foo;
+        Fvv.p = F.d() + no + nmo * no;
+        Foo.p = F.d();
+        Fvv.nd = Foo.nd = 2;
+        Fvv.n[0] = Fvv.n[1] = nv;
+        Foo.n[0] = Foo.n[1] = no;
+        Fvv.s[0] = Foo.s[0] = 1;
+        Fvv.s[1] = Foo.s[1] = nmo;
+        permute_add(ex, 1.0, Fvv, 0.0, tv(X.d(), {nv, nv}));
+        permute_add(ex, 1.0, Foo, 0.0, tv(Y.d(), {no, no}));
+        // X_bc = F_bc - sum_dkl u_bkdl g_ldkc
+        contract(ex, "bkdl,ldkc->bc", -1.0, V4(u.d()), G4, 1.0, tv(X.d(), {nv, nv}));
+        // E2.1 ordered (b,j,a,i)
+        contract(ex, "bc,cjai->bjai", 1.0, tv(X.d(), {nv, nv}), V4(tf.d()), 0.0, V4(om.d()));
+        // Y_kj = F_kj + sum_cdl g_kdlc u_djcl
+        contract(ex, "kdlc,djcl->kj", 1.0, G4, V4(u.d()), 1.0, tv(Y.d(), {no, no}));
+        // E2.2: - sum_k t_aibk Y_kj
+        contract(ex, "aibk,kj->aibj", -1.0, V4(tf.d()), tv(Y.d(), {no, no}), 1.0, V4(om.d()));
+    }
+    // symmetric_sum (src/tools/reordering.F90:416)
+    permute_add(ex, 1.0, V4(om.d()), 0.0, V4(omS.d()));
+    permute_add(ex, 1.0, V4s(om.d(), Sb, Sj, Sa, Si), 1.0, V4(omS.d()));
+    // omega_ccsd_b2 (omega_ccsd.F90:483-583)
+    {
+        contract(ex, "Jai,Jbj->aibj", 1.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_vo.d(), {nJ, nv, no}), 1.0,
+                 V4(omS.d()));
+        DBuf X = dalloc(no * no * no * no, s);
+        TV X4 = tv(X.d(), {no, no, no, no});
+        contract(ex, "Jki,Jlj->klij", 1.0, tv(Lt_oo.d(), {nJ, no, no}), tv(Lt_oo.d(), {nJ, no, no}), 0.0, X4);
+        contract(ex, "kcld,cidj->klij", 1.0, G4, V4(tf.d()), 1.0, X4);
+        contract(ex, "akbl,klij->aibj", 1.0, V4(tf.d()), X4, 1.0, V4(omS.d()));
+    }
+    // omega_ccsd_c2_d2 (omega_ccsd.F90:586-709), eT's DSYMM sequence written as contractions
+    {
+        DBuf C = dalloc(N4, s), D = dalloc(N4, s);
+        TV C4 = V4(C.d()), D4 = V4(D.d());
+        contract(ex, "Jac,Jkj->ckaj", 1.0, tv(Lt_vv.d(), {nJ, nv, nv}), tv(Lt_oo.d(), {nJ, no, no}), 0.0, C4);
+        permute_add(ex, -1.0, C4, 0.0, D4);
+        contract(ex, "Jai,Jkc->ckai", 2.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_ov.d(), {nJ, no, nv}), 1.0, D4);
+        // C_claj -= 1/2 sum_dk g_kcld t_djak        (dsymm 'R','U', -1/2)
+        contract(ex, "kcld,djak->claj", -0.5, G4, V4(tf.d()), 1.0, C4);
+        // D_claj += 1/2 sum_dk (2 g_lckd - g_kcld) u_dkaj   (contra + dsymm 'R','L', +1/2)
+        contract(ex, "lckd,dkaj->claj", 1.0, G4, V4(u.d()), 1.0, D4);
+        contract(ex, "kcld,dkaj->claj", -0.5, G4, V4(u.d()), 1.0, D4);
+        // x = -3/2 sum_ck t_akci C_ckbj  (dsymm 'L','U'); w = 1/2 sum_ck u_aick D_ckbj (dsymm 'L','L')
+        DBuf x = std::move(om);   // reuse
+        contract(ex, "akci,ckbj->aibj", -1.5, V4(tf.d()), C4, 0.0, V4(x.d()));
+        DBuf w = std::move(C);
+        contract(ex, "aick,ckbj->aibj", 0.5, V4(u.d()), D4, 0.0, V4(w.d()));
+        // symmetrize_and_pack(contra, psrq): (x + 2 x_psrq)/3 ; then P(w)
+        permute_add(ex, 1.0 / 3.0, V4(x.d()), 1.0, V4(w.d()));
+        permute_add(ex, 2.0 / 3.0, V4s(x.d(), Sa, Sj, Sb, Si), 1.0, V4(w.d()));
+        permute_add(ex, 1.0, V4(w.d()), 1.0, V4(omS.d()));
+        permute_add(ex, 1.0, V4s(w.d(), Sb, Sj, Sa, Si), 1.0, V4(omS.d()));
+    }
+    // scale_diagonal(1/2) + packin
+    fill(ex, om2, nt2, 0.0);
+    pack_half_diag_add(ex, 1.0, omS.d(), om2, nov);
+    // omega_ccsd_a2
+    ladder(t2, om2);
+}
+
+// ---------------------------------------------------------------------------
+// run_diis_cc_gs (src/solvers/cc/diis_cc_gs_class.F90:209-315)
+// ---------------------------------------------------------------------------
+int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int32_t *iters, double *history) {
+    REQUIRE(have_t && have_L && have_h, CCSD_GPU_ESTATE, "inputs/amplitudes not set");
+    const int maxit = o && o->max_iterations > 0 ? o->max_iterations : 100;
+    const int dim = o && o->diis_dimension > 0 ? std::min(o->diis_dimension, 16) : 8;
+    const double othr = o && o->omega_threshold > 0 ? o->omega_threshold : 1e-5;
+    const double ethr = o ? o->energy_threshold : 1e-5;
+    const double refine = o && o->refine_threshold > 0 ? o->refine_threshold : 1e-4;
+    cudaStream_t s = ex.stream;
+    orbital_differences(ex, eps.d(), no, nv, epsdiff.d());
+    DBuf omega_v = dalloc(namp, s);
+    std::vector<DBuf> errs(dim), pars(dim);
+    for (int k = 0; k < dim; k++) {
+        errs[k] = dalloc(namp, s);
+        pars[k] = dalloc(namp, s);
+    }
+    DBuf Gs = dalloc(16 * 16, s), dots = dalloc(16, s), wts = dalloc(16, s);
+    DBuf stat(sizeof(int), s);
+    std::vector<int> order;   // slots, oldest first
+    const Prec user = ex.prec;
+    bool fp64_phase = (user == Prec::FP64);
+    double prev = 0.0, e = 0.0;
+    int it = 0;
+    bool conv = false;
+    while (it < maxit) {
+        it++;
+        refresh();
+        e = energy();
+        ex.prec = fp64_phase ? Prec::FP64 : user;
+        omega(omega_v.d());
+        dot(ex, omega_v.d(), omega_v.d(), namp, scal.d());
+        double nrm2;
+        CU_CHECK(cudaMemcpyAsync(&nrm2, scal.d(), sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU_CHECK(cudaStreamSynchronize(s));
+        double nrm = std::sqrt(nrm2);
+        if (!std::isfinite(nrm) || !std::isfinite(e)) {
+            ex.prec = user;
+            throw Error(CCSD_GPU_ENAN, "non-finite energy or residual in iteration " + std::to_string(it));
+        }
+        if (history) {
+            history[2 * (it - 1)] = e;
+            history[2 * (it - 1) + 1] = nrm;
+        }
+        if (!fp64_phase && nrm < refine) {
+            // iterative refinement: from here on Omega is evaluated in FP64; re-evaluate now
+            fp64_phase = true;
+            ex.prec = Prec::FP64;
+            omega(omega_v.d());
+            dot(ex, omega_v.d(), omega_v.d(), namp, scal.d());
+            CU_CHECK(cudaMemcpyAsync(&nrm2, scal.d(), sizeof(double), cudaMemcpyDeviceToHost, s));
+            CU_CHECK(cudaStreamSynchronize(s));
+            nrm = std::sqrt(nrm2);
+            if (history) history[2 * (it - 1) + 1] = nrm;
+        }
+        bool econv = ethr < 0 || std::fabs(e - prev) < ethr;
+        if (fp64_phase && nrm < othr && econv) {
+            conv = true;
+            break;
+        }
+        // quasi-Newton step (quasi_newton_updater_class.F90, amplitude_updater_class.F90)
+        qn_update(ex, omega_v.d(), epsdiff.d(), t.d(), namp, nt1);
+        // diis%update(e = scaled preconditioned residual, x = updated amplitudes)
+        int slot;
+        if ((int)order.size() < dim) {
+            slot = (int)order.size();
+            order.push_back(slot);
+        } else {
+            slot = order.front();
+            order.erase(order.begin());
+            order.push_back(slot);
+        }
+        CU_CHECK(cudaMemcpyAsync(errs[slot].d(), omega_v.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
+        CU_CHECK(cudaMemcpyAsync(pars[slot].d(), t.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
+        std::vector<const double *> eptr(dim, nullptr);
+        for (int k = 0; k < dim; k++) eptr[k] = errs[k].d();
+        multi_dot(ex, omega_v.d(), eptr.data(), std::max<int>((int)order.size(), 1), namp, dots.d());
+        DiisOrder ord{};
+        ord.n = (int)order.size();
+        for (int k = 0; k < ord.n; k++) ord.slot[k] = order[k];
+        diis_solve(ex, Gs.d(), 16, dots.d(), slot, ord, wts.d(), stat.as<int>());
+        std::vector<const double *> recs(ord.n);
+        for (int k = 0; k < ord.n; k++) recs[k] = pars[order[k]].d();
+        extrapolate(ex, recs.data(), wts.d(), ord.n, namp, t.d());
+        int st = 0;
+        CU_CHECK(cudaMemcpyAsync(&st, stat.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CU_CHECK(cudaStreamSynchronize(s));
+        if (st) {
+            ex.prec = user;
+            throw Error(CCSD_GPU_ESINGULAR, "could not solve DIIS matrix equation");
+        }
+        prev = e;
+    }
+    ex.prec = user;
+    refresh();
+    if (energy_out) *energy_out = e;
+    if (iters) *iters = it;
+    return conv ? CCSD_GPU_OK : CCSD_GPU_ENOCONV;
+}
+
+// Sum of 2mnk over eT's BLAS call sites of construct_omega (DSFRK: n(n+1)k).
+double Context::omega_flops() const {
+    const double o = (double)no, v = (double)nv, J = (double)nJ, ov = o * v;
+    const double nop = o * (o + 1) / 2, nom = o * (o - 1) / 2, nvp = v * (v + 1) / 2, nvm = v * (v - 1) / 2;
+    double f = 0;
+    f += 2 * J * ov * ov + 2 * v * o * J * v;                  // omega_doubles_a1
+    f += 2 * ov * o * o * J + 2 * v * o * o * o * v;            // b1 (ovoo get + dgemm)
+    f += 2 * ov * ov;                                           // c1
+    f += 2 * ov * ov * J + 2 * v * v * v * o * o * 2 + 2 * o * o * o * v * v * 2;   // e2
+    f += 2 * ov * ov * J * 2 + 2 * o * o * o * o * J + 2 * o * o * o * o * v * v * 2;   // b2
+    f += 2 * v * v * o * o * J + 2 * ov * ov * J * 2 + 8 * ov * ov * ov;   // c2/d2
+    f += v * v * (v * v + 1) * J + 2 * nop * nvp * nvp + 2 * nom * nvm * nvm;   // a2 (single batch)
+    return f;
+}
+
+}  // namespace ccsd

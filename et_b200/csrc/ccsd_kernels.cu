@@ -1,0 +1,358 @@
+// Bandwidth kernels of the CCSD path: packed index algebra, A2 ladder +/- forms,
+// energy, MP2 guess, quasi-Newton update and DIIS (all FP64).
+#include <cmath>
+
+#include "ccsd_kernels.cuh"
+
+namespace ccsd {
+
+namespace {
+
+__device__ __forceinline__ int64_t pk(int64_t x, int64_t y) {
+    int64_t M = x > y ? x : y, m = x > y ? y : x;
+    return M * (M + 1) / 2 + m;
+}
+
+// (M, m) with M >= m from a lower-triangle index M(M+1)/2 + m
+__device__ __forceinline__ void untri(int64_t idx, int64_t &M, int64_t &m) {
+    int64_t r = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while (r * (r + 1) / 2 > idx) r--;
+    while ((r + 1) * (r + 2) / 2 <= idx) r++;
+    M = r;
+    m = idx - r * (r + 1) / 2;
+}
+
+// strict lower triangle: idx = M(M-1)/2 + m, M > m
+__device__ __forceinline__ void untri_strict(int64_t idx, int64_t &M, int64_t &m) {
+    untri(idx, M, m);   // gives (M', m') with idx = M'(M'+1)/2 + m', m' <= M'
+    M += 1;             // M(M-1)/2 = M'(M'+1)/2 with M = M'+1
+}
+
+inline int grid_for(int64_t total, int block) {
+    int64_t g = (total + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 148 * 64) g = 148 * 64;
+    return (int)g;
+}
+
+#define GRID_STRIDE(i, total) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (total); i += (int64_t)gridDim.x * blockDim.x)
+
+__global__ void build_tpm_kernel(const double *__restrict__ t2, double *__restrict__ tp, double *__restrict__ tm,
+                                 int64_t no, int64_t nv) {
+    const int64_t nop = no * (no + 1) / 2, nvp = nv * (nv + 1) / 2, nom = no * (no - 1) / 2;
+    GRID_STRIDE(idx, nop * nvp) {
+        int64_t ij = idx % nop, cd = idx / nop, i, j, c, d;
+        untri(ij, i, j);
+        untri(cd, c, d);
+        double a = t2[pk(c + nv * i, d + nv * j)];
+        double b = t2[pk(c + nv * j, d + nv * i)];
+        double f = (c == d ? 0.5 : 1.0) * (i == j ? 0.5 : 1.0);
+        tp[idx] = f * (a + b);
+        if (i > j && c > d) {
+            int64_t ijm = i * (i - 1) / 2 + j, cdm = c * (c - 1) / 2 + d;
+            tm[ijm + nom * cdm] = a - b;
+        }
+    }
+}
+
+// G[(c + nv*(a-a0)) + ldg*(d + nv*b)] = g_acbd for a in [a0,a1), b in [0,a1)
+__global__ void form_gpm_kernel(const double *__restrict__ G, int64_t ldg, double *__restrict__ gp,
+                                double *__restrict__ gm, int64_t nv, int64_t a0, int64_t a1) {
+    const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
+    const int64_t abp0 = a0 * (a0 + 1) / 2, nabp = a1 * (a1 + 1) / 2 - abp0;
+    const int64_t abm0 = a0 * (a0 - 1) / 2;
+    GRID_STRIDE(idx, nvp * nabp) {
+        int64_t cd = idx % nvp, loc = idx / nvp, a, b, c, d;
+        untri(abp0 + loc, a, b);
+        untri(cd, c, d);
+        double x = G[(c + nv * (a - a0)) + ldg * (d + nv * b)];
+        double y = G[(d + nv * (a - a0)) + ldg * (c + nv * b)];
+        gp[idx] = x + y;
+        if (a > b && c > d) {
+            int64_t cdm = c * (c - 1) / 2 + d, locm = a * (a - 1) / 2 + b - abm0;
+            gm[cdm + nvm * locm] = x - y;
+        }
+    }
+}
+
+__global__ void add_omega_pm_kernel(double *__restrict__ om2, const double *__restrict__ wp,
+                                    const double *__restrict__ wm, int64_t no, int64_t nv, int64_t a0, int64_t a1) {
+    const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
+    const int64_t abp0 = a0 * (a0 + 1) / 2, nabp = a1 * (a1 + 1) / 2 - abp0;
+    const int64_t abm0 = a0 * (a0 - 1) / 2;
+    GRID_STRIDE(idx, nop * nabp) {
+        int64_t ij = idx % nop, loc = idx / nop, i, j, a, b;
+        untri(ij, i, j);
+        untri(abp0 + loc, a, b);
+        double p = wp[idx] * (a == b ? 0.5 : 1.0);
+        double x1 = p, x2 = p;
+        if (i != j && a != b) {
+            int64_t ijm = i * (i - 1) / 2 + j, locm = a * (a - 1) / 2 + b - abm0;
+            double m = wm[ijm + nom * locm];
+            x1 = p + m;
+            x2 = p - m;
+        }
+        int64_t P1 = pk(a + nv * i, b + nv * j), P2 = pk(a + nv * j, b + nv * i);
+        if (P1 == P2) {
+            om2[P1] += x1 + x2;
+        } else {
+            om2[P1] += x1;
+            om2[P2] += x2;
+        }
+    }
+}
+
+// E_corr partial sums: sum_{ai,bj} (t_aibj + t_ai t_bj)(2 g_iajb - g_ibja), g (o,v,o,v)
+__global__ void energy_partial_kernel(const double *__restrict__ t1, const double *__restrict__ t2,
+                                      const double *__restrict__ g, int64_t no, int64_t nv,
+                                      double *__restrict__ partial) {
+    const int64_t nov = no * nv;
+    double acc = 0.0;
+    GRID_STRIDE(idx, nov * nov) {
+        int64_t ai = idx % nov, bj = idx / nov;
+        int64_t a = ai % nv, i = ai / nv, b = bj % nv, j = bj / nv;
+        double t = t2[pk(ai, bj)] + t1[ai] * t1[bj];
+        double g1 = g[i + no * (a + nv * (j + no * b))];
+        double g2 = g[i + no * (b + nv * (j + no * a))];
+        acc += t * (2.0 * g1 - g2);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double r = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = r;
+    }
+}
+
+__global__ void sum_partial_kernel(const double *__restrict__ partial, int n, double add, double *__restrict__ out) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double r = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+        if (threadIdx.x == 0) out[0] = r + add;
+    }
+}
+
+__global__ void orbital_differences_kernel(const double *__restrict__ eps, int64_t no, int64_t nv,
+                                           double *__restrict__ out) {
+    const int64_t nov = no * nv, nt2 = nov * (nov + 1) / 2;
+    GRID_STRIDE(k, nov + nt2) {
+        if (k < nov) {
+            int64_t a = k % nv, i = k / nv;
+            out[k] = eps[no + a] - eps[i];
+        } else {
+            int64_t M, m;
+            untri(k - nov, M, m);
+            int64_t a = M % nv, i = M / nv, b = m % nv, j = m / nv;
+            out[k] = eps[no + a] - eps[i] + eps[no + b] - eps[j];
+        }
+    }
+}
+
+// t2 = g_aibj / (e_i + e_j - e_a - e_b) with g (v,o,v,o) = sum_J L_ai L_bj
+__global__ void mp2_kernel(const double *__restrict__ g, const double *__restrict__ epsdiff, int64_t nov,
+                           double *__restrict__ t2) {
+    const int64_t nt2 = nov * (nov + 1) / 2;
+    GRID_STRIDE(k, nt2) {
+        int64_t M, m;
+        untri(k, M, m);
+        t2[k] = -g[m + nov * M] / epsdiff[nov + k];
+    }
+}
+
+// trace X_J = sum_k L[J,k,k] over an (nJ, no, no) block
+__global__ void trace_kernel(const double *__restrict__ L, int64_t nJ, int64_t no, double *__restrict__ X) {
+    GRID_STRIDE(J, nJ) {
+        double s = 0.0;
+        for (int64_t k = 0; k < no; k++) s += L[J + nJ * (k + no * k)];
+        X[J] = s;
+    }
+}
+
+__device__ __forceinline__ bool is_doubles_diag(int64_t k, int64_t nt1) {
+    if (k < nt1) return false;
+    int64_t M, m;
+    untri(k - nt1, M, m);
+    return M == m;
+}
+
+// residual <- -omega/eps; update = residual (doubles diagonal x2); t += update; residual diagonal x2
+__global__ void qn_update_kernel(double *__restrict__ omega, const double *__restrict__ epsdiff,
+                                 double *__restrict__ t, int64_t n, int64_t nt1) {
+    GRID_STRIDE(k, n) {
+        double r = -omega[k] / epsdiff[k];
+        if (is_doubles_diag(k, nt1)) r *= 2.0;
+        t[k] += r;
+        omega[k] = r;
+    }
+}
+
+__global__ void scale_doubles_diag_kernel(double *__restrict__ x, int64_t nov, int64_t nt1, double f) {
+    GRID_STRIDE(M, nov) {
+        x[nt1 + M * (M + 1) / 2 + M] *= f;
+    }
+}
+
+struct Ptr16 {
+    const double *p[16];
+    double w[16];
+};
+
+// x = sum_k w_k p_k  (weights read from device memory)
+__global__ void extrapolate_kernel(Ptr16 recs, const double *__restrict__ w, int nrec, int64_t n,
+                                   double *__restrict__ x) {
+    GRID_STRIDE(i, n) {
+        double s = 0.0;
+        for (int k = 0; k < nrec; k++) s += w[k] * recs.p[k][i];
+        x[i] = s;
+    }
+}
+
+// Insert the new dot products into the slot-indexed Gram matrix, build the padded DIIS
+// system in logical (oldest -> newest) order and solve it by Gaussian elimination with
+// partial pivoting (dgesv semantics).  Writes w[slot]; status[0] = 0 ok / 1 singular.
+__global__ void diis_solve_kernel(double *__restrict__ Gslot, int maxdim, const double *__restrict__ dots,
+                                  int new_slot, DiisOrder order, double *__restrict__ w, int *__restrict__ status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = order.n;
+    for (int k = 0; k < n; k++) {
+        int s = order.slot[k];
+        Gslot[new_slot * maxdim + s] = dots[s];
+        Gslot[s * maxdim + new_slot] = dots[s];
+    }
+    double A[17][18];
+    const int m = n + 1;
+    for (int r = 0; r < n; r++) {
+        for (int c = 0; c < n; c++) A[r][c] = Gslot[order.slot[r] * maxdim + order.slot[c]];
+        A[r][n] = -1.0;
+        A[r][m] = 0.0;
+    }
+    for (int c = 0; c < n; c++) A[n][c] = -1.0;
+    A[n][n] = 0.0;
+    A[n][m] = -1.0;
+    int st = 0;
+    for (int col = 0; col < m; col++) {
+        int piv = col;
+        double best = fabs(A[col][col]);
+        for (int r = col + 1; r < m; r++)
+            if (fabs(A[r][col]) > best) {
+                best = fabs(A[r][col]);
+                piv = r;
+            }
+        if (best == 0.0) {
+            st = 1;
+            break;
+        }
+        if (piv != col)
+            for (int c = 0; c <= m; c++) {
+                double tmp = A[col][c];
+                A[col][c] = A[piv][c];
+                A[piv][c] = tmp;
+            }
+        for (int r = col + 1; r < m; r++) {
+            double f = A[r][col] / A[col][col];
+            for (int c = col; c <= m; c++) A[r][c] -= f * A[col][c];
+        }
+    }
+    double x[17];
+    if (!st) {
+        for (int r = m - 1; r >= 0; r--) {
+            double s = A[r][m];
+            for (int c = r + 1; c < m; c++) s -= A[r][c] * x[c];
+            x[r] = s / A[r][r];
+        }
+        for (int k = 0; k < n; k++) w[k] = x[k];
+    }
+    status[0] = st;
+}
+
+}  // namespace
+
+void build_tpm(Exec &ex, const double *t2, double *tp, double *tm, int64_t no, int64_t nv) {
+    int64_t total = (no * (no + 1) / 2) * (nv * (nv + 1) / 2);
+    build_tpm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(t2, tp, tm, no, nv);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void form_gpm(Exec &ex, const double *G, int64_t ldg, double *gp, double *gm, int64_t nv, int64_t a0, int64_t a1) {
+    int64_t total = (nv * (nv + 1) / 2) * (a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2);
+    form_gpm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(G, ldg, gp, gm, nv, a0, a1);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int64_t no, int64_t nv, int64_t a0,
+                  int64_t a1) {
+    int64_t total = (no * (no + 1) / 2) * (a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2);
+    add_omega_pm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, wp, wm, no, nv, a0, a1);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void energy_reduce(Exec &ex, const double *t1, const double *t2, const double *g_ovov, int64_t no, int64_t nv,
+                   double add, double *d_out) {
+    const int nb = 592;
+    DBuf part = dalloc(nb, ex.stream);
+    energy_partial_kernel<<<nb, 256, 0, ex.stream>>>(t1, t2, g_ovov, no, nv, part.d());
+    sum_partial_kernel<<<1, 256, 0, ex.stream>>>(part.d(), nb, add, d_out);
+    ex.launches += 2;
+    CU_CHECK(cudaGetLastError());
+}
+
+void orbital_differences(Exec &ex, const double *eps, int64_t no, int64_t nv, double *out) {
+    int64_t nov = no * nv, total = nov + nov * (nov + 1) / 2;
+    orbital_differences_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(eps, no, nv, out);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void mp2_amplitudes(Exec &ex, const double *g_vovo, const double *epsdiff, int64_t nov, double *t2) {
+    mp2_kernel<<<grid_for(nov * (nov + 1) / 2, 256), 256, 0, ex.stream>>>(g_vovo, epsdiff, nov, t2);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void trace_oo(Exec &ex, const double *L_oo, int64_t nJ, int64_t no, double *X) {
+    trace_kernel<<<grid_for(nJ, 128), 128, 0, ex.stream>>>(L_oo, nJ, no, X);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void qn_update(Exec &ex, double *omega, const double *epsdiff, double *t, int64_t n, int64_t nt1) {
+    qn_update_kernel<<<grid_for(n, 256), 256, 0, ex.stream>>>(omega, epsdiff, t, n, nt1);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void scale_doubles_diag(Exec &ex, double *x, int64_t nov, int64_t nt1, double f) {
+    scale_doubles_diag_kernel<<<grid_for(nov, 256), 256, 0, ex.stream>>>(x, nov, nt1, f);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void diis_solve(Exec &ex, double *Gslot, int maxdim, const double *dots, int new_slot, const DiisOrder &order,
+                double *w, int *status) {
+    diis_solve_kernel<<<1, 32, 0, ex.stream>>>(Gslot, maxdim, dots, new_slot, order, w, status);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void extrapolate(Exec &ex, const double *const *recs, const double *w, int nrec, int64_t n, double *x) {
+    Ptr16 p{};
+    for (int k = 0; k < nrec; k++) p.p[k] = recs[k];
+    extrapolate_kernel<<<grid_for(n, 256), 256, 0, ex.stream>>>(p, w, nrec, n, x);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+}  // namespace ccsd

@@ -1,0 +1,33 @@
+// Bandwidth kernels of the CCSD path (declarations).
+#pragma once
+
+#include "common.cuh"
+
+namespace ccsd {
+
+struct DiisOrder {
+    int n;          // active records
+    int slot[16];   // record slots, oldest first
+};
+
+// t+ (n_o_p x n_v_p) and t- (n_o_m x n_v_m) of the A2 ladder (construct_plus_minus_2413_from_packed
+// followed by scale_double_packed_blocks(1/2, 1/2); packed_array_utilities_r.F90:140-197, 99-136)
+void build_tpm(Exec &ex, const double *t2, double *tp, double *tm, int64_t no, int64_t nv);
+// g+- columns for the pairs a in [a0,a1), b <= a from G = g_acbd (construct_plus_minus_1324_from_full)
+void form_gpm(Exec &ex, const double *G, int64_t ldg, double *gp, double *gm, int64_t nv, int64_t a0, int64_t a1);
+// add_double/single_packed_plus_minus with the omega+ (a == b) half scaling
+void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int64_t no, int64_t nv, int64_t a0,
+                  int64_t a1);
+
+void energy_reduce(Exec &ex, const double *t1, const double *t2, const double *g_ovov, int64_t no, int64_t nv,
+                   double add, double *d_out);
+void orbital_differences(Exec &ex, const double *eps, int64_t no, int64_t nv, double *out);
+void mp2_amplitudes(Exec &ex, const double *g_vovo, const double *epsdiff, int64_t nov, double *t2);
+void trace_oo(Exec &ex, const double *L_oo, int64_t nJ, int64_t no, double *X);
+void qn_update(Exec &ex, double *omega, const double *epsdiff, double *t, int64_t n, int64_t nt1);
+void scale_doubles_diag(Exec &ex, double *x, int64_t nov, int64_t nt1, double f);
+void diis_solve(Exec &ex, double *Gslot, int maxdim, const double *dots, int new_slot, const DiisOrder &order,
+                double *w, int *status);
+void extrapolate(Exec &ex, const double *const *recs, const double *w, int nrec, int64_t n, double *x);
+
+}  // namespace ccsd

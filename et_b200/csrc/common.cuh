@@ -1,0 +1,127 @@
+// Shared infrastructure of libccsd_gpu: errors, device buffers, tensor views.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ccsd_gpu.h"
+
+namespace ccsd {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CU_CHECK(x)                                                                        \
+    do {                                                                                   \
+        cudaError_t err__ = (x);                                                           \
+        if (err__ != cudaSuccess) {                                                        \
+            int code__ = (err__ == cudaErrorMemoryAllocation) ? CCSD_GPU_ENOMEM : CCSD_GPU_ECUDA; \
+            throw ::ccsd::Error(code__, std::string(#x) + ": " + cudaGetErrorString(err__) + \
+                                " (" __FILE__ ":" + std::to_string(__LINE__) + ")");       \
+        }                                                                                  \
+    } while (0)
+
+#define BLAS_CHECK(x)                                                                      \
+    do {                                                                                   \
+        cublasStatus_t st__ = (x);                                                         \
+        if (st__ != CUBLAS_STATUS_SUCCESS)                                                 \
+            throw ::ccsd::Error(CCSD_GPU_ECUDA, std::string(#x) + ": cublas status " +     \
+                                std::to_string((int)st__) + " (" __FILE__ ":" +           \
+                                std::to_string(__LINE__) + ")");                           \
+    } while (0)
+
+#define REQUIRE(cond, code, msg)                                                           \
+    do {                                                                                   \
+        if (!(cond)) throw ::ccsd::Error(code, msg);                                       \
+    } while (0)
+
+// Stream-ordered device buffer (cudaMallocAsync from the device's default pool).
+class DBuf {
+  public:
+    DBuf() = default;
+    DBuf(size_t bytes, cudaStream_t s) { alloc(bytes, s); }
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    DBuf(DBuf &&o) noexcept { *this = std::move(o); }
+    DBuf &operator=(DBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            p_ = o.p_;
+            bytes_ = o.bytes_;
+            s_ = o.s_;
+            o.p_ = nullptr;
+            o.bytes_ = 0;
+        }
+        return *this;
+    }
+    ~DBuf() { release(); }
+    void alloc(size_t bytes, cudaStream_t s) {
+        release();
+        s_ = s;
+        bytes_ = bytes;
+        if (bytes) CU_CHECK(cudaMallocAsync(&p_, bytes, s));
+    }
+    void release() noexcept {
+        if (p_) cudaFreeAsync(p_, s_);
+        p_ = nullptr;
+        bytes_ = 0;
+    }
+    template <class T = double> T *as() const { return static_cast<T *>(p_); }
+    double *d() const { return static_cast<double *>(p_); }
+    size_t bytes() const { return bytes_; }
+    explicit operator bool() const { return p_ != nullptr; }
+
+  private:
+    void *p_ = nullptr;
+    size_t bytes_ = 0;
+    cudaStream_t s_ = nullptr;
+};
+
+inline DBuf dalloc(int64_t n, cudaStream_t s) { return DBuf(size_t(n) * sizeof(double), s); }
+
+// A strided view of up to 6 dimensions (element strides, column-major by default).
+struct TV {
+    double *p = nullptr;
+    int nd = 0;
+    int64_t n[6] = {0, 0, 0, 0, 0, 0};
+    int64_t s[6] = {0, 0, 0, 0, 0, 0};
+    int64_t size() const {
+        int64_t t = 1;
+        for (int k = 0; k < nd; k++) t *= n[k];
+        return t;
+    }
+};
+
+inline TV tv(const double *p, std::initializer_list<int64_t> dims) {
+    TV v;
+    v.p = const_cast<double *>(p);
+    int64_t st = 1;
+    for (int64_t d : dims) {
+        v.n[v.nd] = d;
+        v.s[v.nd] = st;
+        st *= d;
+        v.nd++;
+    }
+    return v;
+}
+
+enum class Prec { FP64, MIXED };
+
+// Execution environment handed to the tensor kernels.
+struct Exec {
+    cudaStream_t stream = nullptr;
+    cublasHandle_t blas = nullptr;
+    Prec prec = Prec::FP64;
+    double mixed_min_flops = 2e9;
+    double flops = 0.0;          // algorithmic flops issued (counted by contract())
+    int64_t launches = 0;        // kernels of this library launched
+};
+
+}  // namespace ccsd

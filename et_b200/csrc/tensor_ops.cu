@@ -1,0 +1,475 @@
+// Tensor primitives: strided permutations (smem-tiled when the fastest index changes),
+// GEMM-backed contractions, packed-doubles conversions and deterministic reductions.
+#include <algorithm>
+#include <cstring>
+#include <map>
+
+#include "mixed_gemm.cuh"
+#include "tensor_ops.cuh"
+
+namespace ccsd {
+
+namespace {
+
+constexpr int MAXD = 6;
+
+struct PermArgs {
+    int nd;
+    int64_t n[MAXD];
+    int64_t si[MAXD];
+    int64_t so[MAXD];
+};
+
+// One output element per thread; dims are ordered by output stride (dim 0 fastest).
+__global__ void permute_simple_kernel(PermArgs a, int64_t total, double alpha, const double *__restrict__ in,
+                                      double beta, double *__restrict__ out) {
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = idx, oi = 0, oo = 0;
+#pragma unroll
+        for (int d = 0; d < MAXD; d++) {
+            if (d < a.nd) {
+                int64_t q = r / a.n[d];
+                int64_t i = r - q * a.n[d];
+                r = q;
+                oi += i * a.si[d];
+                oo += i * a.so[d];
+            }
+        }
+        double v = alpha * in[oi];
+        if (beta != 0.0) v += beta * out[oo];
+        out[oo] = v;
+    }
+}
+
+// 32x32 tile over (p = input-fastest dim, q = output-fastest dim); the remaining dims
+// are flattened into the z loop.  Dims 2.. of `a` are the batch dims.
+__global__ void permute_tiled_kernel(PermArgs a, int64_t nbatch, double alpha, const double *__restrict__ in,
+                                     double beta, double *__restrict__ out) {
+    __shared__ double tile[32][33];
+    const int64_t np = a.n[0], nq = a.n[1];
+    const int64_t p0 = (int64_t)blockIdx.x * 32, q0 = (int64_t)blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int64_t b = blockIdx.z; b < nbatch; b += gridDim.z) {
+        int64_t r = b, bi = 0, bo = 0;
+        for (int d = 2; d < a.nd; d++) {
+            int64_t q = r / a.n[d];
+            int64_t i = r - q * a.n[d];
+            r = q;
+            bi += i * a.si[d];
+            bo += i * a.so[d];
+        }
+        for (int k = ty; k < 32; k += 8) {
+            int64_t p = p0 + tx, q = q0 + k;
+            if (p < np && q < nq) tile[k][tx] = in[bi + p * a.si[0] + q * a.si[1]];
+        }
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            int64_t q = q0 + tx, p = p0 + k;
+            if (p < np && q < nq) {
+                int64_t o = bo + p * a.so[0] + q * a.so[1];
+                double v = alpha * tile[tx][k];
+                if (beta != 0.0) v += beta * out[o];
+                out[o] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+int grid_for(int64_t total, int block) {
+    int64_t g = (total + block - 1) / block;
+    return (int)std::min<int64_t>(std::max<int64_t>(g, 1), 148 * 32);
+}
+
+}  // namespace
+
+void permute_add(Exec &ex, double alpha, const TV &in, double beta, const TV &out) {
+    REQUIRE(in.nd == out.nd, CCSD_GPU_EINVAL, "permute_add: rank mismatch");
+    // drop unit dims
+    std::vector<int> dims;
+    for (int d = 0; d < in.nd; d++) {
+        REQUIRE(in.n[d] == out.n[d], CCSD_GPU_EINVAL, "permute_add: extent mismatch");
+        if (in.n[d] > 1) dims.push_back(d);
+    }
+    int64_t total = in.size();
+    if (total == 0) return;
+    PermArgs a{};
+    if (dims.empty()) dims.push_back(0);
+    // order by output stride
+    std::sort(dims.begin(), dims.end(), [&](int x, int y) { return out.s[x] < out.s[y]; });
+    int q = dims[0];                                       // output-fastest
+    int p = *std::min_element(dims.begin(), dims.end(), [&](int x, int y) { return in.s[x] < in.s[y]; });
+    if (p != q && in.n[p] >= 8 && in.n[q] >= 8) {
+        a.nd = (int)dims.size();
+        a.n[0] = in.n[p];
+        a.si[0] = in.s[p];
+        a.so[0] = out.s[p];
+        a.n[1] = in.n[q];
+        a.si[1] = in.s[q];
+        a.so[1] = out.s[q];
+        int k = 2;
+        int64_t nb = 1;
+        for (int d : dims)
+            if (d != p && d != q) {
+                a.n[k] = in.n[d];
+                a.si[k] = in.s[d];
+                a.so[k] = out.s[d];
+                nb *= in.n[d];
+                k++;
+            }
+        dim3 grid((unsigned)((a.n[0] + 31) / 32), (unsigned)((a.n[1] + 31) / 32),
+                  (unsigned)std::min<int64_t>(nb, 65535));
+        permute_tiled_kernel<<<grid, dim3(32, 8), 0, ex.stream>>>(a, nb, alpha, in.p, beta, out.p);
+    } else {
+        a.nd = (int)dims.size();
+        for (size_t k = 0; k < dims.size(); k++) {
+            a.n[k] = in.n[dims[k]];
+            a.si[k] = in.s[dims[k]];
+            a.so[k] = out.s[dims[k]];
+        }
+        permute_simple_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(a, total, alpha, in.p, beta, out.p);
+    }
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// GEMM dispatch
+// ---------------------------------------------------------------------------
+
+void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
+          int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, bool allow_mixed) {
+    if (m == 0 || n == 0) return;
+    double fl = 2.0 * double(m) * double(n) * double(k);
+    ex.flops += fl;
+    if (allow_mixed && ex.prec == Prec::MIXED && fl >= ex.mixed_min_flops && k >= 16) {
+        mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        return;
+    }
+    BLAS_CHECK(cublasDgemm_64(ex.blas, transA ? CUBLAS_OP_T : CUBLAS_OP_N, transB ? CUBLAS_OP_T : CUBLAS_OP_N, m,
+                              n, k, &alpha, A, lda, B, ldb, &beta, C, ldc));
+}
+
+// ---------------------------------------------------------------------------
+// contract()
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct LabelInfo {
+    int64_t n = 1;
+    int dA = -1, dB = -1, dC = -1;
+};
+
+// Is `v` (dims given by `order1` then `order2`) a column-major matrix [group1][group2]?
+// Returns the leading dimension in *ld.
+bool groupable(const TV &v, const std::vector<int> &g1, const std::vector<int> &g2, int64_t *ld) {
+    int64_t expect = 1;
+    for (int d : g1) {
+        if (v.n[d] == 1) continue;
+        if (v.s[d] != expect) return false;
+        expect *= v.n[d];
+    }
+    int64_t lead = -1, exp2 = -1;
+    for (int d : g2) {
+        if (v.n[d] == 1) continue;
+        if (lead < 0) {
+            lead = v.s[d];
+            if (lead < expect) return false;
+            exp2 = lead * v.n[d];
+        } else {
+            if (v.s[d] != exp2) return false;
+            exp2 *= v.n[d];
+        }
+    }
+    *ld = lead < 0 ? std::max<int64_t>(expect, 1) : lead;
+    return true;
+}
+
+std::vector<char> natural_order(const TV &v, const std::vector<char> &labels, const std::map<char, LabelInfo> &info,
+                                int which) {
+    std::vector<char> out = labels;
+    std::stable_sort(out.begin(), out.end(), [&](char x, char y) {
+        const LabelInfo &a = info.at(x), &b = info.at(y);
+        int da = which == 0 ? a.dA : which == 1 ? a.dB : a.dC;
+        int db = which == 0 ? b.dA : which == 1 ? b.dB : b.dC;
+        return v.s[da] < v.s[db];
+    });
+    return out;
+}
+
+std::vector<int> dims_of(const std::vector<char> &labels, const std::map<char, LabelInfo> &info, int which) {
+    std::vector<int> d;
+    for (char c : labels) {
+        const LabelInfo &li = info.at(c);
+        d.push_back(which == 0 ? li.dA : which == 1 ? li.dB : li.dC);
+    }
+    return d;
+}
+
+int64_t prod(const std::vector<char> &labels, const std::map<char, LabelInfo> &info) {
+    int64_t p = 1;
+    for (char c : labels) p *= info.at(c).n;
+    return p;
+}
+
+// Contiguous copy of v with dims reordered as [g1 labels][g2 labels].
+TV make_contiguous(Exec &ex, const TV &v, const std::vector<int> &g1, const std::vector<int> &g2, DBuf &buf) {
+    buf = dalloc(v.size(), ex.stream);
+    TV dst;
+    dst.p = buf.d();
+    dst.nd = v.nd;
+    int64_t st = 1;
+    for (int k = 0; k < v.nd; k++) dst.n[k] = v.n[k];
+    for (int d : g1) {
+        dst.s[d] = st;
+        st *= v.n[d];
+    }
+    for (int d : g2) {
+        dst.s[d] = st;
+        st *= v.n[d];
+    }
+    permute_add(ex, 1.0, v, 0.0, dst);
+    return dst;
+}
+
+}  // namespace
+
+void contract(Exec &ex, const char *spec, double alpha, const TV &A, const TV &B, double beta, const TV &C) {
+    std::string s(spec);
+    size_t comma = s.find(','), arrow = s.find("->");
+    REQUIRE(comma != std::string::npos && arrow != std::string::npos, CCSD_GPU_EINVAL, "contract: bad spec");
+    std::string la = s.substr(0, comma), lb = s.substr(comma + 1, arrow - comma - 1), lc = s.substr(arrow + 2);
+    REQUIRE((int)la.size() == A.nd && (int)lb.size() == B.nd && (int)lc.size() == C.nd, CCSD_GPU_EINVAL,
+            std::string("contract: rank mismatch in ") + spec);
+    std::map<char, LabelInfo> info;
+    for (int d = 0; d < A.nd; d++) {
+        info[la[d]].dA = d;
+        info[la[d]].n = A.n[d];
+    }
+    for (int d = 0; d < B.nd; d++) {
+        auto &li = info[lb[d]];
+        REQUIRE(li.dA < 0 || li.n == B.n[d], CCSD_GPU_EINVAL, std::string("contract: extent mismatch in ") + spec);
+        li.dB = d;
+        li.n = B.n[d];
+    }
+    for (int d = 0; d < C.nd; d++) {
+        auto &li = info[lc[d]];
+        REQUIRE(li.dA >= 0 || li.dB >= 0, CCSD_GPU_EINVAL, std::string("contract: free output label in ") + spec);
+        REQUIRE(li.n == C.n[d], CCSD_GPU_EINVAL, std::string("contract: output extent mismatch in ") + spec);
+        li.dC = d;
+    }
+    std::vector<char> K, M, N;
+    for (auto &kv : info) {
+        const LabelInfo &li = kv.second;
+        int cnt = (li.dA >= 0) + (li.dB >= 0) + (li.dC >= 0);
+        REQUIRE(cnt == 2, CCSD_GPU_EINVAL, std::string("contract: label must appear exactly twice in ") + spec);
+        if (li.dA >= 0 && li.dB >= 0) K.push_back(kv.first);
+        else if (li.dA >= 0) M.push_back(kv.first);
+        else N.push_back(kv.first);
+    }
+    const int64_t mK = prod(K, info), mM = prod(M, info), mN = prod(N, info);
+    if (mM == 0 || mN == 0) return;
+
+    // label orders: M/N from C where possible, K from A
+    std::vector<char> oM = natural_order(C, M, info, 2), oN = natural_order(C, N, info, 2);
+    std::vector<char> oK = natural_order(A, K, info, 0);
+    {
+        std::vector<char> bK = natural_order(B, K, info, 1);
+        int64_t ld;
+        // prefer B's K order when B is the bigger operand and already groupable with it
+        if (B.size() > A.size() && (groupable(B, dims_of(bK, info, 1), dims_of(oN, info, 1), &ld) ||
+                                    groupable(B, dims_of(oN, info, 1), dims_of(bK, info, 1), &ld)))
+            oK = bK;
+    }
+    DBuf bufA, bufB, bufC;
+    TV Au = A, Bu = B;
+    bool tA, tB;
+    int64_t lda, ldb, ldc;
+    {
+        auto dK = dims_of(oK, info, 0), dM = dims_of(oM, info, 0);
+        if (groupable(A, dM, dK, &lda)) tA = false;
+        else if (groupable(A, dK, dM, &lda)) tA = true;
+        else {
+            Au = make_contiguous(ex, A, dK, dM, bufA);
+            tA = true;
+            lda = std::max<int64_t>(mK, 1);
+        }
+    }
+    {
+        auto dK = dims_of(oK, info, 1), dN = dims_of(oN, info, 1);
+        if (groupable(B, dK, dN, &ldb)) tB = false;
+        else if (groupable(B, dN, dK, &ldb)) tB = true;
+        else {
+            Bu = make_contiguous(ex, B, dK, dN, bufB);
+            tB = false;
+            ldb = std::max<int64_t>(mK, 1);
+        }
+    }
+    auto cM = dims_of(oM, info, 2), cN = dims_of(oN, info, 2);
+    if (groupable(C, cM, cN, &ldc)) {
+        gemm(ex, tA, tB, mM, mN, mK, alpha, Au.p, lda, Bu.p, ldb, beta, C.p, ldc);
+    } else if (groupable(C, cN, cM, &ldc)) {
+        gemm(ex, !tB, !tA, mN, mM, mK, alpha, Bu.p, ldb, Au.p, lda, beta, C.p, ldc);
+    } else {
+        bufC = dalloc(mM * mN, ex.stream);
+        gemm(ex, tA, tB, mM, mN, mK, alpha, Au.p, lda, Bu.p, ldb, 0.0, bufC.d(), mM);
+        TV t;
+        t.p = bufC.d();
+        t.nd = C.nd;
+        int64_t st = 1;
+        for (int k = 0; k < C.nd; k++) t.n[k] = C.n[k];
+        for (int d : cM) {
+            t.s[d] = st;
+            st *= C.n[d];
+        }
+        for (int d : cN) {
+            t.s[d] = st;
+            st *= C.n[d];
+        }
+        permute_add(ex, 1.0, t, beta, C);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// packing
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int64_t pk(int64_t x, int64_t y) {
+    int64_t M = x > y ? x : y, m = x > y ? y : x;
+    return M * (M + 1) / 2 + m;
+}
+
+__global__ void squareup_kernel(const double *__restrict__ packed, double *__restrict__ full, int64_t nov) {
+    int64_t total = nov * nov;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = idx % nov, c = idx / nov;
+        full[idx] = packed[pk(r, c)];
+    }
+}
+
+void squareup(Exec &ex, const double *packed, double *full, int64_t nov) {
+    squareup_kernel<<<grid_for(nov * nov, 256), 256, 0, ex.stream>>>(packed, full, nov);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+// one thread per packed element; element (M, m) with M >= m reads full(m, M) = full[m + nov*M]
+__global__ void pack_half_diag_add_kernel(double alpha, const double *__restrict__ full, double *__restrict__ packed,
+                                          int64_t nov) {
+    int64_t total = nov * (nov + 1) / 2;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int64_t M = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+        while (M * (M + 1) / 2 > idx) M--;
+        while ((M + 1) * (M + 2) / 2 <= idx) M++;
+        int64_t m = idx - M * (M + 1) / 2;
+        double v = full[m + nov * M];
+        if (m == M) v *= 0.5;
+        packed[idx] += alpha * v;
+    }
+}
+
+void pack_half_diag_add(Exec &ex, double alpha, const double *full, double *packed, int64_t nov) {
+    pack_half_diag_add_kernel<<<grid_for(nov * (nov + 1) / 2, 256), 256, 0, ex.stream>>>(alpha, full, packed, nov);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr int RBLOCKS = 592;   // 4 x 148 SMs
+constexpr int RTHREADS = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ double block_sum(double v) {
+    __shared__ double sh[32];
+    v = warp_sum(v);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < (blockDim.x + 31) / 32 ? sh[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+struct PtrList {
+    const double *p[16];
+};
+
+__global__ void multi_dot_partial(const double *__restrict__ x, PtrList ys, int nys, int64_t n,
+                                  double *__restrict__ partial) {
+    for (int k = 0; k < nys; k++) {
+        const double *y = ys.p[k];
+        double acc = 0.0;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            acc += x[i] * y[i];
+        acc = block_sum(acc);
+        if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = acc;
+    }
+}
+
+__global__ void finish_partial(const double *__restrict__ partial, int nblocks, int nys, double *__restrict__ out) {
+    int k = blockIdx.x;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) acc += partial[k * nblocks + i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) out[k] = acc;
+}
+
+__global__ void fill_kernel(double *p, int64_t n, double v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+__global__ void axpby_kernel(int64_t n, double a, const double *__restrict__ x, double b, double *__restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = a * x[i] + (b == 0.0 ? 0.0 : b * y[i]);
+}
+}  // namespace
+
+void multi_dot(Exec &ex, const double *x, const double *const *ys, int nys, int64_t n, double *d_results) {
+    if (nys == 0) return;
+    REQUIRE(nys <= 16, CCSD_GPU_EINVAL, "multi_dot: at most 16 vectors");
+    PtrList pl{};
+    for (int k = 0; k < nys; k++) pl.p[k] = ys[k];
+    DBuf part = dalloc((int64_t)RBLOCKS * nys, ex.stream);
+    multi_dot_partial<<<RBLOCKS, RTHREADS, 0, ex.stream>>>(x, pl, nys, n, part.d());
+    finish_partial<<<nys, RTHREADS, 0, ex.stream>>>(part.d(), RBLOCKS, nys, d_results);
+    ex.launches += 2;
+    CU_CHECK(cudaGetLastError());
+}
+
+void dot(Exec &ex, const double *x, const double *y, int64_t n, double *d_result) {
+    const double *ys[1] = {y};
+    multi_dot(ex, x, ys, 1, n, d_result);
+}
+
+void fill(Exec &ex, double *p, int64_t n, double value) {
+    if (n == 0) return;
+    fill_kernel<<<grid_for(n, 256), 256, 0, ex.stream>>>(p, n, value);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void axpby(Exec &ex, int64_t n, double alpha, const double *x, double beta, double *y) {
+    if (n == 0) return;
+    axpby_kernel<<<grid_for(n, 256), 256, 0, ex.stream>>>(n, alpha, x, beta, y);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+}  // namespace ccsd

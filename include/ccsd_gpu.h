@@ -1,0 +1,136 @@
+/*
+ * ccsd_gpu.h - C ABI of the B200 (sm_100a) CCSD hot path.
+ *
+ * The entry points replace the bodies of eT's type-bound procedures on
+ * class(ccsd) (paths relative to the eT source tree).  eT's Fortran binds
+ * them through an ISO_C_BINDING interface block in the style of
+ * src/libint/eri_cdef.F90:25-68 (bind(C), value scalars, real(c_double)
+ * arrays); see INTEGRATION.md for the interface block and the shim.
+ *
+ * Conventions (identical to eT):
+ *  - every array is column-major double precision and owned by the caller;
+ *  - integers are int64_t (eT builds with 64-bit default integers,
+ *    CMakeLists.txt:38);
+ *  - singles are (n_v, n_o) with ai = a + n_v*i; doubles are upper-packed over
+ *    (ai, bj), index max(ai,bj)*(max(ai,bj)+1)/2 + min(ai,bj) (0-based form of
+ *    src/tools/reordering.F90:4174-4198); an amplitude-like vector is
+ *    [singles (n_t1) | packed doubles (n_t2)], n_t1 = n_o*n_v,
+ *    n_t2 = n_t1*(n_t1+1)/2;
+ *  - Cholesky vectors are L[J, p, q] with J fastest over the full MO range
+ *    (occupied first): g_pqrs = sum_J L^J_pq L^J_rs
+ *    (src/eri_tool/eri_tool_class.F90:92-163).
+ *
+ * Every function returns 0 on success or a negative CCSD_GPU_E* status;
+ * ccsd_gpu_last_error() returns a message for the last failure on a context.
+ * A context owns one CUDA stream; calls on one context must come from one
+ * host thread at a time.  Distinct contexts are independent.
+ */
+#ifndef CCSD_GPU_H
+#define CCSD_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CCSD_GPU_OK = 0,
+    CCSD_GPU_EINVAL = -1,        /* bad dimensions / arguments */
+    CCSD_GPU_ECUDA = -2,         /* CUDA runtime or cuBLAS error */
+    CCSD_GPU_ENOMEM = -3,        /* device allocation failed */
+    CCSD_GPU_ESTATE = -4,        /* required input not set yet */
+    CCSD_GPU_ENOCONV = -5,       /* solver did not converge */
+    CCSD_GPU_ENAN = -6,          /* non-finite value detected */
+    CCSD_GPU_ESINGULAR = -7,     /* DIIS / reduced-space system singular */
+    CCSD_GPU_ENODEV = -8         /* no sm_100 device available */
+};
+
+/* arithmetic used by the contractions */
+enum {
+    CCSD_GPU_FP64 = 0,           /* FP64 everywhere (DGEMM on the FP64 tensor pipe) */
+    CCSD_GPU_MIXED = 1           /* large contractions as split-BF16 (3 products) tcgen05 GEMMs,
+                                    FP32 accumulation; everything else FP64 */
+};
+
+typedef struct ccsd_gpu_options {
+    int32_t device;              /* CUDA ordinal */
+    int32_t precision;           /* CCSD_GPU_FP64 or CCSD_GPU_MIXED */
+    int64_t ladder_batch;        /* virtual-index batch of the A2 ladder, 0 = automatic */
+    int64_t mixed_min_flops;     /* contractions below this many flops stay FP64 (0 = default) */
+    int64_t reserved[5];
+} ccsd_gpu_options;
+
+typedef struct ccsd_gpu_solver_options {
+    int32_t max_iterations;      /* diis_cc_gs default 100 (src/solvers/cc/diis_cc_gs_class.F90:139) */
+    int32_t diis_dimension;      /* default 8 */
+    double omega_threshold;      /* |Omega| convergence threshold */
+    double energy_threshold;     /* |dE| convergence threshold (< 0 disables the energy test) */
+    double refine_threshold;     /* MIXED only: |Omega| at which Omega switches to FP64 */
+    int32_t reserved[8];
+} ccsd_gpu_solver_options;
+
+/* Creation / teardown.  Replaces the wavefunction set-up that allocates t, Omega and the
+ * Cholesky storage (src/wavefunctions/ccsd/ccsd_class.F90, src/eri_tool/eri_cholesky_memory_class.F90). */
+int  ccsd_gpu_create(int64_t n_o, int64_t n_v, int64_t n_J, const ccsd_gpu_options *opt, void **ctx);
+void ccsd_gpu_destroy(void *ctx);
+const char *ccsd_gpu_last_error(void *ctx);
+int  ccsd_gpu_set_precision(void *ctx, int32_t precision);
+/* Run the context's work on a caller-provided stream (a cudaStream_t passed as void*);
+ * NULL restores the context's own stream. */
+int  ccsd_gpu_set_stream(void *ctx, void *stream);
+int  ccsd_gpu_synchronize(void *ctx);
+
+/* MO Cholesky vectors L[J,p,q] over the full MO range (wf%L_mo, set in
+ * src/engines/cc/tasks/cholesky_decomposition_task_class.F90:68-138). */
+int ccsd_gpu_set_cholesky_mo(void *ctx, const double *L);
+/* Same data in eT's four o/v blocks, each (n_J, len_p, len_q)
+ * (src/eri_tool/abstract_eri_cholesky_class.F90:290-327). */
+int ccsd_gpu_set_cholesky_mo_blocks(void *ctx, const double *L_oo, const double *L_ov,
+                                    const double *L_vo, const double *L_vv);
+/* MO one-electron Hamiltonian h (n_mo x n_mo), orbital energies (n_mo) and E_HF
+ * (get_t1_oei, src/wavefunctions/ccs/oei_ccs.F90:35-95; wf%orbital_energies; wf%hf_energy). */
+int ccsd_gpu_set_h_mo(void *ctx, const double *h, const double *eps, double e_hf);
+
+/* set_amplitudes + construct_t1_cholesky (src/wavefunctions/ccs/t1_ccs.F90:208-499)
+ * + construct_fock (src/wavefunctions/ccsd/fock_ccsd.F90:34-78). */
+int ccsd_gpu_set_amplitudes(void *ctx, const double *t);
+int ccsd_gpu_get_amplitudes(void *ctx, double *t);
+/* set_initial_amplitudes_guess without restart: t1 = 0, t2 = MP2 guess
+ * (src/wavefunctions/ccsd/ccsd_class.F90:357-410, 478-533). */
+int ccsd_gpu_mp2_guess(void *ctx);
+/* T1 Fock matrix F (n_mo x n_mo) at the current amplitudes (wf%fock_ij/ia/ai/ab). */
+int ccsd_gpu_get_fock(void *ctx, double *F);
+
+/* calculate_energy (src/wavefunctions/ccsd/mean_value_ccsd.F90:36-99). */
+int ccsd_gpu_energy(void *ctx, double *energy);
+/* construct_omega (src/wavefunctions/ccsd/omega_ccsd.F90:39-110): omega has n_t1 + n_t2 entries. */
+int ccsd_gpu_omega(void *ctx, double *omega);
+/* Same with device pointers (output stays in HBM). */
+int ccsd_gpu_omega_device(void *ctx, double *d_omega);
+
+/* jacobian_transformation (src/wavefunctions/ccsd/jacobian_ccsd.F90:74-176):
+ * rho_k = A c_k for n_vec column vectors (column-major (n_t1+n_t2, n_vec)). */
+int ccsd_gpu_jacobian(void *ctx, int64_t n_vec, const double *c, double *rho);
+/* jacobian_transpose_transformation (src/wavefunctions/ccsd/jacobian_transpose_ccsd.F90:129-235):
+ * sigma_k = b_k^T A. */
+int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, double *sigma);
+
+/* run_diis_cc_gs (src/solvers/cc/diis_cc_gs_class.F90:209-315) with the quasi-Newton updater,
+ * entirely on the device.  On exit the context holds the final amplitudes; history (nullable)
+ * receives max_iterations pairs (E, |Omega|). */
+int ccsd_gpu_solve_gs(void *ctx, const ccsd_gpu_solver_options *opt, double *energy,
+                      int32_t *iterations, double *history);
+
+/* Counters since creation: kernels of this library launched and GEMM flops issued. */
+int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops);
+
+/* Algorithmic flop count of one Omega at this context's dimensions, summed over eT's own BLAS
+ * call sites (2mnk per DGEMM, n(n+1)k per DSFRK). */
+double ccsd_gpu_omega_flops(void *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCSD_GPU_H */
