@@ -77,6 +77,9 @@ SIGNATURES = {
     "ccsd_gpu_solve_gs": (ctypes.c_int, [_VP, ctypes.POINTER(SolverOptions), _DP,
                                          ctypes.POINTER(ctypes.c_int32), _DP]),
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
+    "ccsd_gpu_selftest_gemm": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I64, _I64,
+                                              _I64, ctypes.c_double, _DP, _I64, _DP, _I64, ctypes.c_double, _DP,
+                                              _I64]),
     "ccsd_gpu_omega_flops": (ctypes.c_double, [_VP]),
 }
 
@@ -242,6 +245,19 @@ class CCSD:
         f = ctypes.c_double()
         self._check(self.lib.ccsd_gpu_stats(self.ctx, ctypes.byref(n), ctypes.byref(f)))
         return n.value, f.value
+
+    def selftest_gemm(self, A, B, C=None, *, alpha=1.0, beta=0.0, transA=False, transB=False, mixed=True):
+        """C = alpha op(A) op(B) + beta C on the device (diagnostics of the GEMM back ends)."""
+        A = np.asfortranarray(A, dtype=np.float64)
+        B = np.asfortranarray(B, dtype=np.float64)
+        m = A.shape[1] if transA else A.shape[0]
+        k = A.shape[0] if transA else A.shape[1]
+        n = B.shape[0] if transB else B.shape[1]
+        Cf = np.asfortranarray(np.zeros((m, n)) if C is None else C, dtype=np.float64).copy(order="F")
+        self._check(self.lib.ccsd_gpu_selftest_gemm(
+            self.ctx, int(mixed), int(transA), int(transB), m, n, k, alpha, A.ctypes.data_as(_DP), A.shape[0],
+            B.ctypes.data_as(_DP), B.shape[0], beta, Cf.ctypes.data_as(_DP), m))
+        return Cf
 
     def omega_flops(self) -> float:
         return float(self.lib.ccsd_gpu_omega_flops(self.ctx))

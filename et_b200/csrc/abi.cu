@@ -4,6 +4,7 @@
 #include <new>
 
 #include "ccsd.cuh"
+#include "mixed_gemm.cuh"
 #include "ccsd_kernels.cuh"
 #include "tensor_ops.cuh"
 
@@ -217,6 +218,24 @@ int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops) {
     return guarded(ctx, [&](Context &c) {
         if (kernel_launches) *kernel_launches = c.ex.launches;
         if (gemm_flops) *gemm_flops = c.ex.flops;
+    });
+}
+
+int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t transB, int64_t m, int64_t n,
+                           int64_t k, double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+                           double beta, double *C, int64_t ldc) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(m > 0 && n > 0 && k > 0 && A && B && C, CCSD_GPU_EINVAL, "bad gemm arguments");
+        const int64_t na = transA ? lda * m : lda * k, nb = transB ? ldb * k : ldb * n, nc = ldc * n;
+        cudaStream_t s = c.ex.stream;
+        ccsd::DBuf dA = ccsd::dalloc(na, s), dB = ccsd::dalloc(nb, s), dC = ccsd::dalloc(nc, s);
+        h2d(c, dA.d(), A, na);
+        h2d(c, dB.d(), B, nb);
+        h2d(c, dC.d(), C, nc);
+        if (mixed) ccsd::mixed_gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc);
+        else ccsd::gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc, false);
+        d2h(c, C, dC.d(), nc);
+        REQUIRE(ccsd::mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM wait timed out");
     });
 }
 

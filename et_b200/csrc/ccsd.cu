@@ -8,6 +8,7 @@
 
 #include "ccsd.cuh"
 #include "ccsd_kernels.cuh"
+#include "mixed_gemm.cuh"
 #include "tensor_ops.cuh"
 
 namespace ccsd {
@@ -370,6 +371,10 @@ void Context::omega(double *om_out) {
     pack_half_diag_add(ex, 1.0, omS.d(), om2, nov);
     // omega_ccsd_a2
     ladder(t2, om2);
+    if (ex.prec == Prec::MIXED) {
+        CU_CHECK(cudaStreamSynchronize(s));
+        REQUIRE(mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM barrier wait timed out");
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -1,10 +1,346 @@
+// Split-BF16 GEMM for sm_100a: D = alpha * (Ahi Bhi^T + Ahi Blo^T + Alo Bhi^T) + beta * C.
+//
+// FP64 operands are converted once per call into bf16 hi/lo planes, K-major and zero padded
+// (M to 128, N to BN, K to 64).  The kernel is warp specialised: one thread issues TMA loads
+// of the four 128B-swizzled operand tiles into a ring of shared-memory stages, one thread
+// issues tcgen05.mma (kind::f16, FP32 accumulation in TMEM) for the three products of every
+// 16-wide K slice, and all four warps drain the 128 x BN accumulator through tcgen05.ld and
+// write FP64 column-major output (alpha/beta applied in FP64).  Every mbarrier wait is bounded;
+// on time-out the kernel records an error code, skips its remaining work and frees its TMEM.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <mutex>
+
 #include "mixed_gemm.cuh"
 
 namespace ccsd {
 
-void mixed_gemm(Exec &, bool, bool, int64_t, int64_t, int64_t, double, const double *, int64_t, const double *,
-                int64_t, double, double *, int64_t) {
-    throw Error(CCSD_GPU_EINVAL, "mixed precision GEMM is not built into this library");
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int BK = 64;                     // one 128-byte swizzle row of bf16
+constexpr int STAGES = 2;
+constexpr int A_TILE = BM * BK * 2;        // bytes per plane
+constexpr int B_TILE = BN * BK * 2;
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int THREADS = 128;
+constexpr uint32_t TMEM_COLS = BN;         // FP32 accumulator 128 lanes x BN columns
+constexpr long long WAIT_CYCLES = 4000000000ll;   // ~2 s at 2 GHz: far above any legitimate wait
+
+__device__ int g_mixed_gemm_error = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the completion of the phase with the given parity; false on time-out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t addr = smem_u32(bar);
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > WAIT_CYCLES) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1,
+                                            int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+// K-major operand tile, 128-byte swizzle: 8-row x 128 B atoms stacked along M/N (SBO = 1024 B)
+__device__ __forceinline__ uint64_t smem_desc(const void *tile, uint32_t k_byte_offset) {
+    uint64_t addr = smem_u32(tile) + k_byte_offset;
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;              // start address
+    d |= (uint64_t)(16 >> 4) << 16;            // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;          // stride byte offset
+    d |= 1ull << 46;                           // descriptor version (sm_100)
+    d |= 2ull << 61;                           // SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = BN
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
+                   int Kp, double alpha, double beta, double *__restrict__ C, long long ldc) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *done = empty + STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int nk = Kp / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        for (int i = 0; i < nk; i++) {
+            const int s = i % STAGES;
+            if (!mbar_wait(&empty[s], ((i / STAGES) & 1) ^ 1)) {
+                atomicExch(&g_mixed_gemm_error, 1);
+                *abort_flag = 1;
+                break;
+            }
+            if (*abort_flag) break;
+            uint8_t *st = smem + s * STAGE_BYTES;
+            mbar_expect_tx(&full[s], STAGE_BYTES);
+            const int k0 = i * BK;
+            tma_load_3d(&tmA, &full[s], st, k0, m0, 0);                       // A hi
+            tma_load_3d(&tmA, &full[s], st + A_TILE, k0, m0, 1);              // A lo
+            tma_load_3d(&tmB, &full[s], st + 2 * A_TILE, k0, n0, 0);          // B hi
+            tma_load_3d(&tmB, &full[s], st + 2 * A_TILE + B_TILE, k0, n0, 1); // B lo
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        bool ok = true;
+        for (int i = 0; i < nk; i++) {
+            const int s = i % STAGES;
+            if (!mbar_wait(&full[s], (i / STAGES) & 1)) {
+                atomicExch(&g_mixed_gemm_error, 2);
+                *abort_flag = 1;
+                ok = false;
+                break;
+            }
+            if (*abort_flag) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint8_t *st = smem + s * STAGE_BYTES;
+            const uint8_t *ahi = st, *alo = st + A_TILE, *bhi = st + 2 * A_TILE, *blo = st + 2 * A_TILE + B_TILE;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; kk++) {
+                const uint32_t ko = kk * 32;   // 16 bf16 = 32 bytes inside the swizzled row
+                mma_bf16(tmem, smem_desc(ahi, ko), smem_desc(bhi, ko), (i > 0 || kk > 0) ? 1u : 0u);
+                mma_bf16(tmem, smem_desc(ahi, ko), smem_desc(blo, ko), 1u);
+                mma_bf16(tmem, smem_desc(alo, ko), smem_desc(bhi, ko), 1u);
+            }
+            mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
+        }
+        // arrives once every MMA issued so far has completed (also on the abort path)
+        mma_commit(done);
+        (void)ok;
+    }
+    __syncwarp();
+
+    // epilogue: all four warps; warp w owns TMEM lanes 32w..32w+31 (rows m0 + 32w + lane)
+    bool ok = mbar_wait(done, 0);
+    if (!ok) {
+        atomicExch(&g_mixed_gemm_error, 3);
+        *abort_flag = 1;
+    }
+    __syncwarp();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = m0 + warp * 32 + lane;
+    if (ok && !*abort_flag) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int col = n0 + c0 + j;
+                    if (col < N) {
+                        double *dst = C + (long long)col * ldc + row;
+                        double r = alpha * (double)v[j];
+                        if (beta != 0.0) r += beta * *dst;
+                        *dst = r;
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// FP64 (strided view of op(X): element (r, k) at src[r*sr + k*sk]) -> bf16 hi/lo planes,
+// K-major [plane][R_pad][K_pad], zero padded.  32x32 smem tile so both sides stay coalesced.
+__global__ void split_bf16_kernel(const double *__restrict__ src, long long sr, long long sk, int R, int K, int Rp,
+                                  int Kp, __nv_bfloat16 *__restrict__ out) {
+    __shared__ double tile[32][33];
+    const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool k_fast = (sk == 1);
+    for (int i = ty; i < 32; i += 8) {
+        int r, k;
+        if (k_fast) {
+            r = r0 + i;
+            k = k0 + tx;
+        } else {
+            r = r0 + tx;
+            k = k0 + i;
+        }
+        double x = (r < R && k < K) ? src[(long long)r * sr + (long long)k * sk] : 0.0;
+        if (k_fast) tile[i][tx] = x;
+        else tile[tx][i] = x;
+    }
+    __syncthreads();
+    const size_t plane = (size_t)Rp * Kp;
+    for (int i = ty; i < 32; i += 8) {
+        const int r = r0 + i, k = k0 + tx;
+        if (r < Rp && k < Kp) {
+            double x = tile[i][tx];
+            __nv_bfloat16 hi = __double2bfloat16(x);
+            __nv_bfloat16 lo = __double2bfloat16(x - (double)__bfloat162float(hi));
+            out[(size_t)r * Kp + k] = hi;
+            out[plane + (size_t)r * Kp + k] = lo;
+        }
+    }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    REQUIRE(fn != nullptr, CCSD_GPU_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    return fn;
+}
+
+// planes x rows x K tensor of bf16, box (BK, box_rows, 1)
+CUtensorMap make_map(void *base, int rows_pad, int Kp, int box_rows) {
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows_pad, 2};
+    cuuint64_t strides[2] = {(cuuint64_t)Kp * 2, (cuuint64_t)Kp * 2 * rows_pad};
+    cuuint32_t box[3] = {BK, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    REQUIRE(r == CUDA_SUCCESS, CCSD_GPU_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return m;
+}
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
+           __nv_bfloat16 *out) {
+    dim3 grid((unsigned)(Kp / 32), (unsigned)(Rp / 32));
+    split_bf16_kernel<<<grid, dim3(32, 8), 0, ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, out);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+}  // namespace
+
+void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
+                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc) {
+    REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "mixed_gemm: size too large");
+    CU_CHECK(cudaFuncSetAttribute(bf16x3_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, BN);
+    DBuf a(sizeof(__nv_bfloat16) * 2 * Mp * Kp, ex.stream), b(sizeof(__nv_bfloat16) * 2 * Np * Kp, ex.stream);
+    // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T)
+    if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, a.as<__nv_bfloat16>());
+    else split(ex, A, lda, 1, m, k, Mp, Kp, a.as<__nv_bfloat16>());
+    // B operand rows are output columns: op(B)(kk, c) = B[kk + ldb c] (N) or B[c + ldb kk] (T)
+    if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, b.as<__nv_bfloat16>());
+    else split(ex, B, 1, ldb, n, k, Np, Kp, b.as<__nv_bfloat16>());
+    CUtensorMap ta = make_map(a.as<void>(), (int)Mp, (int)Kp, BM);
+    CUtensorMap tb = make_map(b.as<void>(), (int)Np, (int)Kp, BN);
+    dim3 grid((unsigned)(Mp / BM), (unsigned)(Np / BN));
+    bf16x3_gemm_kernel<<<grid, THREADS, SMEM_BYTES, ex.stream>>>(ta, tb, (int)m, (int)n, (int)Kp, alpha, beta, C,
+                                                                   (long long)ldc);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+int mixed_gemm_error_flag(bool reset) {
+    int v = 0;
+    CU_CHECK(cudaMemcpyFromSymbol(&v, g_mixed_gemm_error, sizeof(int)));
+    if (reset && v) {
+        int z = 0;
+        CU_CHECK(cudaMemcpyToSymbol(g_mixed_gemm_error, &z, sizeof(int)));
+    }
+    return v;
 }
 
 }  // namespace ccsd

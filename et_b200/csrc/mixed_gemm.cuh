@@ -10,4 +10,7 @@ namespace ccsd {
 void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha,
                 const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc);
 
+// Error code recorded by a tensor-core GEMM whose bounded barrier wait timed out (0 = none).
+int mixed_gemm_error_flag(bool reset);
+
 }  // namespace ccsd

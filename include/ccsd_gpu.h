@@ -125,6 +125,12 @@ int ccsd_gpu_solve_gs(void *ctx, const ccsd_gpu_solver_options *opt, double *ene
 /* Counters since creation: kernels of this library launched and GEMM flops issued. */
 int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops);
 
+/* Diagnostics: C (m x n, column-major, host) = alpha op(A) op(B) + beta C on the device, through
+ * the FP64 DGEMM (mixed = 0) or the split-BF16 tcgen05 GEMM (mixed = 1) that the contractions use. */
+int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t transB, int64_t m, int64_t n,
+                           int64_t k, double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+                           double beta, double *C, int64_t ldc);
+
 /* Algorithmic flop count of one Omega at this context's dimensions, summed over eT's own BLAS
  * call sites (2mnk per DGEMM, n(n+1)k per DSFRK). */
 double ccsd_gpu_omega_flops(void *ctx);

@@ -1,0 +1,87 @@
+"""Split-BF16 tcgen05 GEMM and the mixed-precision Omega against FP64 references."""
+
+import numpy as np
+import pytest
+
+from et_b200.synthetic import make_system
+from oracle import ccsd as oc
+
+pytestmark = pytest.mark.gpu
+
+# bf16 hi+lo keeps ~16 significant bits per operand; the dropped lo*lo product and the FP32
+# accumulation leave a relative error of order 1e-5 per dot product.
+GEMM_RTOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from et_b200 import CCSD
+    c = CCSD(2, 3, 4)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 256, 64), (200, 300, 100), (1, 1, 16), (129, 257, 65),
+                                   (640, 512, 1200), (300, 1000, 777)])
+@pytest.mark.parametrize("tA,tB", [(False, False), (True, False), (False, True), (True, True)])
+def test_mixed_gemm_matches_fp64(ctx, m, n, k, tA, tB):
+    rng = np.random.default_rng(m * 7 + n * 3 + k)
+    A = rng.standard_normal((k, m) if tA else (m, k))
+    B = rng.standard_normal((n, k) if tB else (k, n))
+    C0 = rng.standard_normal((m, n))
+    ref = 0.7 * ((A.T if tA else A) @ (B.T if tB else B)) - 0.3 * C0
+    out = ctx.selftest_gemm(A, B, C0, alpha=0.7, beta=-0.3, transA=tA, transB=tB, mixed=True)
+    scale = np.abs(A).max() * np.abs(B).max() * np.sqrt(k)
+    assert np.abs(out - ref).max() <= GEMM_RTOL * scale
+
+
+def test_fp64_gemm_path(ctx):
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((70, 50))
+    B = rng.standard_normal((50, 90))
+    out = ctx.selftest_gemm(A, B, mixed=False)
+    assert np.abs(out - A @ B).max() < 1e-12
+
+
+def test_mixed_gemm_repeatable(ctx):
+    """Two calls in a row give bitwise identical results (no state leaks between launches)."""
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((300, 200))
+    B = rng.standard_normal((200, 400))
+    a = ctx.selftest_gemm(A, B, mixed=True)
+    b = ctx.selftest_gemm(A, B, mixed=True)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("dims", [(4, 16, 40), (8, 40, 100)])
+def test_mixed_omega_close_to_oracle(dims):
+    from et_b200 import CCSD, MIXED
+    n_o, n_v, n_J = dims
+    s = make_system(n_o, n_v, n_J, seed=9)
+    ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
+    ref.mp2_start()
+    gpu = CCSD(n_o, n_v, n_J, precision=MIXED, mixed_min_flops=1)
+    gpu.set_system(s.L_mo, s.h_mo, s.eps)
+    gpu.set_amplitudes(ref.get_amplitudes())
+    om = gpu.construct_omega()
+    om_ref = ref.omega()
+    assert np.linalg.norm(om - om_ref) <= 1e-4 * np.linalg.norm(om_ref)
+    gpu.close()
+
+
+def test_mixed_solver_refines_to_fp64_energy():
+    """Mixed iterations followed by FP64 refinement land on the FP64 energy (|dE| <= 1e-8 Eh)."""
+    from et_b200 import CCSD, FP64, MIXED
+    n_o, n_v, n_J = 6, 40, 120
+    s = make_system(n_o, n_v, n_J, seed=21)
+    res = {}
+    for prec in (FP64, MIXED):
+        gpu = CCSD(n_o, n_v, n_J, precision=prec, mixed_min_flops=1)
+        gpu.set_system(s.L_mo, s.h_mo, s.eps)
+        gpu.set_initial_amplitudes_guess()
+        e, it, hist, rc = gpu.solve_ground_state(omega_threshold=1e-9, energy_threshold=1e-11,
+                                                 refine_threshold=1e-5)
+        assert rc == 0
+        res[prec] = e
+        gpu.close()
+    assert abs(res[MIXED] - res[FP64]) <= 1e-8
