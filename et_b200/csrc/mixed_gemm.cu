@@ -234,37 +234,41 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
 }
 
 // FP64 (strided view of op(X): element (r, k) at src[r*sr + k*sk]) -> bf16 hi/lo planes,
-// K-major [plane][R_pad][K_pad], zero padded.  32x32 smem tile so both sides stay coalesced.
+// K-major [plane][R_pad][K_pad], zero padded.  32x32 smem tile so both sides stay coalesced;
+// blockIdx.x runs over row blocks (up to 2^31), blockIdx.y strides over K blocks.
 __global__ void split_bf16_kernel(const double *__restrict__ src, long long sr, long long sk, int R, int K, int Rp,
                                   int Kp, __nv_bfloat16 *__restrict__ out) {
     __shared__ double tile[32][33];
-    const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int r0 = blockIdx.x * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool k_fast = (sk == 1);
-    for (int i = ty; i < 32; i += 8) {
-        int r, k;
-        if (k_fast) {
-            r = r0 + i;
-            k = k0 + tx;
-        } else {
-            r = r0 + tx;
-            k = k0 + i;
-        }
-        double x = (r < R && k < K) ? src[(long long)r * sr + (long long)k * sk] : 0.0;
-        if (k_fast) tile[i][tx] = x;
-        else tile[tx][i] = x;
-    }
-    __syncthreads();
     const size_t plane = (size_t)Rp * Kp;
-    for (int i = ty; i < 32; i += 8) {
-        const int r = r0 + i, k = k0 + tx;
-        if (r < Rp && k < Kp) {
-            double x = tile[i][tx];
-            __nv_bfloat16 hi = __double2bfloat16(x);
-            __nv_bfloat16 lo = __double2bfloat16(x - (double)__bfloat162float(hi));
-            out[(size_t)r * Kp + k] = hi;
-            out[plane + (size_t)r * Kp + k] = lo;
+    for (int k0 = blockIdx.y * 32; k0 < Kp; k0 += gridDim.y * 32) {
+        for (int i = ty; i < 32; i += 8) {
+            int r, k;
+            if (k_fast) {
+                r = r0 + i;
+                k = k0 + tx;
+            } else {
+                r = r0 + tx;
+                k = k0 + i;
+            }
+            double x = (r < R && k < K) ? src[(long long)r * sr + (long long)k * sk] : 0.0;
+            if (k_fast) tile[i][tx] = x;
+            else tile[tx][i] = x;
         }
+        __syncthreads();
+        for (int i = ty; i < 32; i += 8) {
+            const int r = r0 + i, k = k0 + tx;
+            if (r < Rp && k < Kp) {
+                double x = tile[i][tx];
+                __nv_bfloat16 hi = __double2bfloat16(x);
+                __nv_bfloat16 lo = __double2bfloat16(x - (double)__bfloat162float(hi));
+                out[(size_t)r * Kp + k] = hi;
+                out[plane + (size_t)r * Kp + k] = lo;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -304,7 +308,7 @@ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
            __nv_bfloat16 *out) {
-    dim3 grid((unsigned)(Kp / 32), (unsigned)(Rp / 32));
+    dim3 grid((unsigned)(Rp / 32), (unsigned)std::min<int64_t>(Kp / 32, 65535));
     split_bf16_kernel<<<grid, dim3(32, 8), 0, ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());

@@ -143,7 +143,9 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
     if (m == 0 || n == 0) return;
     double fl = 2.0 * double(m) * double(n) * double(k);
     ex.flops += fl;
-    if (allow_mixed && ex.prec == Prec::MIXED && fl >= ex.mixed_min_flops && k >= 16) {
+    // the tensor-core tile is 128 x 256 x 64: skinny products stay on the FP64 pipe
+    if (allow_mixed && ex.prec == Prec::MIXED && fl >= ex.mixed_min_flops && k >= 16 &&
+        (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64))) {
         mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
         return;
     }
