@@ -131,6 +131,41 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["bf16_tflops"]), float(pk.get("bf16_tflops_sustained", pk["bf16_tflops"])), \
+            float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, 1400.0, 6650.0, "fallback"
+
+
+def timed_solve(gpu, stream, iters, refine, world, clocks_dev=None):
+    """Exactly `iters` ground-state iterations from the MP2 start, timed with CUDA events."""
+    import torch
+    gpu.set_initial_amplitudes_guess()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(clocks_dev) if clocks_dev is not None else None
+    if clk:
+        clk.__enter__()
+    ev0.record(stream)
+    e, it, hist, rc = gpu.solve_ground_state(max_iterations=iters, omega_threshold=1e-30, energy_threshold=-1.0,
+                                             refine_threshold=refine, raise_on_failure=False)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    barrier(world)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), e, it, hist, clk
+
+
 def run_gpu(args):
     import torch
     from et_b200 import CCSD, FP64, MIXED
@@ -147,30 +182,15 @@ def run_gpu(args):
     gpu.set_system(sysd.L_mo, sysd.h_mo, sysd.eps, sysd.e_hf)
     flops_iter, flops_omega = iteration_flops(n_o, n_v, n_J)
 
-    # warm-up: W iterations from the MP2 start
-    gpu.set_initial_amplitudes_guess()
-    gpu.solve_ground_state(max_iterations=args.warmup, omega_threshold=1e-30, energy_threshold=-1.0,
-                           refine_threshold=args.refine, raise_on_failure=False)
-    # timed: K iterations from the MP2 start (inputs are > L2: t 419 MB, L 1.19 GB)
-    gpu.set_initial_amplitudes_guess()
+    # warm-up iterations, then exactly K timed iterations from the MP2 start
+    timed_solve(gpu, stream, args.warmup, args.refine, world)
     launches0, _ = gpu.stats()
-    torch.cuda.synchronize()
-    barrier(world)
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        e, it, hist, rc = gpu.solve_ground_state(max_iterations=args.steps, omega_threshold=1e-30,
-                                                 energy_threshold=-1.0, refine_threshold=args.refine,
-                                                 raise_on_failure=False)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    barrier(world)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms, world)
+    gpu.set_profiling(True)
+    ms, e, it, hist, clk = timed_solve(gpu, stream, args.steps, args.refine, world, clocks_dev=local)
+    n_gemm, gemm_ms, gemm_flops = gpu.gemm_profile()
+    gpu.set_profiling(False)
     launches1, _ = gpu.stats()
+    ms = max_over_ranks(ms, world)
     ms_step = ms / max(it, 1)
     value = world * flops_iter * it / (ms * 1e-3) / 1e12
 
@@ -184,11 +204,20 @@ def run_gpu(args):
     for _ in range(e2e_steps):
         gpu.set_amplitudes(t_host)
         gpu.calculate_energy()
-        om = gpu.construct_omega()
+        gpu.construct_omega()
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_s = max_over_ranks(e2e_s, world)
-    e2e_value = world * (flops_omega + iteration_flops(n_o, n_v, n_J)[0] - flops_omega) / e2e_s / 1e12
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
+
+    peak_burst, peak_sust, hbm, peak_kind = load_peaks()
+    roof = None
+    if n_gemm:
+        achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12
+        roof = {"kernel": "bf16x3_gemm_kernel (tcgen05 split-BF16 GEMM)", "bound": "tensor",
+                "achieved": round(achieved, 2), "peak": peak_sust, "unit": "TFLOP/s",
+                "frac": round(achieved / peak_sust, 4), "peak_kind": f"{peak_kind} bf16 sustained (timed inside a long step)",
+                "traffic": None, "launches": n_gemm, "avg_launch_ms": round(gemm_ms / n_gemm, 4),
+                "share_of_step": round(gemm_ms / ms, 4),
+                "flops_counted": "issued tensor flops: 3 bf16 products x 2mnk per launch"}
 
     result = {
         "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": it,
@@ -197,15 +226,30 @@ def run_gpu(args):
         "dtype": "bf16x3+f64" if prec == MIXED else "f64", "data": "synthetic",
         "config": {"workload": f"CCSD ground-state iteration, synthetic Cholesky system o={n_o} v={n_v} N_J={n_J}",
                    "n_o": n_o, "n_v": n_v, "n_J": n_J, "precision": args.precision,
+                   "refine_threshold": args.refine,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "inputs larger than L2 (t2 419 MB, L 1.19 GB at full size)",
                    "flops_per_iter": flops_iter},
-        "clocks": clk.summary(),
-        "e2e": {"value": round(e2e_value, 3), "unit": "TFLOP/s", "s_per_iter": round(e2e_s, 5),
+        "clocks": clk.summary() if clk else None,
+        "e2e": {"value": round(world * flops_iter / e2e_s / 1e12, 3), "unit": "TFLOP/s", "s_per_iter": round(e2e_s, 5),
                 "h2d_bytes_per_step": int(8 * gpu.n_amp), "d2h_bytes_per_step": int(8 * gpu.n_amp + 8)},
         "gpu_launches": int(launches1 - launches0),
-        "energy_after_steps": e, "omega_norm_after_steps": float(hist[-1, 1]) if len(hist) else None,
+        "roofline": roof,
+        "solve": {"energy": e, "omega_norm": float(hist[-1, 1]) if len(hist) else None,
+                  "omega_history": [float(x) for x in hist[:, 1]]},
     }
+    if args.compare and world == 1 and prec == MIXED:
+        # the plain FP64 GPU path on the same system: per-iteration time and converged energy
+        gpu.set_precision(FP64)
+        ms64, _, it64, _, _ = timed_solve(gpu, stream, 3, args.refine, world)
+        gpu.set_initial_amplitudes_guess()
+        e64, n64, _, rc64 = gpu.solve_ground_state(max_iterations=60, omega_threshold=1e-9, energy_threshold=1e-11,
+                                                   raise_on_failure=False)
+        s64 = ms64 / 1e3 / it64
+        result["fp64_path"] = {"s_per_iter": round(s64, 5), "energy": e64, "iterations_to_1e-9": n64,
+                               "converged": rc64 == 0}
+        result["speedup_per_iter_vs_fp64"] = round(s64 / (ms_step / 1e3), 3)
+        result["dE_vs_fp64"] = abs(e - e64)
     gpu.close()
     if world > 1:
         import torch.distributed as dist
@@ -255,11 +299,13 @@ def run_reference(args):
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=15)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    p.add_argument("--refine", type=float, default=1e-5)
+    p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    p.add_argument("--refine", type=float, default=1e-4)
+    p.add_argument("--no-compare", dest="compare", action="store_false",
+                   help="skip the FP64-path comparison (per-iteration time and converged energy)")
     p.add_argument("--n-o", dest="n_o", type=int, default=32)
     p.add_argument("--n-v", dest="n_v", type=int, default=320)
     p.add_argument("--n-J", dest="n_J", type=int, default=1200)

@@ -77,6 +77,8 @@ SIGNATURES = {
     "ccsd_gpu_solve_gs": (ctypes.c_int, [_VP, ctypes.POINTER(SolverOptions), _DP,
                                          ctypes.POINTER(ctypes.c_int32), _DP]),
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
+    "ccsd_gpu_set_profiling": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "ccsd_gpu_gemm_profile": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP, _DP]),
     "ccsd_gpu_selftest_gemm": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I64, _I64,
                                               _I64, ctypes.c_double, _DP, _I64, _DP, _I64, ctypes.c_double, _DP,
                                               _I64]),
@@ -245,6 +247,17 @@ class CCSD:
         f = ctypes.c_double()
         self._check(self.lib.ccsd_gpu_stats(self.ctx, ctypes.byref(n), ctypes.byref(f)))
         return n.value, f.value
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.ccsd_gpu_set_profiling(self.ctx, int(bool(on))))
+
+    def gemm_profile(self):
+        """(launches, device ms, tensor flops) of the tensor-core GEMMs since profiling was enabled."""
+        n = ctypes.c_int64()
+        ms = ctypes.c_double()
+        fl = ctypes.c_double()
+        self._check(self.lib.ccsd_gpu_gemm_profile(self.ctx, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(fl)))
+        return n.value, ms.value, fl.value
 
     def selftest_gemm(self, A, B, C=None, *, alpha=1.0, beta=0.0, transA=False, transB=False, mixed=True):
         """C = alpha op(A) op(B) + beta C on the device (diagnostics of the GEMM back ends)."""

@@ -221,6 +221,29 @@ int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops) {
     });
 }
 
+int ccsd_gpu_set_profiling(void *ctx, int32_t on) {
+    return guarded(ctx, [&](Context &c) {
+        c.prof.clear();
+        c.prof.on = on != 0;
+    });
+}
+
+int ccsd_gpu_gemm_profile(void *ctx, int64_t *launches, double *device_ms, double *tensor_flops) {
+    return guarded(ctx, [&](Context &c) {
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        double ms = 0.0, fl = 0.0;
+        for (size_t i = 0; i < c.prof.events.size(); i++) {
+            float t = 0.f;
+            CU_CHECK(cudaEventElapsedTime(&t, c.prof.events[i].first, c.prof.events[i].second));
+            ms += t;
+            fl += c.prof.flops[i];
+        }
+        if (launches) *launches = (int64_t)c.prof.events.size();
+        if (device_ms) *device_ms = ms;
+        if (tensor_flops) *tensor_flops = fl;
+    });
+}
+
 int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t transB, int64_t m, int64_t n,
                            int64_t k, double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
                            double beta, double *C, int64_t ldc) {

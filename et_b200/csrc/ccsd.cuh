@@ -13,6 +13,7 @@ struct Context {
     cudaStream_t own_stream = nullptr;
     cublasHandle_t blas = nullptr;
     Exec ex;
+    GemmProfile prof;
     int64_t ladder_batch = 0;
     double e_hf = 0.0;
     bool have_L = false, have_h = false, have_t = false;

@@ -114,6 +114,22 @@ inline TV tv(const double *p, std::initializer_list<int64_t> dims) {
 
 enum class Prec { FP64, MIXED };
 
+// CUDA-event timing of the tensor-core GEMM launches (enabled on request).
+struct GemmProfile {
+    bool on = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::vector<double> flops;    // tensor flops issued per launch (3 products x 2mnk)
+    void clear() {
+        for (auto &e : events) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        events.clear();
+        flops.clear();
+    }
+    ~GemmProfile() { clear(); }
+};
+
 // Execution environment handed to the tensor kernels.
 struct Exec {
     cudaStream_t stream = nullptr;
@@ -122,6 +138,7 @@ struct Exec {
     double mixed_min_flops = 2e9;
     double flops = 0.0;          // algorithmic flops issued (counted by contract())
     int64_t launches = 0;        // kernels of this library launched
+    GemmProfile *prof = nullptr;
 };
 
 }  // namespace ccsd

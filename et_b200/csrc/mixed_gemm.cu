@@ -331,10 +331,21 @@ void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     CUtensorMap ta = make_map(a.as<void>(), (int)Mp, (int)Kp, BM);
     CUtensorMap tb = make_map(b.as<void>(), (int)Np, (int)Kp, BN);
     dim3 grid((unsigned)(Mp / BM), (unsigned)(Np / BN));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ex.prof && ex.prof->on) {
+        CU_CHECK(cudaEventCreate(&e0));
+        CU_CHECK(cudaEventCreate(&e1));
+        CU_CHECK(cudaEventRecord(e0, ex.stream));
+    }
     bf16x3_gemm_kernel<<<grid, THREADS, SMEM_BYTES, ex.stream>>>(ta, tb, (int)m, (int)n, (int)Kp, alpha, beta, C,
                                                                    (long long)ldc);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
+    if (e0) {
+        CU_CHECK(cudaEventRecord(e1, ex.stream));
+        ex.prof->events.emplace_back(e0, e1);
+        ex.prof->flops.push_back(3.0 * 2.0 * double(m) * double(n) * double(k));
+    }
 }
 
 int mixed_gemm_error_flag(bool reset) {

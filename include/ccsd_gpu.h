@@ -125,6 +125,12 @@ int ccsd_gpu_solve_gs(void *ctx, const ccsd_gpu_solver_options *opt, double *ene
 /* Counters since creation: kernels of this library launched and GEMM flops issued. */
 int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops);
 
+/* Kernel timing: when enabled, every tensor-core GEMM launch is bracketed by CUDA events on the
+ * context's stream.  ccsd_gpu_gemm_profile returns the launches recorded since it was enabled,
+ * their summed device time (ms) and the tensor flops they issued (3 products x 2mnk). */
+int ccsd_gpu_set_profiling(void *ctx, int32_t on);
+int ccsd_gpu_gemm_profile(void *ctx, int64_t *launches, double *device_ms, double *tensor_flops);
+
 /* Diagnostics: C (m x n, column-major, host) = alpha op(A) op(B) + beta C on the device, through
  * the FP64 DGEMM (mixed = 0) or the split-BF16 tcgen05 GEMM (mixed = 1) that the contractions use. */
 int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t transB, int64_t m, int64_t n,
