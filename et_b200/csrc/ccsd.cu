@@ -1,6 +1,8 @@
 // CCSD hot path on one B200: T1-transformed Cholesky vectors, T1 Fock matrix, energy,
 // the residual Omega(t), and the device-resident quasi-Newton + DIIS ground-state solver.
 // Each step restates one eT routine (paths relative to the eT source tree).
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -192,6 +194,10 @@ void Context::mp2_guess() {
 // omega_ccsd_a2 (src/wavefunctions/ccsd/omega_ccsd.F90:113-480), batched over a.
 // ---------------------------------------------------------------------------
 void Context::ladder(const double *t2, double *om2) {
+    if (ex.prec == Prec::MIXED) {
+        ladder_tc(t2, om2);
+        return;
+    }
     cudaStream_t s = ex.stream;
     const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
     const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
@@ -240,6 +246,57 @@ void Context::ladder(const double *t2, double *om2) {
             gemm(ex, false, false, nom, nabm, nvm, 0.5, tm.d(), nom, gm.d(), nvm, 0.0, wm.d(), nom);
         add_omega_pm(ex, om2, wp.d(), wm.d(), no, nv, a0, a1);
     }
+}
+
+// Tensor-core form of the same ladder.  With M_ab[c,d] = g_acbd the +/- sums of
+// omega_ccsd_a2 over packed c >= d equal sums over all (c, d):
+//   omega+_ij,ab = sum_cd 1/2 (1 - d_ij/2)(t_cidj + t_cjdi) M_ab[c,d]
+//   omega-_ij,ab = sum_cd 1/2 (t_cidj - t_cjdi) M_ab[c,d]
+// so the split-bf16 integrals M_ab (written by the G GEMM epilogue, all pairs b <= a resident
+// in HBM) meet [T+; T-] in one GEMM of N = n_o^2 and K = n_v^2.
+void Context::ladder_tc(const double *t2, double *om2) {
+    cudaStream_t s = ex.stream;
+    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
+    const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
+    // split L~_vv rows r = c + nv a (K = J): source element (r, J) = L~[J, a, c] at J + nJ (a + nv c)
+    const int64_t l_rows = tc_pad_rows_a(nv2);
+    DBuf LS(sizeof(__nv_bfloat16) * 2 * l_rows * Jp, s);
+    {
+        // r = c + nv a  ->  offset nJ*(a + nv*c): not a single stride, so split from the (J, c, a) copy
+        DBuf LT = dalloc(nJ * nv2, s);
+        TV src = tv(Lt_vv.d(), {nJ, nv, nv});   // [J, a, c]
+        TV dst;
+        dst.p = LT.d();
+        dst.nd = 3;
+        dst.n[0] = nJ;
+        dst.n[1] = nv;
+        dst.n[2] = nv;
+        dst.s[0] = 1;
+        dst.s[1] = nJ * nv;   // a
+        dst.s[2] = nJ;        // c
+        permute_add(ex, 1.0, src, 0.0, dst);
+        split_rows(ex, LT.d(), nJ, 1, nv2, nJ, l_rows, Jp, LS.as<__nv_bfloat16>());
+    }
+    const int64_t rows_T = tc_pad_rows_b(nrow);
+    DBuf TS(sizeof(__nv_bfloat16) * 2 * rows_T * Kq, s);
+    build_T(ex, t2, no, nv, rows_T, Kq, TS.as<__nv_bfloat16>());
+    // all pair integrals, resident: [2][mrows][Kq]
+    const int64_t mrows = tc_pad_rows_a(nab);
+    if (mbuf_bytes < sizeof(__nv_bfloat16) * 2 * (size_t)mrows * Kq) {
+        mbuf = DBuf(sizeof(__nv_bfloat16) * 2 * (size_t)mrows * Kq, s);
+        mbuf_bytes = mbuf.bytes();
+        CU_CHECK(cudaMemsetAsync(mbuf.as<void>(), 0, mbuf_bytes, s));   // padding rows / K stay zero
+    }
+    int64_t nA = ladder_batch > 0 ? ladder_batch : 16;
+    for (int64_t a0 = 0; a0 < nv; a0 += nA) {
+        int64_t a1 = std::min(nv, a0 + nA);
+        tc_gemm_pairs(ex, LS.as<__nv_bfloat16>(), l_rows, Jp, nv, a0, a1, mbuf.as<__nv_bfloat16>(), mrows, Kq, nJ);
+    }
+    DBuf W = dalloc(nab * nrow, s);
+    tc_gemm_f64(ex, mbuf.as<__nv_bfloat16>(), mrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nab, nrow, nv2, 1.0, 0.0,
+                W.d(), nab);
+    add_omega_T(ex, om2, W.d(), nab, no, nv);
+    ex.flops += double(nv2) * double(nv2 + 1) * double(nJ) + 2.0 * double(nab) * double(nrow) * double(nv2);
 }
 
 // ---------------------------------------------------------------------------

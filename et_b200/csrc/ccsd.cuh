@@ -26,6 +26,8 @@ struct Context {
     DBuf t;                  // [t1 | packed t2]
     DBuf epsdiff;            // orbital differences (n_amp)
     DBuf scal;               // scalar scratch
+    DBuf mbuf;               // split-bf16 ladder integrals M_ab[c,d] for all pairs (mixed precision)
+    size_t mbuf_bytes = 0;
 
     Context(int64_t no, int64_t nv, int64_t nJ, const ccsd_gpu_options *opt);
     ~Context();
@@ -39,6 +41,7 @@ struct Context {
     void mp2_guess();
     void omega(double *d_omega);
     void ladder(const double *t2, double *om2);
+    void ladder_tc(const double *t2, double *om2);
     int solve_gs(const ccsd_gpu_solver_options *o, double *energy, int32_t *iters, double *history);
     double omega_flops() const;
 };

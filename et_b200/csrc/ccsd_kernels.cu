@@ -2,6 +2,8 @@
 // energy, MP2 guess, quasi-Newton update and DIIS (all FP64).
 #include <cmath>
 
+#include <cuda_bf16.h>
+
 #include "ccsd_kernels.cuh"
 
 namespace ccsd {
@@ -20,12 +22,6 @@ __device__ __forceinline__ void untri(int64_t idx, int64_t &M, int64_t &m) {
     while ((r + 1) * (r + 2) / 2 <= idx) r++;
     M = r;
     m = idx - r * (r + 1) / 2;
-}
-
-// strict lower triangle: idx = M(M-1)/2 + m, M > m
-__device__ __forceinline__ void untri_strict(int64_t idx, int64_t &M, int64_t &m) {
-    untri(idx, M, m);   // gives (M', m') with idx = M'(M'+1)/2 + m', m' <= M'
-    M += 1;             // M(M-1)/2 = M'(M'+1)/2 with M = M'+1
 }
 
 inline int grid_for(int64_t total, int block) {
@@ -90,6 +86,60 @@ __global__ void add_omega_pm_kernel(double *__restrict__ om2, const double *__re
         if (i != j && a != b) {
             int64_t ijm = i * (i - 1) / 2 + j, locm = a * (a - 1) / 2 + b - abm0;
             double m = wm[ijm + nom * locm];
+            x1 = p + m;
+            x2 = p - m;
+        }
+        int64_t P1 = pk(a + nv * i, b + nv * j), P2 = pk(a + nv * j, b + nv * i);
+        if (P1 == P2) {
+            om2[P1] += x1 + x2;
+        } else {
+            om2[P1] += x1;
+            om2[P2] += x2;
+        }
+    }
+}
+
+// T+ and T- of the full-(c,d) ladder as split bf16 rows: row ij_p (i >= j) carries
+// 1/2 (1 - d_ij/2)(t_cidj + t_cjdi), row n_o_p + ij_m (i > j) carries 1/2 (t_cidj - t_cjdi),
+// both at K position c + nv*d; padding rows/columns are zero.
+__global__ void build_T_kernel(const double *__restrict__ t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq,
+                               __nv_bfloat16 *__restrict__ out) {
+    const int64_t nop = no * (no + 1) / 2, nrow = no * no, nv2 = nv * nv;
+    const size_t plane = (size_t)rows_pad * Kq;
+    GRID_STRIDE(idx, rows_pad * Kq) {
+        int64_t row = idx / Kq, k = idx - (idx / Kq) * Kq;
+        double val = 0.0;
+        if (row < nrow && k < nv2) {
+            int64_t c = k % nv, d = k / nv, i, j;
+            bool plus = row < nop;
+            if (plus) untri(row, i, j);
+            else {
+                untri(row - nop, i, j);   // strict: idx = M(M-1)/2 + m maps to (M-1, m)
+                i += 1;
+            }
+            double x = t2[pk(c + nv * i, d + nv * j)];
+            double y = t2[pk(c + nv * j, d + nv * i)];
+            val = plus ? 0.5 * (i == j ? 0.5 : 1.0) * (x + y) : 0.5 * (x - y);
+        }
+        __nv_bfloat16 hi = __double2bfloat16(val);
+        out[idx] = hi;
+        out[plane + idx] = __double2bfloat16(val - (double)__bfloat162float(hi));
+    }
+}
+
+// Omega contributions from W (nab x n_o^2, column-major, ldw): column ij_p holds omega+,
+// column n_o_p + ij_m holds omega- for the pair row ab = a(a+1)/2 + b.
+__global__ void add_omega_T_kernel(double *__restrict__ om2, const double *__restrict__ W, int64_t ldw, int64_t no,
+                                   int64_t nv) {
+    const int64_t nop = no * (no + 1) / 2, nab = nv * (nv + 1) / 2;
+    GRID_STRIDE(idx, nab * nop) {
+        int64_t ab = idx % nab, ij = idx / nab, a, b, i, j;
+        untri(ab, a, b);
+        untri(ij, i, j);
+        double p = W[ab + ldw * ij] * (a == b ? 0.5 : 1.0);
+        double x1 = p, x2 = p;
+        if (i != j && a != b) {
+            double m = W[ab + ldw * (nop + i * (i - 1) / 2 + j)];
             x1 = p + m;
             x2 = p - m;
         }
@@ -295,6 +345,19 @@ void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int
                   int64_t a1) {
     int64_t total = (no * (no + 1) / 2) * (a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2);
     add_omega_pm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, wp, wm, no, nv, a0, a1);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, __nv_bfloat16 *out) {
+    build_T_kernel<<<grid_for(rows_pad * Kq, 256), 256, 0, ex.stream>>>(t2, no, nv, rows_pad, Kq, out);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv) {
+    int64_t total = (nv * (nv + 1) / 2) * (no * (no + 1) / 2);
+    add_omega_T_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, W, ldw, no, nv);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }

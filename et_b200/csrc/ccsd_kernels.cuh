@@ -1,6 +1,8 @@
 // Bandwidth kernels of the CCSD path (declarations).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace ccsd {
@@ -18,6 +20,10 @@ void form_gpm(Exec &ex, const double *G, int64_t ldg, double *gp, double *gm, in
 // add_double/single_packed_plus_minus with the omega+ (a == b) half scaling
 void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int64_t no, int64_t nv, int64_t a0,
                   int64_t a1);
+
+// T+/T- rows of the tensor-core ladder (split bf16, [2][rows_pad][Kq]) and the scatter of its result
+void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, __nv_bfloat16 *out);
+void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv);
 
 void energy_reduce(Exec &ex, const double *t1, const double *t2, const double *g_ovov, int64_t no, int64_t nv,
                    double add, double *d_out);

@@ -112,9 +112,54 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+}  // namespace
+
+// FP64 column-major output with alpha/beta
+struct EpiF64 {
+    double *C;
+    long long ldc;
+    int M, N;
+    double alpha, beta;
+    __device__ __forceinline__ void row_setup(int) {}
+    __device__ __forceinline__ void operator()(int row, int col, float v) const {
+        if (row < M && col < N) {
+            double *dst = C + (long long)col * ldc + row;
+            double r = alpha * (double)v;
+            if (beta != 0.0) r += beta * *dst;
+            *dst = r;
+        }
+    }
+};
+
+// A2 ladder integrals: row (c, a) = c + nv*(a - a0), column (d, b) = d + nv*b of
+// G = L_vv^T L_vv is M_ab[c,d] = g_acbd; kept for b <= a and written as split bf16 at
+// pair row ab = a(a+1)/2 + b, K position c + nv*d.
+struct EpiPairs {
+    __nv_bfloat16 *out;
+    size_t plane;
+    long long ldk;
+    int nv, a0, M, N;
+    int a, c;
+    __device__ __forceinline__ void row_setup(int row) {
+        a = a0 + row / nv;
+        c = row - (row / nv) * nv;
+    }
+    __device__ __forceinline__ void operator()(int row, int col, float v) const {
+        if (row >= M || col >= N) return;
+        const int b = col / nv, d = col - b * nv;
+        if (b > a) return;
+        const size_t idx = (size_t)((long long)a * (a + 1) / 2 + b) * ldk + c + (long long)nv * d;
+        __nv_bfloat16 hi = __float2bfloat16(v);
+        out[idx] = hi;
+        out[plane + idx] = __float2bfloat16(v - __bfloat162float(hi));
+    }
+};
+
+namespace {
+
+template <class Epi>
 __global__ void __launch_bounds__(THREADS, 1)
-bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
-                   int Kp, double alpha, double beta, double *__restrict__ C, long long ldc) {
+bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int Kp, Epi epi) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -207,23 +252,14 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
     __syncwarp();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int row = m0 + warp * 32 + lane;
+    epi.row_setup(row);
     if (ok && !*abort_flag) {
 #pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 16) {
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (row < M) {
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const int col = n0 + c0 + j;
-                    if (col < N) {
-                        double *dst = C + (long long)col * ldc + row;
-                        double r = alpha * (double)v[j];
-                        if (beta != 0.0) r += beta * *dst;
-                        *dst = r;
-                    }
-                }
-            }
+            for (int j = 0; j < 16; j++) epi(row, n0 + c0 + j, v[j]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -290,11 +326,12 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// planes x rows x K tensor of bf16, box (BK, box_rows, 1)
-CUtensorMap make_map(void *base, int rows_pad, int Kp, int box_rows) {
+// planes x rows x K tensor of bf16, box (BK, box_rows, 1); rows beyond `rows` read as zero
+CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t plane_stride) {
     CUtensorMap m;
-    cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows_pad, 2};
-    cuuint64_t strides[2] = {(cuuint64_t)Kp * 2, (cuuint64_t)Kp * 2 * rows_pad};
+    REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, CCSD_GPU_EINVAL, "tensor map base must be 16-byte aligned");
+    cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, 2};
+    cuuint64_t strides[2] = {(cuuint64_t)Kp * 2, (cuuint64_t)plane_stride * 2};
     cuuint32_t box[3] = {BK, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
@@ -305,6 +342,32 @@ CUtensorMap make_map(void *base, int rows_pad, int Kp, int box_rows) {
 }
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// A: rows [0, a_rows) of planes with stride a_plane; the grid covers Mp x Np output tiles.
+template <class Epi>
+void launch_tc(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t Mp,
+               const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t Np, int64_t Kp, const Epi &epi,
+               double issued_flops) {
+    REQUIRE(Mp % BM == 0 && Np % BN == 0 && Kp % BK == 0 && Kp > 0, CCSD_GPU_EINVAL, "tc gemm: bad padding");
+    CU_CHECK(cudaFuncSetAttribute(bf16x3_gemm_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane);
+    CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, BN, b_plane);
+    dim3 grid((unsigned)(Mp / BM), (unsigned)(Np / BN));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ex.prof && ex.prof->on) {
+        CU_CHECK(cudaEventCreate(&e0));
+        CU_CHECK(cudaEventCreate(&e1));
+        CU_CHECK(cudaEventRecord(e0, ex.stream));
+    }
+    bf16x3_gemm_kernel<Epi><<<grid, THREADS, SMEM_BYTES, ex.stream>>>(ta, tb, (int)Kp, epi);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+    if (e0) {
+        CU_CHECK(cudaEventRecord(e1, ex.stream));
+        ex.prof->events.emplace_back(e0, e1);
+        ex.prof->flops.push_back(issued_flops);
+    }
+}
 
 void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
            __nv_bfloat16 *out) {
@@ -319,7 +382,6 @@ void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64
 void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
                 int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc) {
     REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "mixed_gemm: size too large");
-    CU_CHECK(cudaFuncSetAttribute(bf16x3_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, BN);
     DBuf a(sizeof(__nv_bfloat16) * 2 * Mp * Kp, ex.stream), b(sizeof(__nv_bfloat16) * 2 * Np * Kp, ex.stream);
     // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T)
@@ -328,24 +390,41 @@ void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     // B operand rows are output columns: op(B)(kk, c) = B[kk + ldb c] (N) or B[c + ldb kk] (T)
     if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, b.as<__nv_bfloat16>());
     else split(ex, B, 1, ldb, n, k, Np, Kp, b.as<__nv_bfloat16>());
-    CUtensorMap ta = make_map(a.as<void>(), (int)Mp, (int)Kp, BM);
-    CUtensorMap tb = make_map(b.as<void>(), (int)Np, (int)Kp, BN);
-    dim3 grid((unsigned)(Mp / BM), (unsigned)(Np / BN));
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (ex.prof && ex.prof->on) {
-        CU_CHECK(cudaEventCreate(&e0));
-        CU_CHECK(cudaEventCreate(&e1));
-        CU_CHECK(cudaEventRecord(e0, ex.stream));
-    }
-    bf16x3_gemm_kernel<<<grid, THREADS, SMEM_BYTES, ex.stream>>>(ta, tb, (int)m, (int)n, (int)Kp, alpha, beta, C,
-                                                                   (long long)ldc);
-    ex.launches++;
-    CU_CHECK(cudaGetLastError());
-    if (e0) {
-        CU_CHECK(cudaEventRecord(e1, ex.stream));
-        ex.prof->events.emplace_back(e0, e1);
-        ex.prof->flops.push_back(3.0 * 2.0 * double(m) * double(n) * double(k));
-    }
+    EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
+    launch_tc(ex, a.as<__nv_bfloat16>(), Mp, Mp * Kp, Mp, b.as<__nv_bfloat16>(), Np, Np * Kp, Np, Kp, epi,
+              6.0 * double(m) * double(n) * double(k));
+}
+
+int64_t tc_pad_rows_a(int64_t m) { return round_up(m, BM); }
+int64_t tc_pad_rows_b(int64_t n) { return round_up(n, BN); }
+int64_t tc_pad_k(int64_t k) { return round_up(k, BK); }
+
+void split_rows(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
+                __nv_bfloat16 *out) {
+    REQUIRE(Rp % 32 == 0 && Kp % 32 == 0, CCSD_GPU_EINVAL, "split_rows: padding must be a multiple of 32");
+    split(ex, src, sr, sk, R, K, Rp, Kp, out);
+}
+
+void tc_gemm_f64(Exec &ex, const __nv_bfloat16 *A, int64_t Mp, const __nv_bfloat16 *B, int64_t Np, int64_t Kp,
+                 int64_t m, int64_t n, int64_t k_true, double alpha, double beta, double *C, int64_t ldc) {
+    EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
+    launch_tc(ex, A, Mp, Mp * Kp, round_up(m, BM), B, Np, Np * Kp, round_up(n, BN), Kp, epi,
+              6.0 * double(m) * double(n) * double(k_true));
+}
+
+void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,
+                   __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld, int64_t k_true) {
+    EpiPairs epi{};
+    epi.out = out;
+    epi.plane = (size_t)out_rows_pad * (size_t)out_ld;
+    epi.ldk = out_ld;
+    epi.nv = (int)nv;
+    epi.a0 = (int)a0;
+    epi.M = (int)(nv * (a1 - a0));
+    epi.N = (int)(nv * a1);
+    const int64_t r0 = nv * a0;
+    launch_tc(ex, L + r0 * Kp, l_rows - r0, l_rows * Kp, round_up(epi.M, BM), L, l_rows, l_rows * Kp,
+              round_up(epi.N, BN), Kp, epi, 6.0 * double(epi.M) * double(epi.N) * double(k_true));
 }
 
 int mixed_gemm_error_flag(bool reset) {

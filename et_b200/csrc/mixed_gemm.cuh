@@ -1,6 +1,8 @@
 // Split-BF16 ("bf16x3") GEMM on the sm_100a tensor cores (tcgen05 + TMEM + TMA).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace ccsd {
@@ -9,6 +11,27 @@ namespace ccsd {
 // bf16 hi + lo parts; the three products hi*hi + hi*lo + lo*hi accumulate in FP32.
 void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha,
                 const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc);
+
+// Row / K padding of pre-split operands (A rows to 128, B rows to 256, K to 64).
+int64_t tc_pad_rows_a(int64_t m);
+int64_t tc_pad_rows_b(int64_t n);
+int64_t tc_pad_k(int64_t k);
+
+// FP64 strided view (element (r, k) at src[r*sr + k*sk]) -> bf16 hi/lo planes [2][Rp][Kp], zero padded.
+void split_rows(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
+                __nv_bfloat16 *out);
+
+// Tensor-core GEMM on pre-split operands A [2][Mp][Kp], B [2][Np][Kp]:
+// C (m x n, col-major, FP64) = alpha A B^T + beta C.
+void tc_gemm_f64(Exec &ex, const __nv_bfloat16 *A, int64_t Mp, const __nv_bfloat16 *B, int64_t Np, int64_t Kp,
+                 int64_t m, int64_t n, int64_t k_true, double alpha, double beta, double *C, int64_t ldc);
+
+// A2 ladder integrals for a in [a0,a1).  L holds split rows r = c + nv*a (l_rows rows per plane,
+// K = N_J padded to Kp): M_ab[c,d] = sum_J L[c + nv a] L[d + nv b] for b < a1; pairs b <= a are
+// written as split bf16 to out[plane][a(a+1)/2 + b][c + nv*d] (row stride out_ld, plane stride
+// out_rows_pad * out_ld).
+void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,
+                   __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld, int64_t k_true);
 
 // Error code recorded by a tensor-core GEMM whose bounded barrier wait timed out (0 = none).
 int mixed_gemm_error_flag(bool reset);

@@ -96,3 +96,19 @@ def test_mixed_solver_refines_to_fp64_energy():
         res[prec] = e
         gpu.close()
     assert abs(res[MIXED] - res[FP64]) <= 1e-8
+
+
+@pytest.mark.parametrize("batch", [1, 3, 16])
+def test_mixed_ladder_batching(batch):
+    """Tensor-core ladder: any a-batch of the pair-integral GEMM gives the same Omega."""
+    from et_b200 import CCSD, MIXED
+    n_o, n_v, n_J = 5, 19, 33
+    s = make_system(n_o, n_v, n_J, seed=13)
+    ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
+    ref.set_amplitudes(0.05 * np.random.default_rng(2).standard_normal(ref.n_amp))
+    gpu = CCSD(n_o, n_v, n_J, precision=MIXED, mixed_min_flops=1, ladder_batch=batch)
+    gpu.set_system(s.L_mo, s.h_mo, s.eps)
+    gpu.set_amplitudes(ref.get_amplitudes())
+    om, om_ref = gpu.construct_omega(), ref.omega()
+    assert np.linalg.norm(om - om_ref) <= 1e-4 * np.linalg.norm(om_ref)
+    gpu.close()
