@@ -64,10 +64,13 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
 Context::~Context() {
     if (own_stream) cudaStreamSynchronize(own_stream);
     if (ex.stream && ex.stream != own_stream) cudaStreamSynchronize(ex.stream);
-    // buffers are freed (stream-ordered) by their destructors before the stream goes away
-    L_oo.release(); L_ov.release(); L_vo.release(); L_vv.release();
-    Lt_oo.release(); Lt_ov.release(); Lt_vo.release(); Lt_vv.release();
-    h.release(); eps.release(); F.release(); t.release(); epsdiff.release(); scal.release();
+    // every device buffer is freed (stream-ordered) while its stream still exists
+    for (DBuf *b : {&L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
+                    &mbuf})
+        b->release();
+    mbuf_bytes = 0;
+    if (ex.stream) cudaStreamSynchronize(ex.stream);
+    prof.clear();
     if (blas) cublasDestroy(blas);
     if (own_stream) {
         cudaStreamSynchronize(own_stream);
