@@ -480,7 +480,13 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         return std::sqrt(nrm2);
     };
     // FP64 Omega at the current t into omega_v; the correction becomes Omega_fp64 - Omega_mixed
+    bool reset_diis = false;
+    int last_check = 0;
+    std::vector<double> norms;
     auto fp64_check = [&]() {
+        // a refreshed correction changes the residual function: restart the DIIS subspace
+        if (have_corr) reset_diis = true;
+        last_check = it;
         ex.prec = Prec::FP64;
         omega(omega_v.d());
         ex.prec = user;
@@ -504,7 +510,10 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
             if (have_corr) axpby(ex, namp, 1.0, corr.d(), 1.0, omega_v.d());
             nrm = norm_of(omega_v.d());
             bool econv0 = ethr < 0 || std::fabs(e - prev) < ethr;
-            if ((!have_corr && nrm < refine) || (have_corr && nrm < othr && econv0)) {
+            // stalled: no 30% reduction over the last three corrected iterations
+            bool stalled = have_corr && it - last_check > 3 && norms.size() >= 3 &&
+                           nrm > 0.7 * norms[norms.size() - 3];
+            if ((!have_corr && nrm < refine) || (have_corr && nrm < othr && econv0) || stalled) {
                 nrm = fp64_check();
                 exact = true;
             }
@@ -517,6 +526,7 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
             history[2 * (it - 1)] = e;
             history[2 * (it - 1) + 1] = nrm;
         }
+        norms.push_back(nrm);
         bool econv = ethr < 0 || std::fabs(e - prev) < ethr;
         if (exact && nrm < othr && econv) {
             conv = true;
@@ -525,6 +535,10 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         // quasi-Newton step (quasi_newton_updater_class.F90, amplitude_updater_class.F90)
         qn_update(ex, omega_v.d(), epsdiff.d(), t.d(), namp, nt1);
         // diis%update(e = scaled preconditioned residual, x = updated amplitudes)
+        if (reset_diis) {
+            order.clear();
+            reset_diis = false;
+        }
         int slot;
         if ((int)order.size() < dim) {
             slot = (int)order.size();
