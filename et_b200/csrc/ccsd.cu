@@ -380,24 +380,38 @@ void Context::omega(double *om_out) {
         Foo.n[0] = Foo.n[1] = no;
         Fvv.s[0] = Foo.s[0] = 1;
         Fvv.s[1] = Foo.s[1] = nmo;
-        permute_add(ex, 1.0, Fvv, 0.0, tv(X.d(), {nv, nv}));
-        permute_add(ex, 1.0, Foo, 0.0, tv(Y.d(), {no, no}));
-        // X_bc = F_bc - sum_dkl u_bkdl g_ldkc
+        // X_bc = F_bc - sum_dkl u_bkdl g_ldkc and Y_kj = F_kj + sum_cdl g_kdlc u_djcl.  The Fock parts
+        // are large first-order terms: they are applied in FP64 separately so the mixed-precision
+        // rounding only touches the small correlation parts.
+        fill(ex, X.d(), nv * nv, 0.0);
+        fill(ex, Y.d(), no * no, 0.0);
         contract(ex, "bkdl,ldkc->bc", -1.0, V4(u.d()), G4, 1.0, tv(X.d(), {nv, nv}));
         // E2.1 ordered (b,j,a,i)
         contract(ex, "bc,cjai->bjai", 1.0, tv(X.d(), {nv, nv}), V4(tf.d()), 0.0, V4(om.d()));
-        // Y_kj = F_kj + sum_cdl g_kdlc u_djcl
         contract(ex, "kdlc,djcl->kj", 1.0, G4, V4(u.d()), 1.0, tv(Y.d(), {no, no}));
         // E2.2: - sum_k t_aibk Y_kj
         contract(ex, "aibk,kj->aibj", -1.0, V4(tf.d()), tv(Y.d(), {no, no}), 1.0, V4(om.d()));
+        {
+            Prec keep = ex.prec;
+            ex.prec = Prec::FP64;
+            contract(ex, "bc,cjai->bjai", 1.0, Fvv, V4(tf.d()), 1.0, V4(om.d()));
+            contract(ex, "aibk,kj->aibj", -1.0, V4(tf.d()), Foo, 1.0, V4(om.d()));
+            ex.prec = keep;
+        }
     }
     // symmetric_sum (src/tools/reordering.F90:416)
     permute_add(ex, 1.0, V4(om.d()), 0.0, V4(omS.d()));
     permute_add(ex, 1.0, V4s(om.d(), Sb, Sj, Sa, Si), 1.0, V4(omS.d()));
     // omega_ccsd_b2 (omega_ccsd.F90:483-583)
     {
-        contract(ex, "Jai,Jbj->aibj", 1.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_vo.d(), {nJ, nv, no}), 1.0,
-                 V4(omS.d()));
+        {
+            // g_aibj is the zeroth-order source term: FP64 in every precision mode
+            Prec keep = ex.prec;
+            ex.prec = Prec::FP64;
+            contract(ex, "Jai,Jbj->aibj", 1.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_vo.d(), {nJ, nv, no}), 1.0,
+                     V4(omS.d()));
+            ex.prec = keep;
+        }
         DBuf X = dalloc(no * no * no * no, s);
         TV X4 = tv(X.d(), {no, no, no, no});
         contract(ex, "Jki,Jlj->klij", 1.0, tv(Lt_oo.d(), {nJ, no, no}), tv(Lt_oo.d(), {nJ, no, no}), 0.0, X4);
@@ -480,7 +494,7 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         return std::sqrt(nrm2);
     };
     // FP64 Omega at the current t into omega_v; the correction becomes Omega_fp64 - Omega_mixed
-    bool reset_diis = false;
+    bool reset_diis = false, fp64_final = false;
     int last_check = 0;
     std::vector<double> norms;
     auto fp64_check = [&]() {
@@ -501,8 +515,11 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         e = energy();
         double nrm;
         bool exact = !mixed;
-        if (!mixed) {
+        if (!mixed || fp64_final) {
+            exact = true;
+            if (fp64_final) ex.prec = Prec::FP64;
             omega(omega_v.d());
+            ex.prec = user;
             nrm = norm_of(omega_v.d());
         } else {
             omega(om_mixed.d());
@@ -510,12 +527,17 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
             if (have_corr) axpby(ex, namp, 1.0, corr.d(), 1.0, omega_v.d());
             nrm = norm_of(omega_v.d());
             bool econv0 = ethr < 0 || std::fabs(e - prev) < ethr;
-            // stalled: no 30% reduction over the last three corrected iterations
+            // the corrected mixed residual has reached the noise floor of the bf16x3 products when it
+            // stops falling (no 30% reduction over three iterations): finish in FP64
             bool stalled = have_corr && it - last_check > 3 && norms.size() >= 3 &&
                            nrm > 0.7 * norms[norms.size() - 3];
             if ((!have_corr && nrm < refine) || (have_corr && nrm < othr && econv0) || stalled) {
                 nrm = fp64_check();
                 exact = true;
+                if (stalled) {
+                    fp64_final = true;
+                    reset_diis = true;
+                }
             }
         }
         if (!std::isfinite(nrm) || !std::isfinite(e)) {
