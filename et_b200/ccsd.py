@@ -74,6 +74,7 @@ SIGNATURES = {
     "ccsd_gpu_omega_device": (ctypes.c_int, [_VP, _VP]),
     "ccsd_gpu_jacobian": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
     "ccsd_gpu_jacobian_transpose": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
+    "ccsd_gpu_vjp": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
     "ccsd_gpu_solve_gs": (ctypes.c_int, [_VP, ctypes.POINTER(SolverOptions), _DP,
                                          ctypes.POINTER(ctypes.c_int32), _DP]),
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
@@ -226,6 +227,21 @@ class CCSD:
         out = np.empty(self.n_amp * n_vec)
         self._check(self.lib.ccsd_gpu_jacobian_transpose(self.ctx, n_vec, _dp(flat), _dp(out)))
         return out if b.ndim == 1 else out.reshape(self.n_amp, n_vec, order="F")
+
+    def vjp(self, b, *, want_L=False, want_h=False):
+        """b^T dOmega/dt (no D scaling), and optionally b^T dOmega/dL_mo (J,p,q) and b^T dOmega/dh_mo."""
+        b = _f64(b, self.n_amp)
+        dt = np.empty(self.n_amp)
+        dL = np.empty(self.n_J * self.n_mo * self.n_mo) if want_L else None
+        dh = np.empty(self.n_mo * self.n_mo) if want_h else None
+        self._check(self.lib.ccsd_gpu_vjp(self.ctx, _dp(b), _dp(dt), _dp(dL) if want_L else None,
+                                          _dp(dh) if want_h else None))
+        out = [dt]
+        if want_L:
+            out.append(dL.reshape(self.n_J, self.n_mo, self.n_mo, order="F"))
+        if want_h:
+            out.append(dh.reshape(self.n_mo, self.n_mo, order="F"))
+        return out[0] if len(out) == 1 else tuple(out)
 
     def solve_ground_state(self, *, max_iterations=100, diis_dimension=8, omega_threshold=1e-5,
                            energy_threshold=1e-5, refine_threshold=1e-4, raise_on_failure=True):

@@ -137,6 +137,7 @@ int ccsd_gpu_set_h_mo(void *ctx, const double *h, const double *eps, double e_hf
     return guarded(ctx, [&](Context &c) {
         h2d(c, c.h.d(), h, c.nmo * c.nmo);
         h2d(c, c.eps.d(), eps, c.nmo);
+        c.set_h_blocks();
         c.e_hf = e_hf;
         ccsd::orbital_differences(c.ex, c.eps.d(), c.no, c.nv, c.epsdiff.d());
         CU_CHECK(cudaStreamSynchronize(c.ex.stream));
@@ -195,13 +196,39 @@ int ccsd_gpu_omega_device(void *ctx, double *d_omega) {
     });
 }
 
-int ccsd_gpu_jacobian(void *ctx, int64_t, const double *, double *) {
-    return guarded(ctx, [&](Context &) { throw Error(CCSD_GPU_EINVAL, "jacobian transformation not available"); });
+int ccsd_gpu_jacobian(void *ctx, int64_t n_vec, const double *c, double *rho) {
+    return guarded(ctx, [&](Context &x) {
+        REQUIRE(n_vec > 0 && c && rho, CCSD_GPU_EINVAL, "bad jacobian arguments");
+        ccsd::DBuf dc = ccsd::dalloc(x.namp * n_vec, x.ex.stream), dr = ccsd::dalloc(x.namp * n_vec, x.ex.stream);
+        h2d(x, dc.d(), c, x.namp * n_vec);
+        x.jacobian(n_vec, dc.d(), dr.d());
+        d2h(x, rho, dr.d(), x.namp * n_vec);
+    });
 }
 
-int ccsd_gpu_jacobian_transpose(void *ctx, int64_t, const double *, double *) {
-    return guarded(ctx, [&](Context &) {
-        throw Error(CCSD_GPU_EINVAL, "transpose jacobian transformation not available");
+int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, double *sigma) {
+    return guarded(ctx, [&](Context &x) {
+        REQUIRE(n_vec > 0 && b && sigma, CCSD_GPU_EINVAL, "bad transpose arguments");
+        ccsd::DBuf db = ccsd::dalloc(x.namp * n_vec, x.ex.stream), ds = ccsd::dalloc(x.namp * n_vec, x.ex.stream);
+        h2d(x, db.d(), b, x.namp * n_vec);
+        x.jacobian_transpose(n_vec, db.d(), ds.d());
+        d2h(x, sigma, ds.d(), x.namp * n_vec);
+    });
+}
+
+int ccsd_gpu_vjp(void *ctx, const double *b, double *dt, double *dL, double *dh) {
+    return guarded(ctx, [&](Context &x) {
+        REQUIRE(b != nullptr, CCSD_GPU_EINVAL, "null cotangent");
+        cudaStream_t s = x.ex.stream;
+        ccsd::DBuf db = ccsd::dalloc(x.namp, s);
+        h2d(x, db.d(), b, x.namp);
+        ccsd::DBuf ddt = ccsd::dalloc(x.namp, s);
+        ccsd::DBuf ddL = dL ? ccsd::dalloc(x.nJ * x.nmo * x.nmo, s) : ccsd::DBuf();
+        ccsd::DBuf ddh = dh ? ccsd::dalloc(x.nmo * x.nmo, s) : ccsd::DBuf();
+        x.adjoint(db.d(), ddt.d(), dL ? ddL.d() : nullptr, dh ? ddh.d() : nullptr);
+        if (dt) d2h(x, dt, ddt.d(), x.namp);
+        if (dL) d2h(x, dL, ddL.d(), x.nJ * x.nmo * x.nmo);
+        if (dh) d2h(x, dh, ddh.d(), x.nmo * x.nmo);
     });
 }
 

@@ -52,6 +52,10 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     for (auto *b : {&L_vo, &Lt_vo}) *b = dalloc(nJ * nv * no, s);
     for (auto *b : {&L_vv, &Lt_vv}) *b = dalloc(nJ * nv * nv, s);
     h = dalloc(nmo * nmo, s);
+    hb_oo = dalloc(no * no, s);
+    hb_ov = dalloc(no * nv, s);
+    hb_vo = dalloc(nv * no, s);
+    hb_vv = dalloc(nv * nv, s);
     eps = dalloc(nmo, s);
     F = dalloc(nmo * nmo, s);
     t = dalloc(namp, s);
@@ -66,7 +70,7 @@ Context::~Context() {
     if (ex.stream && ex.stream != own_stream) cudaStreamSynchronize(ex.stream);
     // every device buffer is freed (stream-ordered) while its stream still exists
     for (DBuf *b : {&L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
-                    &mbuf})
+                    &mbuf, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
         b->release();
     mbuf_bytes = 0;
     if (ex.stream) cudaStreamSynchronize(ex.stream);
@@ -147,6 +151,23 @@ void Context::construct_fock() {
              blk(Fm, no, no, nv, nv));
 }
 
+void Context::set_h_blocks() {
+    auto blk = [&](int64_t r0, int64_t c0, int64_t nr, int64_t nc, double *dst) {
+        TV v;
+        v.p = h.d() + r0 + nmo * c0;
+        v.nd = 2;
+        v.n[0] = nr;
+        v.n[1] = nc;
+        v.s[0] = 1;
+        v.s[1] = nmo;
+        permute_add(ex, 1.0, v, 0.0, tv(dst, {nr, nc}));
+    };
+    blk(0, 0, no, no, hb_oo.d());
+    blk(0, no, no, nv, hb_ov.d());
+    blk(no, 0, nv, no, hb_vo.d());
+    blk(no, no, nv, nv, hb_vv.d());
+}
+
 void Context::refresh() {
     REQUIRE(have_L && have_h, CCSD_GPU_ESTATE, "Cholesky vectors and h must be set first");
     Prec keep = ex.prec;
@@ -196,9 +217,9 @@ void Context::mp2_guess() {
 // A2 ladder: Omega^ab_ij += sum_cd g_acbd t^cd_ij with the +/- symmetrisation of
 // omega_ccsd_a2 (src/wavefunctions/ccsd/omega_ccsd.F90:113-480), batched over a.
 // ---------------------------------------------------------------------------
-void Context::ladder(const double *t2, double *om2) {
+void Context::ladder(const double *Lvv, const double *t2, double *om2) {
     if (ex.prec == Prec::MIXED) {
-        ladder_tc(t2, om2);
+        ladder_tc(Lvv, t2, om2);
         return;
     }
     cudaStream_t s = ex.stream;
@@ -209,7 +230,7 @@ void Context::ladder(const double *t2, double *om2) {
     // L~_vv as (J, c, a): columns (c, a) of one a-block are contiguous
     DBuf LT = dalloc(nJ * nv * nv, s);
     {
-        TV src = tv(Lt_vv.d(), {nJ, nv, nv});   // [J, a, c]
+        TV src = tv(Lvv, {nJ, nv, nv});   // [J, a, c]
         TV dst;
         dst.p = LT.d();
         dst.nd = 3;
@@ -257,7 +278,7 @@ void Context::ladder(const double *t2, double *om2) {
 //   omega-_ij,ab = sum_cd 1/2 (t_cidj - t_cjdi) M_ab[c,d]
 // so the split-bf16 integrals M_ab (written by the G GEMM epilogue, all pairs b <= a resident
 // in HBM) meet [T+; T-] in one GEMM of N = n_o^2 and K = n_v^2.
-void Context::ladder_tc(const double *t2, double *om2) {
+void Context::ladder_tc(const double *Lvv, const double *t2, double *om2) {
     cudaStream_t s = ex.stream;
     const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
     const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
@@ -267,7 +288,7 @@ void Context::ladder_tc(const double *t2, double *om2) {
     {
         // r = c + nv a  ->  offset nJ*(a + nv*c): not a single stride, so split from the (J, c, a) copy
         DBuf LT = dalloc(nJ * nv2, s);
-        TV src = tv(Lt_vv.d(), {nJ, nv, nv});   // [J, a, c]
+        TV src = tv(Lvv, {nJ, nv, nv});   // [J, a, c]
         TV dst;
         dst.p = LT.d();
         dst.nd = 3;
@@ -300,156 +321,6 @@ void Context::ladder_tc(const double *t2, double *om2) {
                 W.d(), nab);
     add_omega_T(ex, om2, W.d(), nab, no, nv);
     ex.flops += double(nv2) * double(nv2 + 1) * double(nJ) + 2.0 * double(nab) * double(nrow) * double(nv2);
-}
-
-// ---------------------------------------------------------------------------
-// construct_omega_ccsd (src/wavefunctions/ccsd/omega_ccsd.F90:39-110)
-// ---------------------------------------------------------------------------
-void Context::omega(double *om_out) {
-    REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
-    cudaStream_t s = ex.stream;
-    const double *t1 = t.d(), *t2 = t.d() + nt1;
-    double *om1 = om_out, *om2 = om_out + nt1;
-    const int64_t N4 = nov * nov;
-    auto V4 = [&](const double *p) { return tv(p, {nv, no, nv, no}); };
-    // view of x[a,i,b,j] as y[a,i,b,j] = x[P(a,i,b,j)] for the permutation given by strides
-    auto V4s = [&](const double *p, int64_t sa, int64_t si, int64_t sb, int64_t sj) {
-        TV v = tv(p, {nv, no, nv, no});
-        v.s[0] = sa;
-        v.s[1] = si;
-        v.s[2] = sb;
-        v.s[3] = sj;
-        return v;
-    };
-    const int64_t Sa = 1, Si = nv, Sb = nov, Sj = nov * nv;   // strides of a (v,o,v,o) array
-
-    // omega_ccs_a1 (src/wavefunctions/ccs/omega_ccs.F90:62): Omega_ai = F_ai
-    {
-        TV Fvo;
-        Fvo.p = F.d() + no;
-        Fvo.nd = 2;
-        Fvo.n[0] = nv;
-        Fvo.n[1] = no;
-        Fvo.s[0] = 1;
-        Fvo.s[1] = nmo;
-        permute_add(ex, 1.0, Fvo, 0.0, tv(om1, {nv, no}));
-    }
-    DBuf tf = dalloc(N4, s), u = dalloc(N4, s);
-    squareup(ex, t2, tf.d(), nov);
-    // u_aibj = 2 t_aibj - t_ajbi (construct_u_aibj_ccsd, omega_ccsd.F90:881-914)
-    permute_add(ex, 2.0, V4(tf.d()), 0.0, V4(u.d()));
-    permute_add(ex, -1.0, V4s(tf.d(), Sa, Sj, Sb, Si), 1.0, V4(u.d()));
-
-    TV OM1 = tv(om1, {nv, no});
-    // omega_doubles_a1 (src/wavefunctions/doubles/omega_doubles.F90:36-138)
-    {
-        DBuf X = dalloc(nJ * nov, s);
-        contract(ex, "Jcj,cjbi->Jbi", 1.0, tv(L_vo.d(), {nJ, nv, no}), V4(u.d()), 0.0, tv(X.d(), {nJ, nv, no}));
-        contract(ex, "Jab,Jbi->ai", 1.0, tv(Lt_vv.d(), {nJ, nv, nv}), tv(X.d(), {nJ, nv, no}), 1.0, OM1);
-    }
-    // omega_doubles_b1 (:141-204): - sum_jbk u_ajbk g_kbji
-    {
-        DBuf g = dalloc(nov * no * no, s);
-        contract(ex, "Jkb,Jji->kbji", 1.0, tv(Lt_ov.d(), {nJ, no, nv}), tv(Lt_oo.d(), {nJ, no, no}), 0.0,
-                 tv(g.d(), {no, nv, no, no}));
-        contract(ex, "ajbk,kbji->ai", -1.0, V4(u.d()), tv(g.d(), {no, nv, no, no}), 1.0, OM1);
-    }
-    // omega_doubles_c1 (:207-258): sum_bj u_aibj F_jb
-    {
-        TV Fov;
-        Fov.p = F.d() + nmo * no;
-        Fov.nd = 2;
-        Fov.n[0] = no;
-        Fov.n[1] = nv;
-        Fov.s[0] = 1;
-        Fov.s[1] = nmo;
-        contract(ex, "aibj,jb->ai", 1.0, V4(u.d()), Fov, 1.0, OM1);
-    }
-
-    DBuf gov = g_ovov();                 // g[l,d,k,c] = g_ldkc, shared by E2, B2, C2/D2
-    TV G4 = tv(gov.d(), {no, nv, no, nv});
-    DBuf om = dalloc(N4, s), omS = dalloc(N4, s);
-    // omega_ccsd_e2 (omega_ccsd.F90:712-878)
-    {
-        DBuf X = dalloc(nv * nv, s), Y = dalloc(no * no, s);
-        TV Fvv, Foo;
-        Fvv.p = F.d() + no + nmo * no;
-        Foo.p = F.d();
-        Fvv.nd = Foo.nd = 2;
-        Fvv.n[0] = Fvv.n[1] = nv;
-        Foo.n[0] = Foo.n[1] = no;
-        Fvv.s[0] = Foo.s[0] = 1;
-        Fvv.s[1] = Foo.s[1] = nmo;
-        // X_bc = F_bc - sum_dkl u_bkdl g_ldkc and Y_kj = F_kj + sum_cdl g_kdlc u_djcl.  The Fock parts
-        // are large first-order terms: they are applied in FP64 separately so the mixed-precision
-        // rounding only touches the small correlation parts.
-        fill(ex, X.d(), nv * nv, 0.0);
-        fill(ex, Y.d(), no * no, 0.0);
-        contract(ex, "bkdl,ldkc->bc", -1.0, V4(u.d()), G4, 1.0, tv(X.d(), {nv, nv}));
-        // E2.1 ordered (b,j,a,i)
-        contract(ex, "bc,cjai->bjai", 1.0, tv(X.d(), {nv, nv}), V4(tf.d()), 0.0, V4(om.d()));
-        contract(ex, "kdlc,djcl->kj", 1.0, G4, V4(u.d()), 1.0, tv(Y.d(), {no, no}));
-        // E2.2: - sum_k t_aibk Y_kj
-        contract(ex, "aibk,kj->aibj", -1.0, V4(tf.d()), tv(Y.d(), {no, no}), 1.0, V4(om.d()));
-        {
-            Prec keep = ex.prec;
-            ex.prec = Prec::FP64;
-            contract(ex, "bc,cjai->bjai", 1.0, Fvv, V4(tf.d()), 1.0, V4(om.d()));
-            contract(ex, "aibk,kj->aibj", -1.0, V4(tf.d()), Foo, 1.0, V4(om.d()));
-            ex.prec = keep;
-        }
-    }
-    // symmetric_sum (src/tools/reordering.F90:416)
-    permute_add(ex, 1.0, V4(om.d()), 0.0, V4(omS.d()));
-    permute_add(ex, 1.0, V4s(om.d(), Sb, Sj, Sa, Si), 1.0, V4(omS.d()));
-    // omega_ccsd_b2 (omega_ccsd.F90:483-583)
-    {
-        {
-            // g_aibj is the zeroth-order source term: FP64 in every precision mode
-            Prec keep = ex.prec;
-            ex.prec = Prec::FP64;
-            contract(ex, "Jai,Jbj->aibj", 1.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_vo.d(), {nJ, nv, no}), 1.0,
-                     V4(omS.d()));
-            ex.prec = keep;
-        }
-        DBuf X = dalloc(no * no * no * no, s);
-        TV X4 = tv(X.d(), {no, no, no, no});
-        contract(ex, "Jki,Jlj->klij", 1.0, tv(Lt_oo.d(), {nJ, no, no}), tv(Lt_oo.d(), {nJ, no, no}), 0.0, X4);
-        contract(ex, "kcld,cidj->klij", 1.0, G4, V4(tf.d()), 1.0, X4);
-        contract(ex, "akbl,klij->aibj", 1.0, V4(tf.d()), X4, 1.0, V4(omS.d()));
-    }
-    // omega_ccsd_c2_d2 (omega_ccsd.F90:586-709), eT's DSYMM sequence written as contractions
-    {
-        DBuf C = dalloc(N4, s), D = dalloc(N4, s);
-        TV C4 = V4(C.d()), D4 = V4(D.d());
-        contract(ex, "Jac,Jkj->ckaj", 1.0, tv(Lt_vv.d(), {nJ, nv, nv}), tv(Lt_oo.d(), {nJ, no, no}), 0.0, C4);
-        permute_add(ex, -1.0, C4, 0.0, D4);
-        contract(ex, "Jai,Jkc->ckai", 2.0, tv(Lt_vo.d(), {nJ, nv, no}), tv(Lt_ov.d(), {nJ, no, nv}), 1.0, D4);
-        // C_claj -= 1/2 sum_dk g_kcld t_djak        (dsymm 'R','U', -1/2)
-        contract(ex, "kcld,djak->claj", -0.5, G4, V4(tf.d()), 1.0, C4);
-        // D_claj += 1/2 sum_dk (2 g_lckd - g_kcld) u_dkaj   (contra + dsymm 'R','L', +1/2)
-        contract(ex, "lckd,dkaj->claj", 1.0, G4, V4(u.d()), 1.0, D4);
-        contract(ex, "kcld,dkaj->claj", -0.5, G4, V4(u.d()), 1.0, D4);
-        // x = -3/2 sum_ck t_akci C_ckbj  (dsymm 'L','U'); w = 1/2 sum_ck u_aick D_ckbj (dsymm 'L','L')
-        DBuf x = std::move(om);   // reuse
-        contract(ex, "akci,ckbj->aibj", -1.5, V4(tf.d()), C4, 0.0, V4(x.d()));
-        DBuf w = std::move(C);
-        contract(ex, "aick,ckbj->aibj", 0.5, V4(u.d()), D4, 0.0, V4(w.d()));
-        // symmetrize_and_pack(contra, psrq): (x + 2 x_psrq)/3 ; then P(w)
-        permute_add(ex, 1.0 / 3.0, V4(x.d()), 1.0, V4(w.d()));
-        permute_add(ex, 2.0 / 3.0, V4s(x.d(), Sa, Sj, Sb, Si), 1.0, V4(w.d()));
-        permute_add(ex, 1.0, V4(w.d()), 1.0, V4(omS.d()));
-        permute_add(ex, 1.0, V4s(w.d(), Sb, Sj, Sa, Si), 1.0, V4(omS.d()));
-    }
-    // scale_diagonal(1/2) + packin
-    fill(ex, om2, nt2, 0.0);
-    pack_half_diag_add(ex, 1.0, omS.d(), om2, nov);
-    // omega_ccsd_a2
-    ladder(t2, om2);
-    if (ex.prec == Prec::MIXED) {
-        CU_CHECK(cudaStreamSynchronize(s));
-        REQUIRE(mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM barrier wait timed out");
-    }
 }
 
 // ---------------------------------------------------------------------------

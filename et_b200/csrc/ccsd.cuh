@@ -7,6 +7,13 @@
 
 namespace ccsd {
 
+class Graph;
+
+// node ids of the recorded residual
+struct OmegaNodes {
+    int t1, t2, L_oo, L_ov, L_vo, L_vv, h_oo, h_ov, h_vo, h_vv, Lt_vv, om1, om2;
+};
+
 struct Context {
     int64_t no, nv, nJ, nmo, nov, nt1, nt2, namp;
     int device = 0;
@@ -23,6 +30,7 @@ struct Context {
     DBuf L_oo, L_ov, L_vo, L_vv;
     DBuf Lt_oo, Lt_ov, Lt_vo, Lt_vv;
     DBuf h, eps, F;          // h_mo, orbital energies, T1 Fock (n_mo x n_mo)
+    DBuf hb_oo, hb_ov, hb_vo, hb_vv;   // MO h in o/v blocks
     DBuf t;                  // [t1 | packed t2]
     DBuf epsdiff;            // orbital differences (n_amp)
     DBuf scal;               // scalar scratch
@@ -40,8 +48,16 @@ struct Context {
     double energy();
     void mp2_guess();
     void omega(double *d_omega);
-    void ladder(const double *t2, double *om2);
-    void ladder_tc(const double *t2, double *om2);
+    OmegaNodes record_omega(Graph &g);
+    void record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv_in, int tf);
+    void ladder_y(const double *Lvv, const double *tfull, double *Y);
+    void jacobian(int64_t nvec, const double *c, double *rho);
+    void jacobian_transpose(int64_t nvec, const double *b, double *sigma);
+    void adjoint(const double *b, double *dt, double *dL, double *dh);
+    void set_h_blocks();
+    // A2 ladder: om2 += ladder(L_vv in (J, a, c) layout, packed t2)
+    void ladder(const double *Lvv, const double *t2, double *om2);
+    void ladder_tc(const double *Lvv, const double *t2, double *om2);
     int solve_gs(const ccsd_gpu_solver_options *o, double *energy, int32_t *iters, double *history);
     double omega_flops() const;
 };

@@ -116,6 +116,13 @@ int ccsd_gpu_jacobian(void *ctx, int64_t n_vec, const double *c, double *rho);
  * sigma_k = b_k^T A. */
 int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, double *sigma);
 
+/* Vector-Jacobian product of the residual: given a cotangent b (n_t1 + n_t2), returns
+ *   dt = (dOmega/dt)^T b                      (n_t1 + n_t2; sigma = D dt with D = 2 on the doubles diagonal),
+ *   dL = (dOmega/dL_mo)^T b  (nullable)       ((J, p, q) over the full MO range, as ccsd_gpu_set_cholesky_mo),
+ *   dh = (dOmega/dh_mo)^T b  (nullable)       (n_mo x n_mo).
+ * No eT routine returns the L and h parts; they are the density-like contributions of the adjoint. */
+int ccsd_gpu_vjp(void *ctx, const double *b, double *dt, double *dL, double *dh);
+
 /* run_diis_cc_gs (src/solvers/cc/diis_cc_gs_class.F90:209-315) with the quasi-Newton updater,
  * entirely on the device.  On exit the context holds the final amplitudes; history (nullable)
  * receives max_iterations pairs (E, |Omega|). */

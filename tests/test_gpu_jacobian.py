@@ -1,0 +1,122 @@
+"""Jacobian transformation, its transpose and the adjoint into L and h against the CPU oracle."""
+
+import numpy as np
+import pytest
+
+from et_b200.synthetic import make_system
+from oracle import ccsd as oc
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(n_o, n_v, n_J, seed=3, scale=0.05):
+    from et_b200 import CCSD
+    s = make_system(n_o, n_v, n_J, seed=seed)
+    ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
+    amp = scale * np.random.default_rng(seed + 5).standard_normal(ref.n_amp)
+    ref.set_amplitudes(amp)
+    gpu = CCSD(n_o, n_v, n_J)
+    gpu.set_system(s.L_mo, s.h_mo, s.eps)
+    gpu.set_amplitudes(amp)
+    return s, ref, gpu, amp
+
+
+@pytest.mark.parametrize("dims", [(2, 5, 9), (3, 8, 20), (5, 13, 30)])
+def test_jacobian_matches_oracle(dims):
+    s, ref, gpu, amp = _setup(*dims)
+    rng = np.random.default_rng(1)
+    for _ in range(2):
+        c = rng.standard_normal(ref.n_amp)
+        rho = gpu.jacobian_transformation(c)
+        rho_ref = ref.jacobian_transformation(c)
+        assert np.abs(rho - rho_ref).max() <= 1e-11 * max(1.0, np.abs(rho_ref).max())
+    gpu.close()
+
+
+def test_jacobian_block_of_trials():
+    """n_vec trial vectors in one call equal n_vec single calls."""
+    s, ref, gpu, amp = _setup(3, 9, 21)
+    C = np.random.default_rng(2).standard_normal((ref.n_amp, 5))
+    R = gpu.jacobian_transformation(C)
+    for k in range(5):
+        assert np.abs(R[:, k] - ref.jacobian_transformation(C[:, k])).max() < 1e-11 * max(1, np.abs(R).max())
+    gpu.close()
+
+
+def test_transpose_matches_dense_oracle():
+    s, ref, gpu, amp = _setup(2, 6, 12)
+    A = ref.jacobian_matrix()
+    B = np.random.default_rng(3).standard_normal((ref.n_amp, 3))
+    S = gpu.jacobian_transpose_transformation(B)
+    assert np.abs(S - A.T @ B).max() <= 1e-11 * max(1.0, np.abs(A).max())
+    gpu.close()
+
+
+@pytest.mark.parametrize("dims", [(4, 12, 30), (6, 24, 60)])
+def test_transpose_dot_identity(dims):
+    """<b, A c> == <A^T b, c> for random b, c (size-independent property)."""
+    s, ref, gpu, amp = _setup(*dims)
+    rng = np.random.default_rng(4)
+    b, c = rng.standard_normal(ref.n_amp), rng.standard_normal(ref.n_amp)
+    lhs = b @ gpu.jacobian_transformation(c)
+    rhs = gpu.jacobian_transpose_transformation(b) @ c
+    assert abs(lhs - rhs) <= 1e-11 * max(1.0, abs(lhs))
+    gpu.close()
+
+
+def _omega_complex(L, h, amp, n_o):
+    n_v = h.shape[0] - n_o
+    n_t1 = n_o * n_v
+    t1 = amp[:n_t1].reshape(n_v, n_o, order="F")
+    L_t1 = oc.construct_t1_cholesky(L, t1, n_o)
+    F = oc.construct_fock(h, L_t1, t1, n_o)
+    return oc.omega_ccsd(t1, amp[n_t1:], L, L_t1, F, n_o)
+
+
+def test_adjoint_into_cholesky_vectors_and_h():
+    """<dL, dL_dir> + <dh, dh_dir> == b^T (dOmega/d(L,h))(dir) by complex-step differentiation."""
+    s, ref, gpu, amp = _setup(3, 7, 15)
+    rng = np.random.default_rng(6)
+    b = rng.standard_normal(ref.n_amp)
+    dt, dL, dh = gpu.vjp(b, want_L=True, want_h=True)
+    # amplitude part: D (dOmega/dt)^T b is the transpose transformation
+    sig = gpu.jacobian_transpose_transformation(b)
+    assert np.abs(dt * ref.diag_scaling() - sig).max() < 1e-11 * max(1.0, np.abs(sig).max())
+    dLdir = rng.standard_normal(s.L_mo.shape)
+    dhdir = rng.standard_normal(s.h_mo.shape)
+    hstep = 1e-30
+    om_L = _omega_complex(s.L_mo + 1j * hstep * dLdir, s.h_mo.astype(complex), amp, s.n_o)
+    om_h = _omega_complex(s.L_mo.astype(complex), s.h_mo + 1j * hstep * dhdir, amp, s.n_o)
+    ref_L = b @ (np.imag(om_L) / hstep)
+    ref_h = b @ (np.imag(om_h) / hstep)
+    assert abs(np.sum(dL * dLdir) - ref_L) <= 1e-10 * max(1.0, abs(ref_L))
+    assert abs(np.sum(dh * dhdir) - ref_h) <= 1e-10 * max(1.0, abs(ref_h))
+    gpu.close()
+
+
+def test_excitation_energies_match_et(h2o_he):
+    """Davidson on the CPU using the GPU Jacobian reproduces eT's EOM-CCSD roots (H2O+He)."""
+    from et_b200 import CCSD
+    from oracle import frontend as fe
+    d = h2o_he
+    n_J, n_o = d["L_mo"].shape[0], d["n_o"]
+    gpu = CCSD(n_o, d["h_mo"].shape[0] - n_o, n_J)
+    gpu.set_system(d["L_mo"], d["h_mo"], d["eps"], d["e_hf"])
+    gpu.set_initial_amplitudes_guess()
+    gpu.solve_ground_state(omega_threshold=1e-11, energy_threshold=1e-12)
+
+    class GpuA:
+        def __init__(self):
+            s = oc.CCSDSystem(d["L_mo"], d["h_mo"], d["eps"], n_o, d["e_hf"])
+            self.n_amp, self._eps = s.n_amp, s.orbital_differences()
+
+        def orbital_differences(self):
+            return self._eps
+
+        def jacobian_transformation(self, c):
+            return gpu.jacobian_transformation(c)
+
+    w, _, _ = oc.davidson_right(GpuA(), 2, threshold=1e-9)
+    ref = fe.golden_values()["ccsd_right_es_energies"]["excitation_energies"]
+    assert np.allclose(w, ref, atol=1e-10)
+    gpu.close()
