@@ -83,6 +83,8 @@ SIGNATURES = {
     "ccsd_gpu_selftest_gemm": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I64, _I64,
                                               _I64, ctypes.c_double, _DP, _I64, _DP, _I64, ctypes.c_double, _DP,
                                               _I64]),
+    "ccsd_gpu_mixed_gemm_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _I64, _I64, _I64, ctypes.c_double,
+                                                   _VP, _I64, _VP, _I64, ctypes.c_double, _VP, _I64, _VP]),
     "ccsd_gpu_omega_flops": (ctypes.c_double, [_VP]),
 }
 

@@ -289,6 +289,24 @@ int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t tra
     });
 }
 
+int ccsd_gpu_mixed_gemm_noalloc(int32_t transA, int32_t transB, int64_t m, int64_t n, int64_t k, double alpha,
+                                const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C,
+                                int64_t ldc, void *stream) {
+    try {
+        ccsd::mixed_gemm_noalloc(transA != 0, transB != 0, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                 static_cast<cudaStream_t>(stream));
+        CU_CHECK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+        REQUIRE(ccsd::mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM wait timed out");
+        return CCSD_GPU_OK;
+    } catch (const Error &e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return CCSD_GPU_ECUDA;
+    }
+}
+
 double ccsd_gpu_omega_flops(void *ctx) {
     if (!ctx) return 0.0;
     return static_cast<Context *>(ctx)->omega_flops();

@@ -437,4 +437,62 @@ int mixed_gemm_error_flag(bool reset) {
     return v;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the split-BF16 GEMM.
+//
+// Some callers cannot allocate device memory when they call in: a host program that has handed the
+// whole GPU to its own memory pool up front (a Fortran driver that reserved HBM for its arrays, a
+// framework whose caching allocator owns the device), or a code path that must not trigger the
+// device-wide synchronisation a cudaMalloc/cudaFree can cause.  For them the operand split planes
+// live in a fixed file-scope device array instead of stream-ordered allocations.
+// ---------------------------------------------------------------------------
+
+// bf16 elements of the fixed split scratch: hi and lo planes of A (Mp x Kp) and of B (Np x Kp)
+constexpr int64_t NOALLOC_SCRATCH_ELEMS = 8ll << 20;   // 16 MiB, held by every GPU that loads the library
+static __device__ __align__(256) __nv_bfloat16 g_noalloc_split[NOALLOC_SCRATCH_ELEMS];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[128] = {};   // device address of g_noalloc_split, per device ordinal
+}  // namespace
+
+// Device address of the scratch for the current device (looked up once per device; the first call
+// on a device does this set-up).
+static __nv_bfloat16 *noalloc_scratch() {
+    int dev = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    REQUIRE(dev >= 0 && dev < 128, CCSD_GPU_EINVAL, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_split);
+        REQUIRE(rc == cudaSuccess && p != nullptr, CCSD_GPU_ECUDA,
+                std::string("cudaGetSymbolAddress of the no-alloc scratch failed: ") + cudaGetErrorString(rc));
+        g_noalloc_ptr[dev] = p;
+    }
+    return static_cast<__nv_bfloat16 *>(g_noalloc_ptr[dev]);
+}
+
+void mixed_gemm_noalloc(bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
+                        int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc,
+                        cudaStream_t stream) {
+    REQUIRE(m > 0 && n > 0 && k > 0 && A && B && C, CCSD_GPU_EINVAL, "bad gemm arguments");
+    REQUIRE(lda >= (transA ? k : m) && ldb >= (transB ? n : k) && ldc >= m, CCSD_GPU_EINVAL, "bad leading dimension");
+    const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, BN);
+    const int64_t need = 2 * (Mp + Np) * Kp;
+    REQUIRE(need <= NOALLOC_SCRATCH_ELEMS, CCSD_GPU_EINVAL,
+            "no-alloc GEMM: 2 x (round_up(m,128) + round_up(n,256)) x round_up(k,64) = " + std::to_string(need) +
+                " bf16 elements exceeds the fixed scratch of " + std::to_string(NOALLOC_SCRATCH_ELEMS));
+    __nv_bfloat16 *scratch = noalloc_scratch();
+    Exec ex;
+    ex.stream = stream;
+    __nv_bfloat16 *a = scratch, *b = scratch + 2 * Mp * Kp;
+    if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, a);
+    else split(ex, A, lda, 1, m, k, Mp, Kp, a);
+    if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, b);
+    else split(ex, B, 1, ldb, n, k, Np, Kp, b);
+    EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
+    launch_tc(ex, a, Mp, Mp * Kp, Mp, b, Np, Np * Kp, Np, Kp, epi, 6.0 * double(m) * double(n) * double(k));
+}
+
 }  // namespace ccsd

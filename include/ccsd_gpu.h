@@ -144,6 +144,22 @@ int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t tra
                            int64_t k, double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
                            double beta, double *C, int64_t ldc);
 
+/* Allocation-free split-BF16 tensor-core GEMM; no counterpart in eT.
+ * C (m x n, column-major, device) = alpha op(A) op(B) + beta C with A, B, C device pointers on the
+ * current device, run on `stream` (a cudaStream_t as void*, NULL = legacy default stream); returns
+ * after the stream has finished the product.  It is for callers that cannot allocate device memory
+ * when they call in (a host program that reserved the whole GPU for its own pool, or a code path
+ * that must avoid the synchronisation of cudaMalloc/cudaFree): it makes no cudaMalloc/cudaFree or
+ * other allocating call.  Its scratch is a fixed 16 MiB device array inside the library (held by
+ * every GPU that loads it): 2 x (round_up(m,128) + round_up(n,256)) x round_up(k,64) must not exceed
+ * 8388608, larger sizes are rejected with CCSD_GPU_EINVAL.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.  All calls share the
+ * array, so calls that overlap on the GPU (e.g. on two streams) race; serialise them.  Errors are
+ * reported through ccsd_gpu_last_error(NULL). */
+int ccsd_gpu_mixed_gemm_noalloc(int32_t transA, int32_t transB, int64_t m, int64_t n, int64_t k, double alpha,
+                                const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C,
+                                int64_t ldc, void *stream);
+
 /* Algorithmic flop count of one Omega at this context's dimensions, summed over eT's own BLAS
  * call sites (2mnk per DGEMM, n(n+1)k per DSFRK). */
 double ccsd_gpu_omega_flops(void *ctx);
