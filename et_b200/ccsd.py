@@ -43,6 +43,12 @@ class Options(ctypes.Structure):
                 ("mixed_min_flops", ctypes.c_int64), ("reserved", ctypes.c_int64 * 5)]
 
 
+class DavidsonOptions(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_int32), ("block", ctypes.c_int32), ("max_reduced_dim", ctypes.c_int32),
+                ("reserved0", ctypes.c_int32), ("residual_threshold", ctypes.c_double),
+                ("energy_threshold", ctypes.c_double), ("reserved", ctypes.c_int32 * 8)]
+
+
 class SolverOptions(ctypes.Structure):
     _fields_ = [("max_iterations", ctypes.c_int32), ("diis_dimension", ctypes.c_int32),
                 ("omega_threshold", ctypes.c_double), ("energy_threshold", ctypes.c_double),
@@ -75,6 +81,8 @@ SIGNATURES = {
     "ccsd_gpu_jacobian": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
     "ccsd_gpu_jacobian_transpose": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
     "ccsd_gpu_vjp": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
+    "ccsd_gpu_eom_davidson": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(DavidsonOptions), _DP,
+                                             _DP, ctypes.POINTER(ctypes.c_int32)]),
     "ccsd_gpu_solve_gs": (ctypes.c_int, [_VP, ctypes.POINTER(SolverOptions), _DP,
                                          ctypes.POINTER(ctypes.c_int32), _DP]),
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
@@ -244,6 +252,18 @@ class CCSD:
         if want_h:
             out.append(dh.reshape(self.n_mo, self.n_mo, order="F"))
         return out[0] if len(out) == 1 else tuple(out)
+
+    def excited_states(self, n_states, *, left=False, max_iterations=100, block=0, max_reduced_dim=0,
+                       residual_threshold=1e-6, energy_threshold=1e-6, vectors=False):
+        """eigen_davidson_solver on the device: (omegas, vectors or None, iterations)."""
+        opt = DavidsonOptions(max_iterations=max_iterations, block=block, max_reduced_dim=max_reduced_dim,
+                              residual_threshold=residual_threshold, energy_threshold=energy_threshold)
+        om = np.zeros(n_states)
+        vec = np.zeros(self.n_amp * n_states) if vectors else None
+        it = ctypes.c_int32()
+        self._check(self.lib.ccsd_gpu_eom_davidson(self.ctx, n_states, int(bool(left)), ctypes.byref(opt), _dp(om),
+                                                   _dp(vec) if vectors else None, ctypes.byref(it)))
+        return om, (vec.reshape(self.n_amp, n_states, order="F") if vectors else None), it.value
 
     def solve_ground_state(self, *, max_iterations=100, diis_dimension=8, omega_threshold=1e-5,
                            energy_threshold=1e-5, refine_threshold=1e-4, raise_on_failure=True):

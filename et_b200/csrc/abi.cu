@@ -232,6 +232,21 @@ int ccsd_gpu_vjp(void *ctx, const double *b, double *dt, double *dL, double *dh)
     });
 }
 
+int ccsd_gpu_eom_davidson(void *ctx, int32_t n_states, int32_t side, const ccsd_gpu_davidson_options *opt,
+                          double *omega, double *vectors, int32_t *iterations) {
+    int status = CCSD_GPU_OK;
+    int rc = guarded(ctx, [&](Context &c) {
+        REQUIRE(side == 0 || side == 1, CCSD_GPU_EINVAL, "side must be 0 (right) or 1 (left)");
+        REQUIRE(omega != nullptr, CCSD_GPU_EINVAL, "null omega");
+        ccsd::DBuf dv = vectors ? ccsd::dalloc(c.namp * n_states, c.ex.stream) : ccsd::DBuf();
+        status = c.davidson(n_states, side, opt, omega, vectors ? dv.d() : nullptr, iterations);
+        if (vectors) d2h(c, vectors, dv.d(), c.namp * n_states);
+    });
+    if (rc != CCSD_GPU_OK) return rc;
+    if (status != CCSD_GPU_OK) static_cast<Context *>(ctx)->err = "Davidson did not converge";
+    return status;
+}
+
 int ccsd_gpu_solve_gs(void *ctx, const ccsd_gpu_solver_options *opt, double *energy, int32_t *iterations,
                       double *history) {
     int status = CCSD_GPU_OK;

@@ -58,6 +58,8 @@ struct Context {
     // A2 ladder: om2 += ladder(L_vv in (J, a, c) layout, packed t2)
     void ladder(const double *Lvv, const double *t2, double *om2);
     void ladder_tc(const double *Lvv, const double *t2, double *om2);
+    int davidson(int nstates, int side, const ccsd_gpu_davidson_options *o, double *omega_out, double *vectors_out,
+                 int32_t *iters_out);
     int solve_gs(const ccsd_gpu_solver_options *o, double *energy, int32_t *iters, double *history);
     double omega_flops() const;
 };

@@ -123,6 +123,23 @@ int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, doubl
  * No eT routine returns the L and h parts; they are the density-like contributions of the adjoint. */
 int ccsd_gpu_vjp(void *ctx, const double *b, double *dt, double *dL, double *dh);
 
+typedef struct ccsd_gpu_davidson_options {
+    int32_t max_iterations;      /* default 100 */
+    int32_t block;               /* trial vectors per batched transformation (0 = by memory) */
+    int32_t max_reduced_dim;     /* default max(100, 10 n_states), as eT (cc_es_amplitudes_solver_factory_class.F90:307) */
+    int32_t reserved0;
+    double residual_threshold;   /* |A x - w x| */
+    double energy_threshold;     /* |w - w_previous| */
+    int32_t reserved[8];
+} ccsd_gpu_davidson_options;
+
+/* eigen_davidson_solver%run (src/solvers/eigen_davidson_solver_class.F90:122-229) on the device:
+ * the n_states lowest EOM-CCSD excitation energies of A (side 0, right) or A^T (side 1, left) at
+ * the current amplitudes.  omega (n_states) on the host; vectors (nullable, host,
+ * (n_t1 + n_t2) x n_states) receive the normalised eigenvectors. */
+int ccsd_gpu_eom_davidson(void *ctx, int32_t n_states, int32_t side, const ccsd_gpu_davidson_options *opt,
+                          double *omega, double *vectors, int32_t *iterations);
+
 /* run_diis_cc_gs (src/solvers/cc/diis_cc_gs_class.F90:209-315) with the quasi-Newton updater,
  * entirely on the device.  On exit the context holds the final amplitudes; history (nullable)
  * receives max_iterations pairs (E, |Omega|). */
