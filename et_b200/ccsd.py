@@ -83,6 +83,9 @@ SIGNATURES = {
     "ccsd_gpu_vjp": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
     "ccsd_gpu_eom_davidson": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(DavidsonOptions), _DP,
                                              _DP, ctypes.POINTER(ctypes.c_int32)]),
+    "ccsd_gpu_construct_eta": (ctypes.c_int, [_VP, _DP]),
+    "ccsd_gpu_solve_multipliers": (ctypes.c_int, [_VP, ctypes.POINTER(DavidsonOptions), _DP,
+                                                  ctypes.POINTER(ctypes.c_int32)]),
     "ccsd_gpu_solve_gs": (ctypes.c_int, [_VP, ctypes.POINTER(SolverOptions), _DP,
                                          ctypes.POINTER(ctypes.c_int32), _DP]),
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
@@ -264,6 +267,20 @@ class CCSD:
         self._check(self.lib.ccsd_gpu_eom_davidson(self.ctx, n_states, int(bool(left)), ctypes.byref(opt), _dp(om),
                                                    _dp(vec) if vectors else None, ctypes.byref(it)))
         return om, (vec.reshape(self.n_amp, n_states, order="F") if vectors else None), it.value
+
+    def construct_eta(self):
+        out = np.empty(self.n_amp)
+        self._check(self.lib.ccsd_gpu_construct_eta(self.ctx, _dp(out)))
+        return out
+
+    def solve_multipliers(self, *, max_iterations=100, residual_threshold=1e-6, max_reduced_dim=0):
+        """A^T tbar = -eta on the device: (tbar, iterations)."""
+        opt = DavidsonOptions(max_iterations=max_iterations, residual_threshold=residual_threshold,
+                              max_reduced_dim=max_reduced_dim)
+        out = np.empty(self.n_amp)
+        it = ctypes.c_int32()
+        self._check(self.lib.ccsd_gpu_solve_multipliers(self.ctx, ctypes.byref(opt), _dp(out), ctypes.byref(it)))
+        return out, it.value
 
     def solve_ground_state(self, *, max_iterations=100, diis_dimension=8, omega_threshold=1e-5,
                            energy_threshold=1e-5, refine_threshold=1e-4, raise_on_failure=True):

@@ -247,6 +247,27 @@ int ccsd_gpu_eom_davidson(void *ctx, int32_t n_states, int32_t side, const ccsd_
     return status;
 }
 
+int ccsd_gpu_construct_eta(void *ctx, double *eta) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(c.have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+        ccsd::DBuf d = ccsd::dalloc(c.namp, c.ex.stream);
+        c.eta(d.d());
+        d2h(c, eta, d.d(), c.namp);
+    });
+}
+
+int ccsd_gpu_solve_multipliers(void *ctx, const ccsd_gpu_davidson_options *opt, double *tbar, int32_t *iterations) {
+    int status = CCSD_GPU_OK;
+    int rc = guarded(ctx, [&](Context &c) {
+        ccsd::DBuf d = ccsd::dalloc(c.namp, c.ex.stream);
+        status = c.multipliers(opt, d.d(), iterations);
+        d2h(c, tbar, d.d(), c.namp);
+    });
+    if (rc != CCSD_GPU_OK) return rc;
+    if (status != CCSD_GPU_OK) static_cast<Context *>(ctx)->err = "multiplier equations did not converge";
+    return status;
+}
+
 int ccsd_gpu_solve_gs(void *ctx, const ccsd_gpu_solver_options *opt, double *energy, int32_t *iterations,
                       double *history) {
     int status = CCSD_GPU_OK;

@@ -60,6 +60,8 @@ struct Context {
     void ladder_tc(const double *Lvv, const double *t2, double *om2);
     int davidson(int nstates, int side, const ccsd_gpu_davidson_options *o, double *omega_out, double *vectors_out,
                  int32_t *iters_out);
+    void eta(double *out);
+    int multipliers(const ccsd_gpu_davidson_options *o, double *tbar, int32_t *iters_out);
     int solve_gs(const ccsd_gpu_solver_options *o, double *energy, int32_t *iters, double *history);
     double omega_flops() const;
 };

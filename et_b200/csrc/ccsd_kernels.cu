@@ -153,6 +153,39 @@ __global__ void add_omega_T_kernel(double *__restrict__ om2, const double *__res
     }
 }
 
+// eta_ai = 2 F_ia, eta_aibj = 4 g_iajb - 2 g_ibja packed (construct_eta_ccsd); F is n_mo x n_mo,
+// g is (o, v, o, v)
+__global__ void eta_kernel(const double *__restrict__ F, const double *__restrict__ g, int64_t no, int64_t nv,
+                           double *__restrict__ eta) {
+    const int64_t nov = no * nv, nt2 = nov * (nov + 1) / 2, nmo = no + nv;
+    GRID_STRIDE(k, nov + nt2) {
+        if (k < nov) {
+            int64_t a = k % nv, i = k / nv;
+            eta[k] = 2.0 * F[i + nmo * (no + a)];
+        } else {
+            int64_t M, m;
+            untri(k - nov, M, m);
+            int64_t a = M % nv, i = M / nv, b = m % nv, j = m / nv;
+            eta[k] = 4.0 * g[i + no * (a + nv * (j + no * b))] - 2.0 * g[i + no * (b + nv * (j + no * a))];
+        }
+    }
+}
+
+// t1bar = t1, t2bar = 2 t_aibj - t_ajbi (packed contravariant amplitudes)
+__global__ void multiplier_guess_kernel(const double *__restrict__ t, int64_t no, int64_t nv,
+                                        double *__restrict__ out) {
+    const int64_t nov = no * nv, nt2 = nov * (nov + 1) / 2;
+    GRID_STRIDE(k, nov + nt2) {
+        if (k < nov) out[k] = t[k];
+        else {
+            int64_t M, m;
+            untri(k - nov, M, m);
+            int64_t a = M % nv, i = M / nv, b = m % nv, j = m / nv;
+            out[k] = 2.0 * t[nov + k - nov] - t[nov + pk(a + nv * j, b + nv * i)];
+        }
+    }
+}
+
 // E_corr partial sums: sum_{ai,bj} (t_aibj + t_ai t_bj)(2 g_iajb - g_ibja), g (o,v,o,v)
 __global__ void energy_partial_kernel(const double *__restrict__ t1, const double *__restrict__ t2,
                                       const double *__restrict__ g, int64_t no, int64_t nv,
@@ -358,6 +391,20 @@ void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pa
 void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv) {
     int64_t total = (nv * (nv + 1) / 2) * (no * (no + 1) / 2);
     add_omega_T_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, W, ldw, no, nv);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void construct_eta(Exec &ex, const double *F, const double *g_ovov, int64_t no, int64_t nv, double *eta) {
+    int64_t nov = no * nv, total = nov + nov * (nov + 1) / 2;
+    eta_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(F, g_ovov, no, nv, eta);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void multiplier_guess(Exec &ex, const double *t, int64_t no, int64_t nv, double *out) {
+    int64_t nov = no * nv, total = nov + nov * (nov + 1) / 2;
+    multiplier_guess_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(t, no, nv, out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }

@@ -25,6 +25,11 @@ void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int
 void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, __nv_bfloat16 *out);
 void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv);
 
+// eta of the multiplier equation (construct_eta_ccsd, multiplier_equation_ccsd.F90:50-113) and the
+// initial multipliers (t1, packed contravariant t2; ccsd_class.F90:411-475)
+void construct_eta(Exec &ex, const double *F, const double *g_ovov, int64_t no, int64_t nv, double *eta);
+void multiplier_guess(Exec &ex, const double *t, int64_t no, int64_t nv, double *out);
+
 void energy_reduce(Exec &ex, const double *t1, const double *t2, const double *g_ovov, int64_t no, int64_t nv,
                    double add, double *d_out);
 void orbital_differences(Exec &ex, const double *eps, int64_t no, int64_t nv, double *out);

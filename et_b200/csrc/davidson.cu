@@ -225,4 +225,109 @@ int Context::davidson(int nstates, int side, const ccsd_gpu_davidson_options *o,
     return conv ? CCSD_GPU_OK : CCSD_GPU_ENOCONV;
 }
 
+// eta of the multiplier equation at the current amplitudes (construct_eta_ccsd)
+void Context::eta(double *out) {
+    refresh();
+    DBuf g = g_ovov();
+    construct_eta(ex, F.d(), g.d(), no, nv, out);
+}
+
+// Multiplier (Lambda) equations  A^T tbar = -eta  by linear Davidson, restating eT's default
+// multiplier solver (linear_davidson_solver_class.F90; factory default
+// cc_multipliers_solver_factory_class.F90:335-355): Galerkin solve in the trial space built from
+// the transpose transformation, orbital-difference preconditioned residuals as new trials.
+int Context::multipliers(const ccsd_gpu_davidson_options *o, double *tbar, int32_t *iters_out) {
+    REQUIRE(have_t && have_L && have_h, CCSD_GPU_ESTATE, "inputs/amplitudes not set");
+    cudaStream_t s = ex.stream;
+    const int maxit = o && o->max_iterations > 0 ? o->max_iterations : 100;
+    const double rthr = o && o->residual_threshold > 0 ? o->residual_threshold : 1e-6;
+    const int64_t maxdim = o && o->max_reduced_dim > 0 ? o->max_reduced_dim : 100;
+    orbital_differences(ex, eps.d(), no, nv, epsdiff.d());
+    DBuf et = dalloc(namp, s);
+    eta(et.d());
+    DBuf V = dalloc(namp * maxdim, s), AV = dalloc(namp * maxdim, s), x = dalloc(namp, s), r = dalloc(namp, s);
+    DBuf cand = dalloc(namp, s), proj = dalloc(maxdim, s), nrm = dalloc(8, s);
+    DBuf G = dalloc(maxdim * maxdim, s), rhs = dalloc(maxdim, s);
+    int64_t dim = 0;
+    auto host_dot = [&](const double *a, const double *b) {
+        dot(ex, a, b, namp, nrm.d());
+        double v;
+        CU_CHECK(cudaMemcpyAsync(&v, nrm.d(), sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU_CHECK(cudaStreamSynchronize(s));
+        return v;
+    };
+    auto add_trial = [&](double *c) {
+        for (int pass = 0; pass < 2; pass++)
+            if (dim > 0) {
+                gemm(ex, true, false, dim, 1, namp, 1.0, V.d(), namp, c, namp, 0.0, proj.d(), dim, false);
+                gemm(ex, false, false, namp, 1, dim, -1.0, V.d(), namp, proj.d(), dim, 1.0, c, namp, false);
+            }
+        double n2 = host_dot(c, c);
+        if (std::sqrt(n2) < 1e-12 || dim >= maxdim) return false;
+        axpby(ex, namp, 1.0 / std::sqrt(n2), c, 0.0, V.d() + dim * namp);
+        jacobian_transpose(1, V.d() + dim * namp, AV.d() + dim * namp);
+        dim++;
+        return true;
+    };
+    multiplier_guess(ex, t.d(), no, nv, cand.d());   // set_initial_multipliers_guess_ccsd
+    add_trial(cand.d());
+    cusolverDnHandle_t hs = nullptr;
+    cusolverDnParams_t ps = nullptr;
+    SOLVER_CHECK(cusolverDnCreate(&hs));
+    SOLVER_CHECK(cusolverDnSetStream(hs, s));
+    SOLVER_CHECK(cusolverDnCreateParams(&ps));
+    struct Guard {
+        cusolverDnHandle_t h;
+        cusolverDnParams_t p;
+        ~Guard() {
+            cusolverDnDestroyParams(p);
+            cusolverDnDestroy(h);
+        }
+    } guard{hs, ps};
+    int it = 0;
+    bool conv = false;
+    while (it < maxit) {
+        it++;
+        // reduced system (V^T A^T V) y = -V^T eta, solved by LU on the device
+        gemm(ex, true, false, dim, dim, namp, 1.0, V.d(), namp, AV.d(), namp, 0.0, G.d(), dim, false);
+        gemm(ex, true, false, dim, 1, namp, -1.0, V.d(), namp, et.d(), namp, 0.0, rhs.d(), dim, false);
+        DBuf piv(sizeof(int64_t) * dim, s), info(sizeof(int), s);
+        size_t db = 0, hb = 0;
+        SOLVER_CHECK(cusolverDnXgetrf_bufferSize(hs, ps, dim, dim, CUDA_R_64F, G.d(), dim, CUDA_R_64F, &db, &hb));
+        DBuf dw(std::max<size_t>(db, 8), s);
+        std::vector<char> hw(std::max<size_t>(hb, 8));
+        SOLVER_CHECK(cusolverDnXgetrf(hs, ps, dim, dim, CUDA_R_64F, G.d(), dim, piv.as<int64_t>(), CUDA_R_64F,
+                                      dw.as<void>(), db, hw.data(), hb, info.as<int>()));
+        SOLVER_CHECK(cusolverDnXgetrs(hs, ps, CUBLAS_OP_N, dim, 1, CUDA_R_64F, G.d(), dim, piv.as<int64_t>(),
+                                      CUDA_R_64F, rhs.d(), dim, info.as<int>()));
+        int inf = 0;
+        CU_CHECK(cudaMemcpyAsync(&inf, info.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CU_CHECK(cudaStreamSynchronize(s));
+        REQUIRE(inf == 0, CCSD_GPU_ESINGULAR, "reduced multiplier system is singular");
+        // x = V y ; r = A^T x + eta = AV y + eta
+        gemm(ex, false, false, namp, 1, dim, 1.0, V.d(), namp, rhs.d(), dim, 0.0, x.d(), namp, false);
+        CU_CHECK(cudaMemcpyAsync(r.d(), et.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
+        gemm(ex, false, false, namp, 1, dim, 1.0, AV.d(), namp, rhs.d(), dim, 1.0, r.d(), namp, false);
+        const double rn = std::sqrt(host_dot(r.d(), r.d()));
+        if (!std::isfinite(rn)) throw Error(CCSD_GPU_ENAN, "non-finite multiplier residual");
+        if (rn < rthr) {
+            conv = true;
+            break;
+        }
+        if (dim >= maxdim) {
+            // restart from the current solution
+            CU_CHECK(cudaMemcpyAsync(cand.d(), x.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
+            dim = 0;
+            add_trial(cand.d());
+        }
+        precondition_kernel<<<grid_for(namp, 256), 256, 0, s>>>(r.d(), epsdiff.d(), 0.0, namp, cand.d());
+        ex.launches++;
+        if (!add_trial(cand.d())) break;
+    }
+    CU_CHECK(cudaMemcpyAsync(tbar, x.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
+    CU_CHECK(cudaStreamSynchronize(s));
+    if (iters_out) *iters_out = it;
+    return conv ? CCSD_GPU_OK : CCSD_GPU_ENOCONV;
+}
+
 }  // namespace ccsd

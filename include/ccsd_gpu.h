@@ -140,6 +140,15 @@ typedef struct ccsd_gpu_davidson_options {
 int ccsd_gpu_eom_davidson(void *ctx, int32_t n_states, int32_t side, const ccsd_gpu_davidson_options *opt,
                           double *omega, double *vectors, int32_t *iterations);
 
+/* construct_eta (src/wavefunctions/ccsd/multiplier_equation_ccsd.F90:50-113) at the current amplitudes:
+ * eta = [2 F_ia ; packed 4 g_iajb - 2 g_ibja] (n_t1 + n_t2, host). */
+int ccsd_gpu_construct_eta(void *ctx, double *eta);
+
+/* Multiplier (Lambda) equations A^T tbar = -eta by linear Davidson on the device (eT's default
+ * multiplier solver, src/solvers/linear_davidson_solver_class.F90), started from t1bar = t1,
+ * t2bar = packed 2 t_aibj - t_ajbi.  tbar (host, n_t1 + n_t2). */
+int ccsd_gpu_solve_multipliers(void *ctx, const ccsd_gpu_davidson_options *opt, double *tbar, int32_t *iterations);
+
 /* run_diis_cc_gs (src/solvers/cc/diis_cc_gs_class.F90:209-315) with the quasi-Newton updater,
  * entirely on the device.  On exit the context holds the final amplitudes; history (nullable)
  * receives max_iterations pairs (E, |Omega|). */

@@ -448,6 +448,23 @@ class CCSDSystem:
         return A
 
 
+def construct_eta(F, L_t1, n_o):
+    """eta = [2 F_ia ; pack(4 g_iajb - 2 g_ibja)]; construct_eta_ccsd, multiplier_equation_ccsd.F90:50-113."""
+    n_v = F.shape[0] - n_o
+    eta1 = 2.0 * F[:n_o, n_o:].T                                  # eta_ai = 2 F_ia
+    L_ov = L_t1[:, :n_o, n_o:]
+    g = eri(L_ov, L_ov)                                            # g[i,a,j,b]
+    eta2 = 4.0 * np.einsum("iajb->aibj", g) - 2.0 * np.einsum("ibja->aibj", g)
+    return np.concatenate([eta1.reshape(-1, order="F"), packin(eta2, n_v, n_o)])
+
+
+def multiplier_guess(t1, t2p, n_o):
+    """t1bar = t1, t2bar = 2 t_aibj - t_ajbi packed (set_initial_multipliers_guess_ccsd, ccsd_class.F90:411-475)."""
+    n_v = t1.shape[0]
+    t = squareup(t2p, n_v, n_o)
+    return np.concatenate([t1.reshape(-1, order="F"), packin(2.0 * t - np.einsum("ajbi->aibj", t), n_v, n_o)])
+
+
 # --------------------------------------------------------------------------
 # solvers: quasi-Newton + DIIS ground state (src/solvers/cc/diis_cc_gs_class.F90)
 # --------------------------------------------------------------------------

@@ -152,3 +152,44 @@ def test_device_davidson_block_matches_oracle():
     w, _, _ = gpu.excited_states(3, block=3, residual_threshold=1e-9, energy_threshold=1e-11)
     assert np.allclose(np.sort(w), np.sort(w_ref), atol=1e-9)
     gpu.close()
+
+
+def test_eta_matches_oracle():
+    s, ref, gpu, amp = _setup(3, 8, 20)
+    eta = gpu.construct_eta()
+    eta_ref = oc.construct_eta(ref.fock, ref.L_t1, ref.n_o)
+    assert np.abs(eta - eta_ref).max() < 1e-12 * max(1.0, np.abs(eta_ref).max())
+    gpu.close()
+
+
+def test_multipliers_match_dense_oracle_solve():
+    """Lambda equations A^T tbar = -eta at the ground-state solution vs a dense oracle solve."""
+    from et_b200 import CCSD
+    n_o, n_v, n_J = 3, 8, 20
+    s = make_system(n_o, n_v, n_J, seed=17)
+    ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
+    ref.mp2_start()
+    oc.solve_gs(ref, omega_threshold=1e-11, energy_threshold=1e-13)
+    gpu = CCSD(n_o, n_v, n_J)
+    gpu.set_system(s.L_mo, s.h_mo, s.eps)
+    gpu.set_amplitudes(ref.get_amplitudes())
+    tbar, it = gpu.solve_multipliers(residual_threshold=1e-10)
+    A = ref.jacobian_matrix()
+    eta = oc.construct_eta(ref.fock, ref.L_t1, ref.n_o)
+    tbar_ref = np.linalg.solve(A.T, -eta)
+    assert np.abs(tbar - tbar_ref).max() < 1e-8 * max(1.0, np.abs(tbar_ref).max())
+    gpu.close()
+
+
+def test_multipliers_residual_h2o_he(h2o_he):
+    from et_b200 import CCSD
+    d = h2o_he
+    n_J, n_o = d["L_mo"].shape[0], d["n_o"]
+    gpu = CCSD(n_o, d["h_mo"].shape[0] - n_o, n_J)
+    gpu.set_system(d["L_mo"], d["h_mo"], d["eps"], d["e_hf"])
+    gpu.set_initial_amplitudes_guess()
+    gpu.solve_ground_state(omega_threshold=1e-10, energy_threshold=1e-12)
+    tbar, it = gpu.solve_multipliers(residual_threshold=1e-9)
+    r = gpu.jacobian_transpose_transformation(tbar) + gpu.construct_eta()
+    assert np.linalg.norm(r) < 1e-8
+    gpu.close()
