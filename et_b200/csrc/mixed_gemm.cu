@@ -120,10 +120,11 @@ struct EpiF64 {
     long long ldc;
     int M, N;
     double alpha, beta;
+    long long zstride = 0;   // split-K: slice z of the grid writes its partial product at C + z*zstride
     __device__ __forceinline__ void row_setup(int) {}
     __device__ __forceinline__ void operator()(int row, int col, float v) const {
         if (row < M && col < N) {
-            double *dst = C + (long long)col * ldc + row;
+            double *dst = C + blockIdx.z * zstride + (long long)col * ldc + row;
             double r = alpha * (double)v;
             if (beta != 0.0) r += beta * *dst;
             *dst = r;
@@ -170,7 +171,10 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int nk = Kp / BK;
+    // K range of this CTA: split-K slices the BK-wide K tiles over gridDim.z
+    const int nk_all = Kp / BK, nks = (nk_all + gridDim.z - 1) / gridDim.z;
+    const int kt0 = blockIdx.z * nks;
+    const int nk = min(nks, nk_all - kt0);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
@@ -204,7 +208,7 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
             if (*abort_flag) break;
             uint8_t *st = smem + s * STAGE_BYTES;
             mbar_expect_tx(&full[s], STAGE_BYTES);
-            const int k0 = i * BK;
+            const int k0 = (kt0 + i) * BK;
             tma_load_3d(&tmA, &full[s], st, k0, m0, 0);                       // A hi
             tma_load_3d(&tmA, &full[s], st + A_TILE, k0, m0, 1);              // A lo
             tma_load_3d(&tmB, &full[s], st + 2 * A_TILE, k0, n0, 0);          // B hi
@@ -308,6 +312,19 @@ __global__ void split_bf16_kernel(const double *__restrict__ src, long long sr, 
     }
 }
 
+// C = beta C + sum_z P_z  (P_z dense m x n, z-major)
+__global__ void sum_splits_kernel(const double *__restrict__ P, int splits, int64_t m, int64_t n, double beta,
+                                  double *__restrict__ C, int64_t ldc) {
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < m * n;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = idx % m, c = idx / m;
+        double acc = 0.0;
+        for (int z = 0; z < splits; z++) acc += P[(int64_t)z * m * n + idx];
+        double *dst = C + r + ldc * c;
+        *dst = beta != 0.0 ? beta * *dst + acc : acc;
+    }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -347,12 +364,12 @@ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 template <class Epi>
 void launch_tc(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t Mp,
                const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t Np, int64_t Kp, const Epi &epi,
-               double issued_flops) {
+               double issued_flops, int splits = 1) {
     REQUIRE(Mp % BM == 0 && Np % BN == 0 && Kp % BK == 0 && Kp > 0, CCSD_GPU_EINVAL, "tc gemm: bad padding");
     CU_CHECK(cudaFuncSetAttribute(bf16x3_gemm_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane);
     CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, BN, b_plane);
-    dim3 grid((unsigned)(Mp / BM), (unsigned)(Np / BN));
+    dim3 grid((unsigned)(Mp / BM), (unsigned)(Np / BN), (unsigned)splits);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ex.prof && ex.prof->on) {
         CU_CHECK(cudaEventCreate(&e0));
@@ -390,9 +407,28 @@ void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     // B operand rows are output columns: op(B)(kk, c) = B[kk + ldb c] (N) or B[c + ldb kk] (T)
     if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, b.as<__nv_bfloat16>());
     else split(ex, B, 1, ldb, n, k, Np, Kp, b.as<__nv_bfloat16>());
-    EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
+    // split K when the output tiles cannot fill the 148 SMs: deterministic partial products, then a sum
+    const int64_t tiles = (Mp / BM) * (Np / BN), nkt = Kp / BK;
+    int splits = 1;
+    if (tiles < 148 && nkt >= 16) {
+        int64_t want = std::min<int64_t>((296 + tiles - 1) / tiles, nkt / 8);
+        int64_t per = (nkt + want - 1) / want;
+        splits = (int)((nkt + per - 1) / per);
+    }
+    if (splits <= 1) {
+        EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
+        launch_tc(ex, a.as<__nv_bfloat16>(), Mp, Mp * Kp, Mp, b.as<__nv_bfloat16>(), Np, Np * Kp, Np, Kp, epi,
+                  6.0 * double(m) * double(n) * double(k));
+        return;
+    }
+    DBuf part = dalloc((int64_t)splits * m * n, ex.stream);
+    EpiF64 epi{part.d(), (long long)m, (int)m, (int)n, alpha, 0.0, (long long)m * n};
     launch_tc(ex, a.as<__nv_bfloat16>(), Mp, Mp * Kp, Mp, b.as<__nv_bfloat16>(), Np, Np * Kp, Np, Kp, epi,
-              6.0 * double(m) * double(n) * double(k));
+              6.0 * double(m) * double(n) * double(k), splits);
+    sum_splits_kernel<<<(unsigned)std::min<int64_t>((m * n + 255) / 256, 148 * 64), 256, 0, ex.stream>>>(
+        part.d(), splits, m, n, beta, C, ldc);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
 }
 
 int64_t tc_pad_rows_a(int64_t m) { return round_up(m, BM); }

@@ -22,7 +22,8 @@ def ctx():
 
 
 @pytest.mark.parametrize("m,n,k", [(128, 256, 64), (200, 300, 100), (1, 1, 16), (129, 257, 65),
-                                   (640, 512, 1200), (300, 1000, 777)])
+                                   (640, 512, 1200), (300, 1000, 777),
+                                   (200, 300, 20000), (320, 320, 41000)])   # the last two run split-K
 @pytest.mark.parametrize("tA,tB", [(False, False), (True, False), (False, True), (True, True)])
 def test_mixed_gemm_matches_fp64(ctx, m, n, k, tA, tB):
     rng = np.random.default_rng(m * 7 + n * 3 + k)
