@@ -27,8 +27,9 @@ constexpr int A_TILE = BM * BK * 2;        // bytes per plane
 constexpr int B_TILE = BN * BK * 2;
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-constexpr int THREADS = 128;
-constexpr uint32_t TMEM_COLS = BN;         // FP32 accumulator 128 lanes x BN columns
+constexpr int THREADS = 192;              // producer warp, MMA warp, four epilogue warps
+constexpr int EPI_THREADS = 128;
+constexpr uint32_t TMEM_COLS = 2 * BN;     // two FP32 accumulators of 128 lanes x BN columns
 constexpr long long WAIT_CYCLES = 4000000000ll;   // ~2 s at 2 GHz: far above any legitimate wait
 
 __device__ int g_mixed_gemm_error = 0;
@@ -120,11 +121,13 @@ struct EpiF64 {
     long long ldc;
     int M, N;
     double alpha, beta;
-    long long zstride = 0;   // split-K: slice z of the grid writes its partial product at C + z*zstride
+    long long zstride = 0;   // split-K: slice z writes its partial product at C + z*zstride
+    long long zoff = 0;
+    __device__ __forceinline__ void tile_setup(int z) { zoff = (long long)z * zstride; }
     __device__ __forceinline__ void row_setup(int) {}
     __device__ __forceinline__ void operator()(int row, int col, float v) const {
         if (row < M && col < N) {
-            double *dst = C + blockIdx.z * zstride + (long long)col * ldc + row;
+            double *dst = C + zoff + (long long)col * ldc + row;
             double r = alpha * (double)v;
             if (beta != 0.0) r += beta * *dst;
             *dst = r;
@@ -141,6 +144,7 @@ struct EpiPairs {
     long long ldk;
     int nv, a0, M, N;
     int a, c;
+    __device__ __forceinline__ void tile_setup(int) {}
     __device__ __forceinline__ void row_setup(int row) {
         a = a0 + row / nv;
         c = row - (row / nv) * nv;
@@ -158,28 +162,57 @@ struct EpiPairs {
 
 namespace {
 
+// Tile t of the flattened (split, m-tile, n-tile) space.  With few n-tiles the n index runs fastest
+// so the CTAs that run at the same time share A tiles in L2; otherwise the m index runs fastest.
+struct TileMap {
+    int num_mt, num_nt, nk_all, nks;
+    bool n_fast;
+    __device__ __forceinline__ void decode(int t, int &m0, int &n0, int &z, int &kt0, int &nk) const {
+        const int per_split = num_mt * num_nt;
+        z = t / per_split;
+        const int r = t - z * per_split;
+        int mt, nt;
+        if (n_fast) {
+            nt = r % num_nt;
+            mt = r / num_nt;
+        } else {
+            mt = r % num_mt;
+            nt = r / num_mt;
+        }
+        m0 = mt * BM;
+        n0 = nt * BN;
+        kt0 = z * nks;
+        nk = min(nks, nk_all - kt0);
+    }
+};
+
+// Persistent, warp-specialised: warp 0 = TMA producer, warp 1 = MMA issuer (and TMEM owner),
+// warps 2..5 = epilogue.  Two 128 x BN FP32 accumulators in TMEM (512 columns) let the epilogue
+// of one tile overlap the main loop of the next.
 template <class Epi>
 __global__ void __launch_bounds__(THREADS, 1)
-bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int Kp, Epi epi) {
+bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TileMap map,
+                   int num_tiles, Epi epi) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
     uint64_t *empty = full + STAGES;
-    uint64_t *done = empty + STAGES;
+    uint64_t *acc_full = empty + STAGES;    // [2]
+    uint64_t *acc_empty = acc_full + 2;     // [2]
+    uint64_t *done = acc_empty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    // K range of this CTA: split-K slices the BK-wide K tiles over gridDim.z
-    const int nk_all = Kp / BK, nks = (nk_all + gridDim.z - 1) / gridDim.z;
-    const int kt0 = blockIdx.z * nks;
-    const int nk = min(nks, nk_all - kt0);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], EPI_THREADS);
         }
         mbar_init(done, 1);
         *abort_flag = 0;
@@ -196,83 +229,108 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0) {
-        // TMA producer
-        for (int i = 0; i < nk; i++) {
-            const int s = i % STAGES;
-            if (!mbar_wait(&empty[s], ((i / STAGES) & 1) ^ 1)) {
-                atomicExch(&g_mixed_gemm_error, 1);
-                *abort_flag = 1;
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer: one ring of stages across all tiles of this CTA
+            int g = 0;
+            for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
+                int m0, n0, z, kt0, nk;
+                map.decode(t, m0, n0, z, kt0, nk);
+                for (int i = 0; i < nk; i++, g++) {
+                    const int s = g % STAGES;
+                    if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1) || *abort_flag) {
+                        atomicExch(&g_mixed_gemm_error, 1);
+                        *abort_flag = 1;
+                        break;
+                    }
+                    uint8_t *st = smem + s * STAGE_BYTES;
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    const int k0 = (kt0 + i) * BK;
+                    tma_load_3d(&tmA, &full[s], st, k0, m0, 0);                       // A hi
+                    tma_load_3d(&tmA, &full[s], st + A_TILE, k0, m0, 1);              // A lo
+                    tma_load_3d(&tmB, &full[s], st + 2 * A_TILE, k0, n0, 0);          // B hi
+                    tma_load_3d(&tmB, &full[s], st + 2 * A_TILE + B_TILE, k0, n0, 1); // B lo
+                }
             }
-            if (*abort_flag) break;
-            uint8_t *st = smem + s * STAGE_BYTES;
-            mbar_expect_tx(&full[s], STAGE_BYTES);
-            const int k0 = (kt0 + i) * BK;
-            tma_load_3d(&tmA, &full[s], st, k0, m0, 0);                       // A hi
-            tma_load_3d(&tmA, &full[s], st + A_TILE, k0, m0, 1);              // A lo
-            tma_load_3d(&tmB, &full[s], st + 2 * A_TILE, k0, n0, 0);          // B hi
-            tma_load_3d(&tmB, &full[s], st + 2 * A_TILE + B_TILE, k0, n0, 1); // B lo
         }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        bool ok = true;
-        for (int i = 0; i < nk; i++) {
-            const int s = i % STAGES;
-            if (!mbar_wait(&full[s], (i / STAGES) & 1)) {
-                atomicExch(&g_mixed_gemm_error, 2);
-                *abort_flag = 1;
-                ok = false;
-                break;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer
+            int g = 0, tc = 0;
+            for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x, tc++) {
+                int m0, n0, z, kt0, nk;
+                map.decode(t, m0, n0, z, kt0, nk);
+                const int acc = tc & 1;
+                if (!mbar_wait(&acc_empty[acc], ((tc >> 1) & 1) ^ 1)) {
+                    atomicExch(&g_mixed_gemm_error, 4);
+                    *abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(acc * BN);
+                for (int i = 0; i < nk; i++, g++) {
+                    const int s = g % STAGES;
+                    if (!mbar_wait(&full[s], (g / STAGES) & 1) || *abort_flag) {
+                        atomicExch(&g_mixed_gemm_error, 2);
+                        *abort_flag = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint8_t *st = smem + s * STAGE_BYTES;
+                    const uint8_t *ahi = st, *alo = st + A_TILE, *bhi = st + 2 * A_TILE, *blo = st + 2 * A_TILE + B_TILE;
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; kk++) {
+                        const uint32_t ko = kk * 32;   // 16 bf16 = 32 bytes inside the swizzled row
+                        mma_bf16(d, smem_desc(ahi, ko), smem_desc(bhi, ko), (i > 0 || kk > 0) ? 1u : 0u);
+                        mma_bf16(d, smem_desc(ahi, ko), smem_desc(blo, ko), 1u);
+                        mma_bf16(d, smem_desc(alo, ko), smem_desc(bhi, ko), 1u);
+                    }
+                    mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
+                }
+                mma_commit(&acc_full[acc]);  // accumulator ready for the epilogue
             }
-            if (*abort_flag) {
-                ok = false;
+            mma_commit(done);                // every MMA of this CTA has completed
+        }
+    } else {
+        // epilogue: warp w reads TMEM lanes 32*(w % 4) .. +31
+        const int quarter = warp & 3;
+        int tc = 0;
+        for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, tc++) {
+            int m0, n0, z, kt0, nk;
+            map.decode(t, m0, n0, z, kt0, nk);
+            const int acc = tc & 1;
+            bool ok = !*abort_flag && mbar_wait(&acc_full[acc], (tc >> 1) & 1);
+            __syncwarp();
+            if (!ok || *abort_flag) {
+                atomicExch(&g_mixed_gemm_error, 3);
+                *abort_flag = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint8_t *st = smem + s * STAGE_BYTES;
-            const uint8_t *ahi = st, *alo = st + A_TILE, *bhi = st + 2 * A_TILE, *blo = st + 2 * A_TILE + B_TILE;
-#pragma unroll
-            for (int kk = 0; kk < BK / 16; kk++) {
-                const uint32_t ko = kk * 32;   // 16 bf16 = 32 bytes inside the swizzled row
-                mma_bf16(tmem, smem_desc(ahi, ko), smem_desc(bhi, ko), (i > 0 || kk > 0) ? 1u : 0u);
-                mma_bf16(tmem, smem_desc(ahi, ko), smem_desc(blo, ko), 1u);
-                mma_bf16(tmem, smem_desc(alo, ko), smem_desc(bhi, ko), 1u);
-            }
-            mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
-        }
-        // arrives once every MMA issued so far has completed (also on the abort path)
-        mma_commit(done);
-        (void)ok;
-    }
-    __syncwarp();
-
-    // epilogue: all four warps; warp w owns TMEM lanes 32w..32w+31 (rows m0 + 32w + lane)
-    bool ok = mbar_wait(done, 0);
-    if (!ok) {
-        atomicExch(&g_mixed_gemm_error, 3);
-        *abort_flag = 1;
-    }
-    __syncwarp();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int row = m0 + warp * 32 + lane;
-    epi.row_setup(row);
-    if (ok && !*abort_flag) {
+            const int row = m0 + quarter * 32 + lane;
+            epi.tile_setup(z);
+            epi.row_setup(row);
+            const uint32_t base = tmem + (uint32_t)(acc * BN) + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                float v[16];
+                tmem_ld16(base + (uint32_t)c0, v);
 #pragma unroll
-            for (int j = 0; j < 16; j++) epi(row, n0 + c0 + j, v[j]);
+                for (int j = 0; j < 16; j++) epi(row, n0 + c0 + j, v[j]);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[acc])) : "memory");
         }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    // all MMAs complete before the TMEM is released
+    if (!mbar_wait(done, 0)) atomicExch(&g_mixed_gemm_error, 5);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 1) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
     }
 }
-
 // FP64 (strided view of op(X): element (r, k) at src[r*sr + k*sk]) -> bf16 hi/lo planes,
 // K-major [plane][R_pad][K_pad], zero padded.  32x32 smem tile so both sides stay coalesced;
 // blockIdx.x runs over row blocks (up to 2^31), blockIdx.y strides over K blocks.
@@ -361,6 +419,7 @@ CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 // A: rows [0, a_rows) of planes with stride a_plane; the grid covers Mp x Np output tiles.
+
 template <class Epi>
 void launch_tc(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t Mp,
                const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t Np, int64_t Kp, const Epi &epi,
@@ -369,14 +428,27 @@ void launch_tc(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane
     CU_CHECK(cudaFuncSetAttribute(bf16x3_gemm_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane);
     CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, BN, b_plane);
-    dim3 grid((unsigned)(Mp / BM), (unsigned)(Np / BN), (unsigned)splits);
+    TileMap map;
+    map.num_mt = (int)(Mp / BM);
+    map.num_nt = (int)(Np / BN);
+    map.nk_all = (int)(Kp / BK);
+    map.nks = (map.nk_all + splits - 1) / splits;
+    map.n_fast = map.num_nt <= 16;
+    const int num_tiles = map.num_mt * map.num_nt * splits;
+    int nsm = 148;
+    {
+        int dev = 0;
+        CU_CHECK(cudaGetDevice(&dev));
+        CU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    }
+    dim3 grid((unsigned)std::min(num_tiles, nsm));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ex.prof && ex.prof->on) {
         CU_CHECK(cudaEventCreate(&e0));
         CU_CHECK(cudaEventCreate(&e1));
         CU_CHECK(cudaEventRecord(e0, ex.stream));
     }
-    bf16x3_gemm_kernel<Epi><<<grid, THREADS, SMEM_BYTES, ex.stream>>>(ta, tb, (int)Kp, epi);
+    bf16x3_gemm_kernel<Epi><<<grid, THREADS, SMEM_BYTES, ex.stream>>>(ta, tb, map, num_tiles, epi);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
     if (e0) {
