@@ -260,6 +260,160 @@ def run_gpu(args):
         print(json.dumps(result), flush=True)
 
 
+def _event_time(fn, stream):
+    import torch
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    fn()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / 1e3
+
+
+def run_eom(args):
+    """EOM-CCSD right roots with a batched Davidson block (o=24, v=240, N_J=792, 12 roots, 24 trials)."""
+    import torch
+    from et_b200 import CCSD, FP64, MIXED
+    from et_b200.synthetic import make_system
+    n_o, n_v, n_J = 24, 240, 792
+    s = make_system(n_o, n_v, n_J, seed=2026)
+    stream = torch.cuda.current_stream()
+    gpu = CCSD(n_o, n_v, n_J, precision=MIXED)
+    gpu.set_stream(stream.cuda_stream)
+    gpu.set_system(s.L_mo, s.h_mo, s.eps, s.e_hf)
+    gpu.set_initial_amplitudes_guess()
+    e, it, _, rc = gpu.solve_ground_state(max_iterations=60, omega_threshold=1e-9, energy_threshold=1e-10,
+                                          raise_on_failure=False)
+    out = {"workload": "EOM-CCSD right roots, synthetic o=24 v=240 N_J=792", "gs_energy": e, "gs_iterations": it}
+    n = gpu.n_amp
+    C = torch.randn(n, 24, dtype=torch.float64, device="cuda")
+    R = torch.empty_like(C)
+    for prec, name in ((MIXED, "mixed"), (FP64, "fp64")):
+        gpu.set_precision(prec)
+        gpu.jacobian_device(1, C.data_ptr(), R.data_ptr())                     # warm-up
+        t1 = min(_event_time(lambda: gpu.jacobian_device(1, C.data_ptr(), R.data_ptr()), stream) for _ in range(2))
+        t24 = _event_time(lambda: gpu.jacobian_device(24, C.data_ptr(), R.data_ptr()), stream)
+        out[f"s_per_transform_{name}"] = round(t1, 4)
+        out[f"s_per_24_block_{name}"] = round(t24, 4)
+    nroots = args.roots
+    gpu.set_precision(MIXED)
+    t0 = time.perf_counter()
+    w_mix, X, it_mix = gpu.excited_states(nroots, block=24, residual_threshold=1e-4, energy_threshold=1e-5,
+                                          vectors=True, max_iterations=60)
+    gpu.set_precision(FP64)
+    w_ref, _, it_ref = gpu.excited_states(nroots, block=24, residual_threshold=1e-6, energy_threshold=1e-8,
+                                          start=X, max_iterations=60)
+    t_mixed_path = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    w64, _, it64 = gpu.excited_states(nroots, block=24, residual_threshold=1e-6, energy_threshold=1e-8,
+                                      max_iterations=60)
+    t_fp64_path = time.perf_counter() - t0
+    out.update({"roots": nroots, "omega_mixed_refined": list(map(float, w_ref)), "omega_fp64": list(map(float, w64)),
+                "max_abs_domega": float(np.max(np.abs(np.sort(w_ref) - np.sort(w64)))),
+                "davidson_iterations_mixed_then_fp64": [it_mix, it_ref], "davidson_iterations_fp64": it64,
+                "s_mixed_plus_refinement": round(t_mixed_path, 2), "s_fp64": round(t_fp64_path, 2)})
+    gpu.close()
+    print(json.dumps(out), flush=True)
+
+
+def run_adjoint(args):
+    """Adjoint check at o=16, v=128, N_J=432: VJP into (t, L, h) vs central finite differences, and Lambda."""
+    from et_b200 import CCSD
+    from et_b200.synthetic import make_system
+    n_o, n_v, n_J = 16, 128, 432
+    s = make_system(n_o, n_v, n_J, seed=2026)
+    gpu = CCSD(n_o, n_v, n_J)
+    gpu.set_system(s.L_mo, s.h_mo, s.eps, s.e_hf)
+    gpu.set_initial_amplitudes_guess()
+    rng = np.random.default_rng(7)
+    t = gpu.get_amplitudes()
+    t = t * (1.0 + 0.1 * rng.standard_normal(t.size))
+    gpu.set_amplitudes(t)
+    b = rng.standard_normal(gpu.n_amp)
+    b /= np.linalg.norm(b)
+    t0 = time.perf_counter()
+    dt, dL, dh = gpu.vjp(b, want_L=True, want_h=True)
+    t_vjp = time.perf_counter() - t0
+    h = 1e-5
+    errs = []
+
+    def f(tt, LL, hh):
+        gpu.set_cholesky_mo(LL)
+        gpu.set_h_mo(hh, s.eps, s.e_hf)
+        gpu.set_amplitudes(tt)
+        return float(b @ gpu.construct_omega())
+
+    for _ in range(args.directions):
+        d_t = rng.standard_normal(t.size)
+        d_L = rng.standard_normal(s.L_mo.shape)
+        d_L = 0.5 * (d_L + d_L.transpose(0, 2, 1))
+        d_h = rng.standard_normal(s.h_mo.shape)
+        fd = (f(t + h * d_t, s.L_mo + h * d_L, s.h_mo + h * d_h) -
+              f(t - h * d_t, s.L_mo - h * d_L, s.h_mo - h * d_h)) / (2 * h)
+        ad = float(dt @ d_t + np.sum(dL * d_L) + np.sum(dh * d_h))
+        errs.append(abs(fd - ad) / max(abs(ad), 1e-300))
+    # Lambda equations through the adjoint (transpose transformation) at the converged amplitudes
+    gpu.set_cholesky_mo(s.L_mo)
+    gpu.set_h_mo(s.h_mo, s.eps, s.e_hf)
+    gpu.set_initial_amplitudes_guess()
+    gpu.solve_ground_state(omega_threshold=1e-9, energy_threshold=1e-11)
+    t0 = time.perf_counter()
+    tbar, it_l = gpu.solve_multipliers(residual_threshold=1e-8)
+    t_lambda = time.perf_counter() - t0
+    resid = float(np.linalg.norm(gpu.jacobian_transpose_transformation(tbar) + gpu.construct_eta()))
+    gpu.close()
+    print(json.dumps({"workload": "adjoint vs central finite differences, synthetic o=16 v=128 N_J=432",
+                      "directions": args.directions, "h": h, "max_rel_error": max(errs),
+                      "median_rel_error": float(np.median(errs)), "s_vjp_t_L_h": round(t_vjp, 3),
+                      "lambda_iterations": it_l, "lambda_residual": resid, "s_lambda": round(t_lambda, 2)}),
+          flush=True)
+
+
+def run_batch(args):
+    """64 independent systems o ~ U{6..24}, v = 8o, N_J = 3(o+v): systems/s, mixed+refinement vs FP64."""
+    import torch
+    from et_b200 import CCSD, FP64, MIXED
+    from et_b200.synthetic import make_system
+    rank, local, world = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(2026)
+    sizes = [int(o) for o in rng.integers(6, 25, size=args.systems)]
+    mine = list(range(rank, args.systems, world))
+    res = {}
+    for prec, name in ((MIXED, "mixed"), (FP64, "fp64")):
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        energies = {}
+        for k in mine:
+            o = sizes[k]
+            v, J = 8 * o, 3 * (o + 8 * o)
+            s = make_system(o, v, J, seed=2026 + k)
+            with CCSD(o, v, J, precision=prec, device=local) as gpu:
+                gpu.set_system(s.L_mo, s.h_mo, s.eps, s.e_hf)
+                gpu.set_initial_amplitudes_guess()
+                e, it, _, rc = gpu.solve_ground_state(max_iterations=80, omega_threshold=1e-8,
+                                                      energy_threshold=1e-10, raise_on_failure=False)
+                energies[k] = (e, it, rc)
+        torch.cuda.synchronize()
+        dt = max_over_ranks(time.perf_counter() - t0, world)
+        res[name] = (dt, energies)
+    de = max(abs(res["mixed"][1][k][0] - res["fp64"][1][k][0]) for k in mine)
+    de = max_over_ranks(de, world)
+    if rank == 0:
+        print(json.dumps({"workload": f"uneven batch of {args.systems} synthetic systems, o~U{{6..24}}, v=8o, N_J=3(o+v)",
+                          "n_gpus": world, "systems_per_s_mixed": round(args.systems / res["mixed"][0], 3),
+                          "systems_per_s_fp64": round(args.systems / res["fp64"][0], 3),
+                          "speedup": round(res["fp64"][0] / res["mixed"][0], 3), "max_abs_dE": de,
+                          "all_converged": all(v[2] == 0 for r in res.values() for v in r[1].values())}),
+              flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def cpu_sample(args):
     """The CPU oracle (numpy + threaded BLAS) on a bounded sample: GS iterations at a reduced size."""
     from oracle import ccsd as oc
@@ -302,6 +456,11 @@ def main():
     p.add_argument("--steps", type=int, default=15)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="gs", choices=["gs", "eom", "adjoint", "batch"],
+                   help="gs: the headline ground-state iteration; eom / adjoint / batch: the other workloads")
+    p.add_argument("--roots", type=int, default=12)
+    p.add_argument("--directions", type=int, default=256)
+    p.add_argument("--systems", type=int, default=64)
     p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--refine", type=float, default=1e-4)
     p.add_argument("--no-compare", dest="compare", action="store_false",
@@ -317,6 +476,12 @@ def main():
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "eom":
+        run_eom(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_gpu(args)
 

@@ -45,7 +45,7 @@ class Options(ctypes.Structure):
 
 class DavidsonOptions(ctypes.Structure):
     _fields_ = [("max_iterations", ctypes.c_int32), ("block", ctypes.c_int32), ("max_reduced_dim", ctypes.c_int32),
-                ("reserved0", ctypes.c_int32), ("residual_threshold", ctypes.c_double),
+                ("start_from_vectors", ctypes.c_int32), ("residual_threshold", ctypes.c_double),
                 ("energy_threshold", ctypes.c_double), ("reserved", ctypes.c_int32 * 8)]
 
 
@@ -80,6 +80,8 @@ SIGNATURES = {
     "ccsd_gpu_omega_device": (ctypes.c_int, [_VP, _VP]),
     "ccsd_gpu_jacobian": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
     "ccsd_gpu_jacobian_transpose": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
+    "ccsd_gpu_jacobian_device": (ctypes.c_int, [_VP, _I64, _VP, _VP]),
+    "ccsd_gpu_jacobian_transpose_device": (ctypes.c_int, [_VP, _I64, _VP, _VP]),
     "ccsd_gpu_vjp": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
     "ccsd_gpu_eom_davidson": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(DavidsonOptions), _DP,
                                              _DP, ctypes.POINTER(ctypes.c_int32)]),
@@ -241,6 +243,11 @@ class CCSD:
         self._check(self.lib.ccsd_gpu_jacobian_transpose(self.ctx, n_vec, _dp(flat), _dp(out)))
         return out if b.ndim == 1 else out.reshape(self.n_amp, n_vec, order="F")
 
+    def jacobian_device(self, n_vec: int, d_c: int, d_rho: int, transpose: bool = False):
+        """rho = A c (or sigma = b^T A) on device pointers of (n_amp x n_vec) column blocks."""
+        fn = self.lib.ccsd_gpu_jacobian_transpose_device if transpose else self.lib.ccsd_gpu_jacobian_device
+        self._check(fn(self.ctx, n_vec, _VP(d_c), _VP(d_rho)))
+
     def vjp(self, b, *, want_L=False, want_h=False):
         """b^T dOmega/dt (no D scaling), and optionally b^T dOmega/dL_mo (J,p,q) and b^T dOmega/dh_mo."""
         b = _f64(b, self.n_amp)
@@ -257,12 +264,19 @@ class CCSD:
         return out[0] if len(out) == 1 else tuple(out)
 
     def excited_states(self, n_states, *, left=False, max_iterations=100, block=0, max_reduced_dim=0,
-                       residual_threshold=1e-6, energy_threshold=1e-6, vectors=False):
-        """eigen_davidson_solver on the device: (omegas, vectors or None, iterations)."""
+                       residual_threshold=1e-6, energy_threshold=1e-6, vectors=False, start=None):
+        """eigen_davidson_solver on the device: (omegas, vectors or None, iterations).
+
+        ``start`` ((n_amp, n_states)) seeds the trial space, e.g. with mixed-precision eigenvectors."""
         opt = DavidsonOptions(max_iterations=max_iterations, block=block, max_reduced_dim=max_reduced_dim,
-                              residual_threshold=residual_threshold, energy_threshold=energy_threshold)
+                              residual_threshold=residual_threshold, energy_threshold=energy_threshold,
+                              start_from_vectors=int(start is not None))
         om = np.zeros(n_states)
-        vec = np.zeros(self.n_amp * n_states) if vectors else None
+        if start is not None:
+            vectors = True
+            vec = np.ascontiguousarray(np.asarray(start, dtype=np.float64).reshape(-1, order="F"))
+        else:
+            vec = np.zeros(self.n_amp * n_states) if vectors else None
         it = ctypes.c_int32()
         self._check(self.lib.ccsd_gpu_eom_davidson(self.ctx, n_states, int(bool(left)), ctypes.byref(opt), _dp(om),
                                                    _dp(vec) if vectors else None, ctypes.byref(it)))

@@ -216,6 +216,20 @@ int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, doubl
     });
 }
 
+int ccsd_gpu_jacobian_device(void *ctx, int64_t n_vec, const double *d_c, double *d_rho) {
+    return guarded(ctx, [&](Context &x) {
+        REQUIRE(n_vec > 0 && d_c && d_rho, CCSD_GPU_EINVAL, "bad jacobian arguments");
+        x.jacobian(n_vec, d_c, d_rho);
+    });
+}
+
+int ccsd_gpu_jacobian_transpose_device(void *ctx, int64_t n_vec, const double *d_b, double *d_sigma) {
+    return guarded(ctx, [&](Context &x) {
+        REQUIRE(n_vec > 0 && d_b && d_sigma, CCSD_GPU_EINVAL, "bad transpose arguments");
+        x.jacobian_transpose(n_vec, d_b, d_sigma);
+    });
+}
+
 int ccsd_gpu_vjp(void *ctx, const double *b, double *dt, double *dL, double *dh) {
     return guarded(ctx, [&](Context &x) {
         REQUIRE(b != nullptr, CCSD_GPU_EINVAL, "null cotangent");
@@ -239,7 +253,10 @@ int ccsd_gpu_eom_davidson(void *ctx, int32_t n_states, int32_t side, const ccsd_
         REQUIRE(side == 0 || side == 1, CCSD_GPU_EINVAL, "side must be 0 (right) or 1 (left)");
         REQUIRE(omega != nullptr, CCSD_GPU_EINVAL, "null omega");
         ccsd::DBuf dv = vectors ? ccsd::dalloc(c.namp * n_states, c.ex.stream) : ccsd::DBuf();
-        status = c.davidson(n_states, side, opt, omega, vectors ? dv.d() : nullptr, iterations);
+        const bool start = opt && opt->start_from_vectors;
+        REQUIRE(!start || vectors, CCSD_GPU_EINVAL, "start_from_vectors needs the vectors argument");
+        if (start) h2d(c, dv.d(), vectors, c.namp * n_states);
+        status = c.davidson(n_states, side, opt, omega, vectors ? dv.d() : nullptr, iterations, start ? dv.d() : nullptr);
         if (vectors) d2h(c, vectors, dv.d(), c.namp * n_states);
     });
     if (rc != CCSD_GPU_OK) return rc;

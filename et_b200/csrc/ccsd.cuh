@@ -59,7 +59,7 @@ struct Context {
     void ladder(const double *Lvv, const double *t2, double *om2);
     void ladder_tc(const double *Lvv, const double *t2, double *om2);
     int davidson(int nstates, int side, const ccsd_gpu_davidson_options *o, double *omega_out, double *vectors_out,
-                 int32_t *iters_out);
+                 int32_t *iters_out, const double *start = nullptr);
     void eta(double *out);
     int multipliers(const ccsd_gpu_davidson_options *o, double *tbar, int32_t *iters_out);
     int solve_gs(const ccsd_gpu_solver_options *o, double *energy, int32_t *iters, double *history);

@@ -89,7 +89,7 @@ struct Geev {
 }  // namespace
 
 int Context::davidson(int nstates, int side, const ccsd_gpu_davidson_options *o, double *omega_out,
-                      double *vectors_out, int32_t *iters_out) {
+                      double *vectors_out, int32_t *iters_out, const double *start) {
     REQUIRE(have_t && have_L && have_h, CCSD_GPU_ESTATE, "inputs/amplitudes not set");
     REQUIRE(nstates > 0 && nstates <= namp, CCSD_GPU_EINVAL, "bad number of states");
     cudaStream_t s = ex.stream;
@@ -116,8 +116,13 @@ int Context::davidson(int nstates, int side, const ccsd_gpu_davidson_options *o,
     DBuf V = dalloc(namp * maxdim, s), AV = dalloc(namp * maxdim, s);
     int64_t dim = 0, nnew = 0;
     DBuf newv = dalloc(namp * std::max<int64_t>(nstates, 1), s);
-    for (int k = 0; k < nstates; k++)
-        unit_vector_kernel<<<grid_for(namp, 256), 256, 0, s>>>(newv.d() + k * namp, namp, order[k]);
+    if (start) {
+        // start vectors supplied (e.g. the converged mixed-precision eigenvectors)
+        CU_CHECK(cudaMemcpyAsync(newv.d(), start, sizeof(double) * namp * nstates, cudaMemcpyDeviceToDevice, s));
+    } else {
+        for (int k = 0; k < nstates; k++)
+            unit_vector_kernel<<<grid_for(namp, 256), 256, 0, s>>>(newv.d() + k * namp, namp, order[k]);
+    }
     nnew = nstates;
     std::vector<double> omega(nstates, 0.0), prev(nstates, 0.0);
     DBuf G = dalloc(maxdim * maxdim, s), X = dalloc(namp * nstates, s), R = dalloc(namp * nstates, s);

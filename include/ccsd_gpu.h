@@ -116,6 +116,10 @@ int ccsd_gpu_jacobian(void *ctx, int64_t n_vec, const double *c, double *rho);
  * sigma_k = b_k^T A. */
 int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, double *sigma);
 
+/* The same two transformations on device pointers (trial and result blocks stay in HBM). */
+int ccsd_gpu_jacobian_device(void *ctx, int64_t n_vec, const double *d_c, double *d_rho);
+int ccsd_gpu_jacobian_transpose_device(void *ctx, int64_t n_vec, const double *d_b, double *d_sigma);
+
 /* Vector-Jacobian product of the residual: given a cotangent b (n_t1 + n_t2), returns
  *   dt = (dOmega/dt)^T b                      (n_t1 + n_t2; sigma = D dt with D = 2 on the doubles diagonal),
  *   dL = (dOmega/dL_mo)^T b  (nullable)       ((J, p, q) over the full MO range, as ccsd_gpu_set_cholesky_mo),
@@ -127,7 +131,7 @@ typedef struct ccsd_gpu_davidson_options {
     int32_t max_iterations;      /* default 100 */
     int32_t block;               /* trial vectors per batched transformation (0 = by memory) */
     int32_t max_reduced_dim;     /* default max(100, 10 n_states), as eT (cc_es_amplitudes_solver_factory_class.F90:307) */
-    int32_t reserved0;
+    int32_t start_from_vectors;  /* 1: the `vectors` argument holds start vectors on entry (e.g. a mixed-precision solution) */
     double residual_threshold;   /* |A x - w x| */
     double energy_threshold;     /* |w - w_previous| */
     int32_t reserved[8];
