@@ -300,7 +300,7 @@ def run_eom(args):
     nroots = args.roots
     gpu.set_precision(MIXED)
     t0 = time.perf_counter()
-    w_mix, X, it_mix = gpu.excited_states(nroots, block=24, residual_threshold=1e-4, energy_threshold=1e-5,
+    w_mix, X, it_mix = gpu.excited_states(nroots, block=24, residual_threshold=1e-5, energy_threshold=1e-7,
                                           vectors=True, max_iterations=60)
     gpu.set_precision(FP64)
     w_ref, _, it_ref = gpu.excited_states(nroots, block=24, residual_threshold=1e-6, energy_threshold=1e-8,
@@ -346,10 +346,14 @@ def run_adjoint(args):
         return float(b @ gpu.construct_omega())
 
     for _ in range(args.directions):
+        # unit directions in each block so that h = 1e-5 is a small step
         d_t = rng.standard_normal(t.size)
+        d_t /= np.linalg.norm(d_t)
         d_L = rng.standard_normal(s.L_mo.shape)
         d_L = 0.5 * (d_L + d_L.transpose(0, 2, 1))
+        d_L /= np.linalg.norm(d_L)
         d_h = rng.standard_normal(s.h_mo.shape)
+        d_h /= np.linalg.norm(d_h)
         fd = (f(t + h * d_t, s.L_mo + h * d_L, s.h_mo + h * d_h) -
               f(t - h * d_t, s.L_mo - h * d_L, s.h_mo - h * d_h)) / (2 * h)
         ad = float(dt @ d_t + np.sum(dL * d_L) + np.sum(dh * d_h))
