@@ -209,6 +209,22 @@ class CCSD:
     def set_initial_amplitudes_guess(self):
         self._check(self.lib.ccsd_gpu_mp2_guess(self.ctx))
 
+    def save_amplitudes(self, path: str, energy: float | None = None):
+        """Write t in eT's amplitude-file layout (save_amplitudes_ccs, file_handling_ccs.F90:147-169),
+        so eT can restart from it; the energy field is the current CCSD energy unless given."""
+        from . import restart
+        e = self.calculate_energy() if energy is None else energy
+        restart.save_amplitudes(path, self.get_amplitudes(), restart.ccsd_blocks(self.n_o, self.n_v), e)
+
+    def read_amplitudes(self, path: str) -> int:
+        """Set t from an eT amplitude file (read_amplitudes_ccs, file_handling_ccs.F90:172-195).
+
+        Returns the number of values read; with singles only on file the doubles are zero."""
+        from . import restart
+        v, _, n = restart.read_amplitudes(path, restart.ccsd_blocks(self.n_o, self.n_v))
+        self.set_amplitudes(v)
+        return n
+
     def get_fock(self):
         out = np.empty(self.n_mo * self.n_mo)
         self._check(self.lib.ccsd_gpu_get_fock(self.ctx, _dp(out)))

@@ -273,6 +273,32 @@ def et_test_system(name: str, cd_threshold=None):
     return build_system(sym, xyz, golden_basis(), cd_threshold=thr)
 
 
+def et_restart_system() -> dict:
+    """eT's H2O+He/cc-pVDZ restart test (tests/restart_ccsd_v1.0) in eT's own MO basis.
+
+    The MO coefficients come from the restart files eT wrote, so L_mo and h_mo are expressed in
+    exactly the orbitals of eT's amplitudes; the Cholesky threshold is the test's 1e-12.  Also
+    returns eT's converged t, multipliers tbar, right/left EOM vectors r, l (rows) and the
+    excitation energies omega."""
+    v = golden_values()["restart_ccsd_v1.0"]
+    z = np.load(os.path.join(GOLDEN, "et_restart_h2o_he.npz"))
+    mol = molecule_from_angstrom([a[0] for a in v["atoms"]], [a[1:] for a in v["atoms"]])
+    S, Tk, V, eri = ao_integrals(mol, golden_basis())
+    C = z["C"]
+    n_o = int(z["n_o"])
+    L_ao = pivoted_cholesky(eri, v["cd_threshold"])
+    L_mo = np.einsum("mp,Jmn,nq->Jpq", C, L_ao, C, optimize=True)
+    h_mo = C.T @ (Tk + V) @ C
+    L_oo = L_mo[:, :n_o, :n_o]
+    fock_oo = (h_mo[:n_o, :n_o] + 2.0 * np.einsum("Jpq,Jkk->pq", L_oo, L_oo)
+               - np.einsum("Jpk,Jkq->pq", L_oo, L_oo))
+    e_nuc = mol.nuclear_repulsion()
+    e_hf = e_nuc + float(np.trace(h_mo[:n_o, :n_o]) + np.trace(fock_oo))
+    return dict(L_mo=L_mo, h_mo=h_mo, eps=z["eps"].copy(), n_o=n_o, e_hf=e_hf, e_nuc=e_nuc, C=C, S=S,
+                t=z["t"].copy(), tbar=z["tbar"].copy(), r=z["r"].copy(), l=z["l"].copy(),
+                omega=z["omega"].copy(), e_ccsd=v["e_ccsd"])
+
+
 # H2O at O (0,0,0), H (0, +-0.757, 0.587) Angstrom, cc-pVDZ, Cholesky threshold 1e-8:
 # the plain-FP64 drop-in workload (5 occupied, 19 virtual orbitals).
 WATER_SYMBOLS = ["O", "H", "H"]

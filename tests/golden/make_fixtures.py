@@ -12,9 +12,14 @@ It writes
 * ``et_reference_values.json`` - numbers parsed from eT's committed
   regression outputs (``tests/*/result/*.out``): geometries, HF energies,
   the (E, |Omega|) history of the DIIS ground-state solver, final CCSD
-  energies, the number of Cholesky vectors and EOM-CCSD excitation energies.
+  energies, the number of Cholesky vectors and EOM-CCSD excitation energies;
+* ``et_restart_h2o_he.npz`` - the vectors eT itself wrote for H2O+He/cc-pVDZ
+  (``tests/restart_ccsd_v1.0/old_restart_files``, eT 1.0 record files, read with
+  ``et_b200.restart``): MO coefficients and energies, converged amplitudes t,
+  multipliers tbar, and three right/left EOM-CCSD eigenvectors with their
+  excitation energies.
 
-Nothing here is executed by the tests; they only read the two JSON files.
+Nothing here is executed by the tests; they only read the files written.
 """
 
 from __future__ import annotations
@@ -80,6 +85,21 @@ def _test(root, name):
     return inp, out
 
 
+def _restart_vectors(d: str) -> None:
+    import numpy as np
+    from et_b200 import restart as rs
+    n_o, n_v, n_gs, n_es = rs.read_legacy_cc_dimensions(os.path.join(d, "cc_restart_file"))
+    n_ao = int.from_bytes(rs.read_records(os.path.join(d, "scf_restart_file"))[0], "little")
+    C, eps = rs.read_legacy_orbitals(d, n_ao)
+    w = rs.read_legacy_excitation_energies(os.path.join(d, "excitation_energies"))
+    vec = lambda name: rs.read_legacy_vector(os.path.join(d, name))
+    np.savez(os.path.join(HERE, "et_restart_h2o_he.npz"),
+             source=np.array("tests/restart_ccsd_v1.0/old_restart_files"),
+             n_o=n_o, n_v=n_v, C=C, eps=eps, t=vec("t"), tbar=vec("tbar"), omega=w,
+             r=np.stack([vec(f"r_{k + 1:03d}") for k in range(w.size)]),
+             l=np.stack([vec(f"l_{k + 1:03d}") for k in range(w.size)]))
+
+
 def main(root: str) -> None:
     values = {}
     for name in ("ccsd_gs_energy", "ccsd_lr_polarizability"):
@@ -97,10 +117,17 @@ def main(root: str) -> None:
         values[name] = dict(source=f"tests/{name}/result/{name}.out", basis=basis, atoms=atoms,
                             cd_threshold=_cd_threshold(inp), e_ccsd=_final_cc(out),
                             excitation_energies=_excitations(out))
+    name = "restart_ccsd_v1.0"
+    inp, out = _test(root, name)
+    basis, atoms = _geometry(inp)
+    values[name] = dict(source=f"tests/{name}/result/{name}.out", basis=basis, atoms=atoms,
+                        cd_threshold=_cd_threshold(inp), e_ccsd=_final_cc(out),
+                        excitation_energies=_excitations(out))
     with open(os.path.join(HERE, "et_reference_values.json"), "w") as f:
         json.dump(values, f, indent=1)
 
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    _restart_vectors(os.path.join(root, "tests", name, "old_restart_files"))
     from oracle.frontend import parse_g94
     text = open(os.path.join(root, "ao_basis", "cc-pvdz.g94")).read()
     basis = parse_g94(text, {"H", "He", "O"})
