@@ -137,10 +137,23 @@ int Context::davidson(int nstates, int side, const ccsd_gpu_davidson_options *o,
             else jacobian_transpose(c, in + c0 * namp, out + c0 * namp);
         }
     };
-    // orthonormalise `count` candidate columns against V and each other; append the survivors
+    // orthonormalise `count` candidate columns against V and each other; append the survivors.  As in
+    // davidson_tool (add_new_trial, davidson_tool_class.F90:342; orthonormalize_trial_vecs, :517) each
+    // candidate is normalised first and counts as linearly dependent when less than
+    // min(1e-11, 0.1 residual_threshold) of it is left after Gram-Schmidt
+    // (cc_es_amplitudes_solver_factory_class.F90:315); eT stops there, this solver drops the candidate.
+    const double lindep = std::min(1e-11, 0.1 * rthr);
     auto add_trials = [&](double *cand, int64_t count) {
         for (int64_t k = 0; k < count; k++) {
             double *x = cand + k * namp;
+            {
+                double c2;
+                dot(ex, x, x, namp, nrm.d());
+                CU_CHECK(cudaMemcpyAsync(&c2, nrm.d(), sizeof(double), cudaMemcpyDeviceToHost, s));
+                CU_CHECK(cudaStreamSynchronize(s));
+                if (!(c2 > 0.0)) continue;
+                axpby(ex, namp, 1.0 / std::sqrt(c2), x, 0.0, x);
+            }
             for (int pass = 0; pass < 2; pass++) {
                 if (dim > 0) {
                     // x -= V (V^T x)
@@ -152,7 +165,7 @@ int Context::davidson(int nstates, int side, const ccsd_gpu_davidson_options *o,
             double n2;
             CU_CHECK(cudaMemcpyAsync(&n2, nrm.d(), sizeof(double), cudaMemcpyDeviceToHost, s));
             CU_CHECK(cudaStreamSynchronize(s));
-            if (std::sqrt(n2) < 1e-10 || dim >= maxdim) continue;
+            if (std::sqrt(n2) < lindep || dim >= maxdim) continue;
             axpby(ex, namp, 1.0 / std::sqrt(n2), x, 0.0, V.d() + dim * namp);
             dim++;
         }
@@ -261,14 +274,20 @@ int Context::multipliers(const ccsd_gpu_davidson_options *o, double *tbar, int32
         CU_CHECK(cudaStreamSynchronize(s));
         return v;
     };
+    // normalise, Gram-Schmidt twice, drop when less than min(1e-11, 0.1 threshold) remains (as in the
+    // eigenvalue solver above)
+    const double lindep = std::min(1e-11, 0.1 * rthr);
     auto add_trial = [&](double *c) {
+        const double c2 = host_dot(c, c);
+        if (!(c2 > 0.0)) return false;
+        axpby(ex, namp, 1.0 / std::sqrt(c2), c, 0.0, c);
         for (int pass = 0; pass < 2; pass++)
             if (dim > 0) {
                 gemm(ex, true, false, dim, 1, namp, 1.0, V.d(), namp, c, namp, 0.0, proj.d(), dim, false);
                 gemm(ex, false, false, namp, 1, dim, -1.0, V.d(), namp, proj.d(), dim, 1.0, c, namp, false);
             }
         double n2 = host_dot(c, c);
-        if (std::sqrt(n2) < 1e-12 || dim >= maxdim) return false;
+        if (std::sqrt(n2) < lindep || dim >= maxdim) return false;
         axpby(ex, namp, 1.0 / std::sqrt(n2), c, 0.0, V.d() + dim * namp);
         jacobian_transpose(1, V.d() + dim * namp, AV.d() + dim * namp);
         dim++;

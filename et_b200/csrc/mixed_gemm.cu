@@ -162,23 +162,21 @@ struct EpiPairs {
 
 namespace {
 
-// Tile t of the flattened (split, m-tile, n-tile) space.  With few n-tiles the n index runs fastest
-// so the CTAs that run at the same time share A tiles in L2; otherwise the m index runs fastest.
+// Tile t of the flattened (split, m-tile, n-tile) space.  Tiles are rasterised in groups of
+// `group_m` m-tiles: inside a group the m index runs fastest, then n, so the ~148 tiles resident at
+// one time cover about group_m A panels and 148/group_m B panels, which L2 serves to all of them
+// (instead of every wave streaming the whole of A or B from HBM again).
 struct TileMap {
-    int num_mt, num_nt, nk_all, nks;
-    bool n_fast;
+    int num_mt, num_nt, nk_all, nks, group_m;
     __device__ __forceinline__ void decode(int t, int &m0, int &n0, int &z, int &kt0, int &nk) const {
         const int per_split = num_mt * num_nt;
         z = t / per_split;
         const int r = t - z * per_split;
-        int mt, nt;
-        if (n_fast) {
-            nt = r % num_nt;
-            mt = r / num_nt;
-        } else {
-            mt = r % num_mt;
-            nt = r / num_mt;
-        }
+        const int per_group = group_m * num_nt;
+        const int grp = r / per_group, in = r - grp * per_group;
+        const int first_m = grp * group_m;
+        const int gsz = min(group_m, num_mt - first_m);
+        const int mt = first_m + in % gsz, nt = in / gsz;
         m0 = mt * BM;
         n0 = nt * BN;
         kt0 = z * nks;
@@ -433,7 +431,7 @@ void launch_tc(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane
     map.num_nt = (int)(Np / BN);
     map.nk_all = (int)(Kp / BK);
     map.nks = (map.nk_all + splits - 1) / splits;
-    map.n_fast = map.num_nt <= 16;
+    map.group_m = std::min(map.num_mt, 16);
     const int num_tiles = map.num_mt * map.num_nt * splits;
     int nsm = 148;
     {
