@@ -142,8 +142,47 @@ def load_peaks():
         return 1590.0, 1400.0, 6650.0, "fallback"
 
 
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "launch_list_gs_iteration_o32_v320_J1200_mixed.md")
+
+
+def gemm_traffic(n_o, n_v, n_J):
+    """DRAM bytes per tensor-core GEMM launch (read + write) from the committed ncu launch list of
+    this workload (o=32 v=320 N_J=1200), or None for other sizes."""
+    if (n_o, n_v, n_J) != (32, 320, 1200):
+        return None
+    try:
+        for line in open(TRAFFIC_PROFILE):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def converged_solve(gpu, stream, refine, thr=1e-9, ethr=1e-11):
+    """From the MP2 start to |Omega| < thr and |dE| < ethr between iterations (certified by an FP64
+    evaluation in mixed precision): (seconds by CUDA events, iterations, energy, converged)."""
+    import torch
+    gpu.set_initial_amplitudes_guess()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    e, it, _, rc = gpu.solve_ground_state(max_iterations=60, omega_threshold=thr, energy_threshold=ethr,
+                                          refine_threshold=refine, raise_on_failure=False)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / 1e3, it, e, rc == 0
+
+
+# the accuracy the benchmark solves for: |dE| <= 1e-8 Eh against the converged FP64 energy, reached with
+# |Omega| < 1e-6 and |dE| < 1e-8 between iterations; the timed window refines toward that residual
+REFINE_TARGET = 1e-6
+
+
 def timed_solve(gpu, stream, iters, refine, world, clocks_dev=None):
-    """Exactly `iters` ground-state iterations from the MP2 start, timed with CUDA events."""
+    """Exactly `iters` ground-state iterations from the MP2 start (no early exit), timed with CUDA
+    events; mixed precision refines toward a true residual of REFINE_TARGET."""
     import torch
     gpu.set_initial_amplitudes_guess()
     torch.cuda.synchronize()
@@ -156,7 +195,8 @@ def timed_solve(gpu, stream, iters, refine, world, clocks_dev=None):
         clk.__enter__()
     ev0.record(stream)
     e, it, hist, rc = gpu.solve_ground_state(max_iterations=iters, omega_threshold=1e-30, energy_threshold=-1.0,
-                                             refine_threshold=refine, raise_on_failure=False)
+                                             refine_threshold=refine, refine_target=REFINE_TARGET,
+                                             raise_on_failure=False)
     ev1.record(stream)
     torch.cuda.synchronize()
     if clk:
@@ -215,7 +255,8 @@ def run_gpu(args):
         roof = {"kernel": "bf16x3_gemm_kernel (tcgen05 split-BF16 GEMM)", "bound": "tensor",
                 "achieved": round(achieved, 2), "peak": peak_sust, "unit": "TFLOP/s",
                 "frac": round(achieved / peak_sust, 4), "peak_kind": f"{peak_kind} bf16 sustained (timed inside a long step)",
-                "traffic": None, "launches": n_gemm, "avg_launch_ms": round(gemm_ms / n_gemm, 4),
+                "traffic": gemm_traffic(n_o, n_v, n_J), "traffic_source": "ncu launch list (profiles/), "
+                "DRAM read + write bytes per GEMM launch", "launches": n_gemm, "avg_launch_ms": round(gemm_ms / n_gemm, 4),
                 "share_of_step": round(gemm_ms / ms, 4),
                 "flops_counted": "issued tensor flops: 3 bf16 products x 2mnk per launch"}
 
@@ -226,7 +267,7 @@ def run_gpu(args):
         "dtype": "bf16x3+f64" if prec == MIXED else "f64", "data": "synthetic",
         "config": {"workload": f"CCSD ground-state iteration, synthetic Cholesky system o={n_o} v={n_v} N_J={n_J}",
                    "n_o": n_o, "n_v": n_v, "n_J": n_J, "precision": args.precision,
-                   "refine_threshold": args.refine,
+                   "refine_threshold": args.refine, "refine_target": REFINE_TARGET,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "inputs larger than L2 (t2 419 MB, L 1.19 GB at full size)",
                    "flops_per_iter": flops_iter},
@@ -240,16 +281,32 @@ def run_gpu(args):
     }
     if args.compare and world == 1 and prec == MIXED:
         # the plain FP64 GPU path on the same system: per-iteration time and converged energy
+        # time to solution from the MP2 start, FP64 path vs mixed path (mixed convergence is certified
+        # by an FP64 evaluation).  The reference energy is the tightly converged FP64 one; the target
+        # thresholds (|Omega| < 1e-6, |dE| < 1e-8 between iterations) are those that put both paths
+        # within 1e-8 Eh of it; the tight ones (1e-9, 1e-11) are reported beside them.
         gpu.set_precision(FP64)
         ms64, _, it64, _, _ = timed_solve(gpu, stream, 3, args.refine, world)
-        gpu.set_initial_amplitudes_guess()
-        e64, n64, _, rc64 = gpu.solve_ground_state(max_iterations=60, omega_threshold=1e-9, energy_threshold=1e-11,
-                                                   raise_on_failure=False)
         s64 = ms64 / 1e3 / it64
-        result["fp64_path"] = {"s_per_iter": round(s64, 5), "energy": e64, "iterations_to_1e-9": n64,
-                               "converged": rc64 == 0}
+        t64, n64, e_ref, ok64 = converged_solve(gpu, stream, args.refine, 1e-9, 1e-11)
+        t64b, n64b, e64b, ok64b = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8)
+        gpu.set_precision(MIXED)
+        tmb, itmb, emb, okmb = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8)
+        tm, itm, em, okm = converged_solve(gpu, stream, args.refine, 1e-9, 1e-11)
+        result["fp64_path"] = {"s_per_iter": round(s64, 5), "energy": e_ref, "converged": ok64,
+                               "to_1e-9": {"s": round(t64, 3), "iterations": n64},
+                               "to_target": {"s": round(t64b, 3), "iterations": n64b, "converged": ok64b,
+                                             "dE": abs(e64b - e_ref)}}
+        result["mixed_path"] = {"to_1e-9": {"s": round(tm, 3), "iterations": itm, "converged": okm,
+                                            "dE": abs(em - e_ref)},
+                                "to_target": {"s": round(tmb, 3), "iterations": itmb, "converged": okmb,
+                                              "dE": abs(emb - e_ref)}}
+        result["target"] = "|dE| <= 1e-8 Eh vs converged FP64: thresholds |Omega| < 1e-6, |dE| < 1e-8"
         result["speedup_per_iter_vs_fp64"] = round(s64 / (ms_step / 1e3), 3)
-        result["dE_vs_fp64"] = abs(e - e64)
+        result["speedup_to_target_vs_fp64"] = round(t64b / tmb, 3)
+        result["speedup_to_1e-9_vs_fp64"] = round(t64 / tm, 3)
+        result["dE_vs_fp64"] = abs(emb - e_ref)
+        result["dE_window_vs_fp64"] = abs(e - e_ref)
     gpu.close()
     if world > 1:
         import torch.distributed as dist

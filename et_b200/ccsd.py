@@ -40,7 +40,8 @@ class CCSDGPUError(RuntimeError):
 
 class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("ladder_batch", ctypes.c_int64),
-                ("mixed_min_flops", ctypes.c_int64), ("reserved", ctypes.c_int64 * 5)]
+                ("mixed_min_flops", ctypes.c_int64), ("mixed_k_chunk", ctypes.c_int64),
+                ("reserved", ctypes.c_int64 * 4)]
 
 
 class DavidsonOptions(ctypes.Structure):
@@ -52,7 +53,8 @@ class DavidsonOptions(ctypes.Structure):
 class SolverOptions(ctypes.Structure):
     _fields_ = [("max_iterations", ctypes.c_int32), ("diis_dimension", ctypes.c_int32),
                 ("omega_threshold", ctypes.c_double), ("energy_threshold", ctypes.c_double),
-                ("refine_threshold", ctypes.c_double), ("reserved", ctypes.c_int32 * 8)]
+                ("refine_threshold", ctypes.c_double), ("refine_target", ctypes.c_double),
+                ("reserved", ctypes.c_int32 * 6)]
 
 
 _lib = None
@@ -133,7 +135,8 @@ def _f64(a, n=None):
 class CCSD:
     """One Cholesky-factored closed-shell CCSD system resident on one GPU."""
 
-    def __init__(self, n_o, n_v, n_J, *, precision=FP64, device=0, ladder_batch=0, mixed_min_flops=0):
+    def __init__(self, n_o, n_v, n_J, *, precision=FP64, device=0, ladder_batch=0, mixed_min_flops=0,
+                 mixed_k_chunk=0):
         self.lib = load_library()
         self.n_o, self.n_v, self.n_J = int(n_o), int(n_v), int(n_J)
         self.n_mo = self.n_o + self.n_v
@@ -141,7 +144,7 @@ class CCSD:
         self.n_t2 = self.n_t1 * (self.n_t1 + 1) // 2
         self.n_amp = self.n_t1 + self.n_t2
         opt = Options(device=device, precision=precision, ladder_batch=ladder_batch,
-                      mixed_min_flops=mixed_min_flops)
+                      mixed_min_flops=mixed_min_flops, mixed_k_chunk=mixed_k_chunk)
         ctx = _VP()
         rc = self.lib.ccsd_gpu_create(self.n_o, self.n_v, self.n_J, ctypes.byref(opt), ctypes.byref(ctx))
         if rc != 0:
@@ -313,11 +316,15 @@ class CCSD:
         return out, it.value
 
     def solve_ground_state(self, *, max_iterations=100, diis_dimension=8, omega_threshold=1e-5,
-                           energy_threshold=1e-5, refine_threshold=1e-4, raise_on_failure=True):
-        """run_diis_cc_gs on the device; returns (energy, iterations, history[(E, |Omega|)], status)."""
+                           energy_threshold=1e-5, refine_threshold=1e-4, refine_target=0.0,
+                           raise_on_failure=True):
+        """run_diis_cc_gs on the device; returns (energy, iterations, history[(E, |Omega|)], status).
+
+        Mixed precision only: ``refine_threshold`` is |Omega| of the first FP64 refresh,
+        ``refine_target`` the true residual the refreshes aim at (0: ``omega_threshold``)."""
         opt = SolverOptions(max_iterations=max_iterations, diis_dimension=diis_dimension,
                             omega_threshold=omega_threshold, energy_threshold=energy_threshold,
-                            refine_threshold=refine_threshold)
+                            refine_threshold=refine_threshold, refine_target=refine_target)
         e = ctypes.c_double()
         it = ctypes.c_int32()
         hist = np.zeros(2 * max_iterations)
@@ -345,7 +352,9 @@ class CCSD:
         return n.value, ms.value, fl.value
 
     def selftest_gemm(self, A, B, C=None, *, alpha=1.0, beta=0.0, transA=False, transB=False, mixed=True):
-        """C = alpha op(A) op(B) + beta C on the device (diagnostics of the GEMM back ends)."""
+        """C = alpha op(A) op(B) + beta C on the device (diagnostics of the GEMM back ends).
+
+        ``mixed``: False/0 = FP64 DGEMM, True/1 = split-BF16 with 2 planes, 2 = with 3 planes."""
         A = np.asfortranarray(A, dtype=np.float64)
         B = np.asfortranarray(B, dtype=np.float64)
         m = A.shape[1] if transA else A.shape[0]

@@ -83,8 +83,7 @@ const char *ccsd_gpu_last_error(void *ctx) {
 
 int ccsd_gpu_set_precision(void *ctx, int32_t precision) {
     return guarded(ctx, [&](Context &c) {
-        REQUIRE(precision == CCSD_GPU_FP64 || precision == CCSD_GPU_MIXED, CCSD_GPU_EINVAL, "unknown precision");
-        c.ex.prec = precision == CCSD_GPU_MIXED ? ccsd::Prec::MIXED : ccsd::Prec::FP64;
+        c.set_precision(precision);
     });
 }
 
@@ -335,8 +334,18 @@ int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t tra
         h2d(c, dA.d(), A, na);
         h2d(c, dB.d(), B, nb);
         h2d(c, dC.d(), C, nc);
-        if (mixed) ccsd::mixed_gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc);
-        else ccsd::gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc, false);
+        REQUIRE(mixed >= 0 && mixed <= 2, CCSD_GPU_EINVAL, "mixed must be 0, 1 or 2");
+        if (mixed) {
+            const int planes = c.ex.planes;
+            c.ex.planes = mixed == 2 ? 3 : 2;
+            try {
+                ccsd::mixed_gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc);
+            } catch (...) {
+                c.ex.planes = planes;
+                throw;
+            }
+            c.ex.planes = planes;
+        } else ccsd::gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc, false);
         d2h(c, C, dC.d(), nc);
         REQUIRE(ccsd::mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM wait timed out");
     });

@@ -5,6 +5,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 
@@ -43,8 +45,9 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     set_stream(nullptr);
     ex.blas = blas;
     ex.prof = &prof;
-    ex.prec = (opt && opt->precision == CCSD_GPU_MIXED) ? Prec::MIXED : Prec::FP64;
+    set_precision(opt ? opt->precision : CCSD_GPU_FP64);
     if (opt && opt->mixed_min_flops > 0) ex.mixed_min_flops = (double)opt->mixed_min_flops;
+    if (opt && opt->mixed_k_chunk != 0) ex.k_chunk = opt->mixed_k_chunk;
     ladder_batch = opt ? opt->ladder_batch : 0;
     cudaStream_t s = ex.stream;
     for (auto *b : {&L_oo, &Lt_oo}) *b = dalloc(nJ * no * no, s);
@@ -272,6 +275,11 @@ void Context::ladder(const double *Lvv, const double *t2, double *om2) {
     }
 }
 
+void Context::set_precision(int32_t precision) {
+    REQUIRE(precision == CCSD_GPU_FP64 || precision == CCSD_GPU_MIXED, CCSD_GPU_EINVAL, "unknown precision");
+    ex.prec = precision == CCSD_GPU_FP64 ? Prec::FP64 : Prec::MIXED;
+}
+
 // Tensor-core form of the same ladder.  With M_ab[c,d] = g_acbd the +/- sums of
 // omega_ccsd_a2 over packed c >= d equal sums over all (c, d):
 //   omega+_ij,ab = sum_cd 1/2 (1 - d_ij/2)(t_cidj + t_cjdi) M_ab[c,d]
@@ -282,9 +290,10 @@ void Context::ladder_tc(const double *Lvv, const double *t2, double *om2) {
     cudaStream_t s = ex.stream;
     const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
     const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
+    const int np = ex.planes;
     // split L~_vv rows r = c + nv a (K = J): source element (r, J) = L~[J, a, c] at J + nJ (a + nv c)
     const int64_t l_rows = tc_pad_rows_a(nv2);
-    DBuf LS(sizeof(__nv_bfloat16) * 2 * l_rows * Jp, s);
+    DBuf LS(sizeof(__nv_bfloat16) * np * l_rows * Jp, s);
     {
         // r = c + nv a  ->  offset nJ*(a + nv*c): not a single stride, so split from the (J, c, a) copy
         DBuf LT = dalloc(nJ * nv2, s);
@@ -302,12 +311,13 @@ void Context::ladder_tc(const double *Lvv, const double *t2, double *om2) {
         split_rows(ex, LT.d(), nJ, 1, nv2, nJ, l_rows, Jp, LS.as<__nv_bfloat16>());
     }
     const int64_t rows_T = tc_pad_rows_b(nrow);
-    DBuf TS(sizeof(__nv_bfloat16) * 2 * rows_T * Kq, s);
-    build_T(ex, t2, no, nv, rows_T, Kq, TS.as<__nv_bfloat16>());
-    // all pair integrals, resident: [2][mrows][Kq]
+    DBuf TS(sizeof(__nv_bfloat16) * np * rows_T * Kq, s);
+    build_T(ex, t2, no, nv, rows_T, Kq, np, TS.as<__nv_bfloat16>());
+    // all pair integrals, resident: [np][mrows][Kq] (padding rows / K positions are never written, so
+    // they stay zero when the plane count changes)
     const int64_t mrows = tc_pad_rows_a(nab);
-    if (mbuf_bytes < sizeof(__nv_bfloat16) * 2 * (size_t)mrows * Kq) {
-        mbuf = DBuf(sizeof(__nv_bfloat16) * 2 * (size_t)mrows * Kq, s);
+    if (mbuf_bytes < sizeof(__nv_bfloat16) * np * (size_t)mrows * Kq) {
+        mbuf = DBuf(sizeof(__nv_bfloat16) * np * (size_t)mrows * Kq, s);
         mbuf_bytes = mbuf.bytes();
         CU_CHECK(cudaMemsetAsync(mbuf.as<void>(), 0, mbuf_bytes, s));   // padding rows / K stay zero
     }
@@ -333,6 +343,7 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     const double othr = o && o->omega_threshold > 0 ? o->omega_threshold : 1e-5;
     const double ethr = o ? o->energy_threshold : 1e-5;
     const double refine = o && o->refine_threshold > 0 ? o->refine_threshold : 1e-4;
+    const double rtarget = o && o->refine_target > 0 ? o->refine_target : othr;
     cudaStream_t s = ex.stream;
     orbital_differences(ex, eps.d(), no, nv, epsdiff.d());
     DBuf omega_v = dalloc(namp, s);
@@ -346,14 +357,40 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     std::vector<int> order;   // slots, oldest first
     const Prec user = ex.prec;
     const bool mixed = (user == Prec::MIXED);
+    // the arithmetic changes during the solve; the caller's choice is restored on every exit
+    struct Restore {
+        Exec &ex;
+        Prec prec;
+        int planes;
+        ~Restore() {
+            ex.prec = prec;
+            ex.planes = planes;
+        }
+    } restore{ex, ex.prec, ex.planes};
     // Mixed precision with defect correction: Omega~(t) = Omega_mixed(t) + c, where
-    // c = Omega_fp64(t_c) - Omega_mixed(t_c) is refreshed with one FP64 evaluation when
-    // |Omega~| first drops below refine_threshold and whenever |Omega~| meets the convergence
-    // test (that FP64 evaluation is also the convergence check).  The remaining error
-    // (Omega_fp64 - Omega_mixed)(t) - c is linear in t - t_c with the ~1e-5 relative error of the
-    // mixed Jacobian, so one or two FP64 evaluations finish the solve.
+    // c = Omega_fp64(t_c) - Omega_mixed(t_c) is refreshed by one FP64 evaluation at a time.  The mixed
+    // error d(t) = Omega_fp64(t) - Omega_mixed(t) is mostly frozen, but the truncating FP32
+    // accumulation of the tensor cores rounds differently as soon as t changes, so d drifts even for
+    // tiny steps (a 1e-10 step moves it by ~2e-9, a long solve path by ~4e-7 at o=32, v=320):
+    // iterating on Omega~ lowers the true residual only down to that drift.  The policy:
+    //  * first refresh when |Omega_mixed| < refine_threshold;
+    //  * refresh again when |Omega~| meets the convergence test (the refresh is then the FP64
+    //    convergence check), when it stops falling (no 30% reduction in three iterations), or, if
+    //    the expected drift is above refine_target (default: the residual threshold), once |Omega~|
+    //    is below half of it
+    //    (further mixed iterations would not lower the true residual).  The expected drift is what
+    //    the previous refresh measured; after the first refresh, which measures the whole mixed
+    //    error d rather than its drift, it is 0.15 |d| (the ratio seen along bf16x3 solve paths);
+    //  * a refresh that finds the residual function moved by more than 0.3 of a true residual still
+    //    above refine_target (drift dominates), or a cycle that gained less than a factor 2, hands
+    //    the remaining iterations to FP64.
+    // A refresh changes the residual function by the same vector c_new - c_old at every t (up to the
+    // drift), so the stored DIIS error vectors are shifted by its quasi-Newton image (and their Gram
+    // matrix recomputed) instead of restarting the DIIS subspace.
     DBuf om_mixed = mixed ? dalloc(namp, s) : DBuf(), corr = mixed ? dalloc(namp, s) : DBuf();
+    DBuf moved_v = mixed ? dalloc(namp, s) : DBuf();
     bool have_corr = false;
+    double r_c = 0.0, drift_est = 0.0;
     double prev = 0.0, e = 0.0;
     int it = 0;
     bool conv = false;
@@ -364,21 +401,54 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         CU_CHECK(cudaStreamSynchronize(s));
         return std::sqrt(nrm2);
     };
-    // FP64 Omega at the current t into omega_v; the correction becomes Omega_fp64 - Omega_mixed
     bool reset_diis = false, fp64_final = false;
     int last_check = 0;
     std::vector<double> norms;
+    // CCSD_GPU_TRACE=1: one line per iteration on stderr with the refinement decisions
+    const bool trace = std::getenv("CCSD_GPU_TRACE") && std::getenv("CCSD_GPU_TRACE")[0] == '1';
+    double trace_moved = 0.0;
+    const char *trace_why = "";
+    // shift every stored DIIS error vector by v and rebuild their Gram matrix
+    auto shift_diis = [&](const double *v) {
+        const int n = (int)order.size();
+        if (n == 0) return;
+        for (int k = 0; k < n; k++) axpby(ex, namp, 1.0, v, 1.0, errs[order[k]].d());
+        std::vector<const double *> ptr(n);
+        for (int k = 0; k < n; k++) ptr[k] = errs[order[k]].d();
+        DBuf g = dalloc(16 * 16, s);
+        for (int k = 0; k < n; k++) multi_dot(ex, ptr[k], ptr.data(), n, namp, g.d() + 16 * k);
+        std::vector<double> gh(16 * 16), G(16 * 16, 0.0);
+        CU_CHECK(cudaMemcpyAsync(gh.data(), g.d(), sizeof(double) * 256, cudaMemcpyDeviceToHost, s));
+        CU_CHECK(cudaMemcpyAsync(G.data(), Gs.d(), sizeof(double) * 256, cudaMemcpyDeviceToHost, s));
+        CU_CHECK(cudaStreamSynchronize(s));
+        for (int a = 0; a < n; a++)
+            for (int b = 0; b < n; b++) G[order[a] * 16 + order[b]] = gh[16 * a + b];
+        CU_CHECK(cudaMemcpyAsync(Gs.d(), G.data(), sizeof(double) * 256, cudaMemcpyHostToDevice, s));
+    };
+    // FP64 Omega at the current t into omega_v (which holds Omega~ on entry); the correction becomes
+    // Omega_fp64 - Omega_mixed
     auto fp64_check = [&]() {
-        // a refreshed correction changes the residual function: restart the DIIS subspace
-        if (have_corr) reset_diis = true;
         last_check = it;
+        CU_CHECK(cudaMemcpyAsync(moved_v.d(), omega_v.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
         ex.prec = Prec::FP64;
         omega(omega_v.d());
         ex.prec = user;
         CU_CHECK(cudaMemcpyAsync(corr.d(), omega_v.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
         axpby(ex, namp, -1.0, om_mixed.d(), 1.0, corr.d());
+        axpby(ex, namp, 1.0, omega_v.d(), -1.0, moved_v.d());   // c_new - c_old
+        const double moved = norm_of(moved_v.d()), nrm64 = norm_of(omega_v.d());
+        trace_moved = moved;
+        drift_est = have_corr ? moved : 0.15 * moved;
+        if (have_corr && ((moved > 0.3 * nrm64 && nrm64 >= rtarget) || nrm64 > 0.5 * r_c)) fp64_final = true;
+        if (fp64_final) {
+            reset_diis = true;
+        } else {
+            qn_precondition(ex, moved_v.d(), epsdiff.d(), namp, nt1);
+            shift_diis(moved_v.d());
+        }
+        r_c = nrm64;
         have_corr = true;
-        return norm_of(omega_v.d());
+        return nrm64;
     };
     while (it < maxit) {
         it++;
@@ -397,19 +467,21 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
             CU_CHECK(cudaMemcpyAsync(omega_v.d(), om_mixed.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
             if (have_corr) axpby(ex, namp, 1.0, corr.d(), 1.0, omega_v.d());
             nrm = norm_of(omega_v.d());
-            bool econv0 = ethr < 0 || std::fabs(e - prev) < ethr;
-            // the corrected mixed residual has reached the noise floor of the bf16x3 products when it
-            // stops falling (no 30% reduction over three iterations): finish in FP64
-            bool stalled = have_corr && it - last_check > 3 && norms.size() >= 3 &&
-                           nrm > 0.7 * norms[norms.size() - 3];
-            if ((!have_corr && nrm < refine) || (have_corr && nrm < othr && econv0) || stalled) {
+            const bool econv0 = ethr < 0 || std::fabs(e - prev) < ethr;
+            const bool stalled = it - last_check > 3 && norms.size() >= 3 && nrm > 0.7 * norms[norms.size() - 3];
+            const bool below = have_corr && drift_est > rtarget && nrm < 0.5 * drift_est;
+            trace_moved = 0.0;
+            trace_why = "";
+            if ((!have_corr && nrm < refine) || (nrm < othr && econv0) || below || stalled) {
+                trace_why = !have_corr ? "refine" : (nrm < othr && econv0) ? "check" : below ? "cycle" : "stall";
+                if (trace) std::fprintf(stderr, "ccsd_gpu gs %3d  mixed |Omega~| %.3e\n", it, nrm);
                 nrm = fp64_check();
                 exact = true;
-                if (stalled) {
-                    fp64_final = true;
-                    reset_diis = true;
-                }
             }
+        }
+        if (trace) {
+            std::fprintf(stderr, "ccsd_gpu gs %3d  E %.12f  |Omega| %.3e  %s  %-6s moved %.3e r_c %.3e%s\n", it, e, nrm,
+                         exact ? "fp64 " : "mixed", trace_why, trace_moved, r_c, fp64_final ? "  fp64 from here" : "");
         }
         if (!std::isfinite(nrm) || !std::isfinite(e)) {
             ex.prec = user;

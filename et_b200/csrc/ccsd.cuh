@@ -44,6 +44,7 @@ struct Context {
     void t1_transform_cholesky();
     void construct_fock();
     void refresh();                        // T1 transformation + Fock at the current t
+    void set_precision(int32_t precision);   // CCSD_GPU_FP64 / CCSD_GPU_MIXED
     DBuf g_ovov();
     double energy();
     void mp2_guess();

@@ -103,7 +103,7 @@ __global__ void add_omega_pm_kernel(double *__restrict__ om2, const double *__re
 // 1/2 (1 - d_ij/2)(t_cidj + t_cjdi), row n_o_p + ij_m (i > j) carries 1/2 (t_cidj - t_cjdi),
 // both at K position c + nv*d; padding rows/columns are zero.
 __global__ void build_T_kernel(const double *__restrict__ t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq,
-                               __nv_bfloat16 *__restrict__ out) {
+                               int np, __nv_bfloat16 *__restrict__ out) {
     const int64_t nop = no * (no + 1) / 2, nrow = no * no, nv2 = nv * nv;
     const size_t plane = (size_t)rows_pad * Kq;
     GRID_STRIDE(idx, rows_pad * Kq) {
@@ -121,9 +121,11 @@ __global__ void build_T_kernel(const double *__restrict__ t2, int64_t no, int64_
             double y = t2[pk(c + nv * j, d + nv * i)];
             val = plus ? 0.5 * (i == j ? 0.5 : 1.0) * (x + y) : 0.5 * (x - y);
         }
-        __nv_bfloat16 hi = __double2bfloat16(val);
-        out[idx] = hi;
-        out[plane + idx] = __double2bfloat16(val - (double)__bfloat162float(hi));
+        for (int p = 0; p < np; p++) {
+            __nv_bfloat16 q = __double2bfloat16(val);
+            out[p * plane + idx] = q;
+            val -= (double)__bfloat162float(q);
+        }
     }
 }
 
@@ -279,6 +281,17 @@ __global__ void qn_update_kernel(double *__restrict__ omega, const double *__res
     }
 }
 
+// the quasi-Newton image of a residual without the amplitude update: v <- -v / eps, doubles
+// diagonal x2 (the DIIS error vector of quasi_newton_updater_class.F90)
+__global__ void qn_precondition_kernel(double *__restrict__ v, const double *__restrict__ epsdiff, int64_t n,
+                                       int64_t nt1) {
+    GRID_STRIDE(k, n) {
+        double r = -v[k] / epsdiff[k];
+        if (is_doubles_diag(k, nt1)) r *= 2.0;
+        v[k] = r;
+    }
+}
+
 __global__ void scale_doubles_diag_kernel(double *__restrict__ x, int64_t nov, int64_t nt1, double f) {
     GRID_STRIDE(M, nov) {
         x[nt1 + M * (M + 1) / 2 + M] *= f;
@@ -382,8 +395,9 @@ void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int
     CU_CHECK(cudaGetLastError());
 }
 
-void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, __nv_bfloat16 *out) {
-    build_T_kernel<<<grid_for(rows_pad * Kq, 256), 256, 0, ex.stream>>>(t2, no, nv, rows_pad, Kq, out);
+void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
+             __nv_bfloat16 *out) {
+    build_T_kernel<<<grid_for(rows_pad * Kq, 256), 256, 0, ex.stream>>>(t2, no, nv, rows_pad, Kq, np, out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }
@@ -440,6 +454,12 @@ void trace_oo(Exec &ex, const double *L_oo, int64_t nJ, int64_t no, double *X) {
 
 void qn_update(Exec &ex, double *omega, const double *epsdiff, double *t, int64_t n, int64_t nt1) {
     qn_update_kernel<<<grid_for(n, 256), 256, 0, ex.stream>>>(omega, epsdiff, t, n, nt1);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void qn_precondition(Exec &ex, double *v, const double *epsdiff, int64_t n, int64_t nt1) {
+    qn_precondition_kernel<<<grid_for(n, 256), 256, 0, ex.stream>>>(v, epsdiff, n, nt1);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }

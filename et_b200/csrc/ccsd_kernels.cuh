@@ -21,8 +21,10 @@ void form_gpm(Exec &ex, const double *G, int64_t ldg, double *gp, double *gm, in
 void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int64_t no, int64_t nv, int64_t a0,
                   int64_t a1);
 
-// T+/T- rows of the tensor-core ladder (split bf16, [2][rows_pad][Kq]) and the scatter of its result
-void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, __nv_bfloat16 *out);
+// T+/T- rows of the tensor-core ladder (np split-bf16 planes, [np][rows_pad][Kq]) and the scatter of
+// its result
+void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
+             __nv_bfloat16 *out);
 void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv);
 
 // eta of the multiplier equation (construct_eta_ccsd, multiplier_equation_ccsd.F90:50-113) and the
@@ -36,6 +38,8 @@ void orbital_differences(Exec &ex, const double *eps, int64_t no, int64_t nv, do
 void mp2_amplitudes(Exec &ex, const double *g_vovo, const double *epsdiff, int64_t nov, double *t2);
 void trace_oo(Exec &ex, const double *L_oo, int64_t nJ, int64_t no, double *X);
 void qn_update(Exec &ex, double *omega, const double *epsdiff, double *t, int64_t n, int64_t nt1);
+// v <- the quasi-Newton image of the residual v (-v / eps, doubles diagonal x2), t untouched
+void qn_precondition(Exec &ex, double *v, const double *epsdiff, int64_t n, int64_t nt1);
 void scale_doubles_diag(Exec &ex, double *x, int64_t nov, int64_t nt1, double f);
 void diis_solve(Exec &ex, double *Gslot, int maxdim, const double *dots, int new_slot, const DiisOrder &order,
                 double *w, int *status);

@@ -1,11 +1,19 @@
-// Split-BF16 GEMM for sm_100a: D = alpha * (Ahi Bhi^T + Ahi Blo^T + Alo Bhi^T) + beta * C.
+// Split-BF16 GEMM for sm_100a: D = alpha * sum_(p,q) A_p B_q^T + beta * C over bf16 planes.
 //
-// FP64 operands are converted once per call into bf16 hi/lo planes, K-major and zero padded
-// (M to 128, N to BN, K to 64).  The kernel is warp specialised: one thread issues TMA loads
-// of the four 128B-swizzled operand tiles into a ring of shared-memory stages, one thread
-// issues tcgen05.mma (kind::f16, FP32 accumulation in TMEM) for the three products of every
-// 16-wide K slice, and all four warps drain the 128 x BN accumulator through tcgen05.ld and
-// write FP64 column-major output (alpha/beta applied in FP64).  Every mbarrier wait is bounded;
+// FP64 operands are converted once per call into NP bf16 planes (x = x_0 + x_1 [+ x_2], each plane
+// the bf16 rounding of what the planes before it leave), K-major and zero padded (M to 128, N to
+// 256, K to 64).  Two modes:
+//   bf16x3: NP = 2, products (0,0) (0,1) (1,0), N tile 256            (~16 significant bits)
+//   bf16x6: NP = 3, products (0,0) (0,1) (1,0) (0,2) (1,1) (2,0), N tile 128   (~24 bits)
+// Both keep two 96 KB shared-memory stages.  The kernel is persistent and warp specialised: one
+// thread issues TMA loads of the 128B-swizzled operand tiles into the ring of stages, one thread
+// issues tcgen05.mma (kind::f16, FP32 accumulation in TMEM) for every product of every 16-wide K
+// slice, and four warps drain the 128 x BN accumulator through tcgen05.ld and write FP64
+// column-major output (alpha/beta applied in FP64).  The tensor cores' FP32
+// accumulation loses a little at every MMA step, so long K ranges are cut into chunks
+// (Exec::k_chunk, 4096 by default): each chunk accumulates in one TMEM buffer and the epilogue
+// adds it to the FP64 output while the next chunk accumulates in the other; the same CTA takes
+// the chunks of a tile in order, so the sum is deterministic.  Every mbarrier wait is bounded;
 // on time-out the kernel records an error code, skips its remaining work and frees its TMEM.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -20,17 +28,35 @@ namespace ccsd {
 namespace {
 
 constexpr int BM = 128;
-constexpr int BN = 256;
 constexpr int BK = 64;                     // one 128-byte swizzle row of bf16
 constexpr int STAGES = 2;
-constexpr int A_TILE = BM * BK * 2;        // bytes per plane
-constexpr int B_TILE = BN * BK * 2;
-constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int B_ROW_PAD = 256;             // B operand rows are padded to 256 in both modes
 constexpr int THREADS = 192;              // producer warp, MMA warp, four epilogue warps
 constexpr int EPI_THREADS = 128;
-constexpr uint32_t TMEM_COLS = 2 * BN;     // two FP32 accumulators of 128 lanes x BN columns
 constexpr long long WAIT_CYCLES = 4000000000ll;   // ~2 s at 2 GHz: far above any legitimate wait
+
+// plane count and N tile of one mode
+template <int NP_, int BN_>
+struct Mode {
+    static constexpr int NP = NP_;
+    static constexpr int BN = BN_;
+    static constexpr int NPROD = NP == 2 ? 3 : 6;
+    static constexpr int A_TILE = BM * BK * 2;       // bytes per plane
+    static constexpr int B_TILE = BN * BK * 2;
+    static constexpr int STAGE_BYTES = NP * (A_TILE + B_TILE);
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    static constexpr uint32_t TMEM_COLS = 2 * BN;    // two FP32 accumulators of 128 lanes x BN columns
+    // kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = BN
+    static constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    // plane pair (A plane, B plane) of product p, largest products first
+    __host__ __device__ static constexpr int pa(int p) { return p == 2 || p == 4 ? 1 : (p == 5 ? 2 : 0); }
+    __host__ __device__ static constexpr int pb(int p) { return p == 1 || p == 4 ? 1 : (p == 3 ? 2 : 0); }
+};
+using ModeX3 = Mode<2, 256>;
+using ModeX6 = Mode<3, 128>;
+static_assert(ModeX3::STAGE_BYTES == 96 * 1024 && ModeX6::STAGE_BYTES == 96 * 1024, "stage size");
+static_assert(B_ROW_PAD % ModeX3::BN == 0 && B_ROW_PAD % ModeX6::BN == 0, "B padding");
 
 __device__ int g_mixed_gemm_error = 0;
 
@@ -85,15 +111,13 @@ __device__ __forceinline__ uint64_t smem_desc(const void *tile, uint32_t k_byte_
     return d;
 }
 
-// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = BN
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate));
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -117,6 +141,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 
 // FP64 column-major output with alpha/beta
 struct EpiF64 {
+    static constexpr bool kChunked = true;   // can accumulate K chunks into the output
     double *C;
     long long ldc;
     int M, N;
@@ -125,38 +150,59 @@ struct EpiF64 {
     long long zoff = 0;
     __device__ __forceinline__ void tile_setup(int z) { zoff = (long long)z * zstride; }
     __device__ __forceinline__ void row_setup(int) {}
-    __device__ __forceinline__ void operator()(int row, int col, float v) const {
-        if (row < M && col < N) {
-            double *dst = C + zoff + (long long)col * ldc + row;
-            double r = alpha * (double)v;
-            if (beta != 0.0) r += beta * *dst;
-            *dst = r;
+    // 16 consecutive columns of one row.  first: the first K chunk of the tile (beta applies);
+    // later chunks add to what is there, in FP64.  The 16 old values are loaded before any store so
+    // their L2 latencies overlap.
+    __device__ __forceinline__ void apply16(int row, int col0, const float (&v)[16], bool first) const {
+        if (row >= M) return;
+        double *base = C + zoff + (long long)col0 * ldc + row;
+        const bool need_old = !first || beta != 0.0;
+        double old[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) old[j] = (need_old && col0 + j < N) ? __ldcg(base + (long long)j * ldc) : 0.0;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            if (col0 + j < N) {
+                double r = alpha * (double)v[j];
+                if (!first) r += old[j];
+                else if (beta != 0.0) r += beta * old[j];
+                base[(long long)j * ldc] = r;
+            }
         }
     }
 };
 
 // A2 ladder integrals: row (c, a) = c + nv*(a - a0), column (d, b) = d + nv*b of
-// G = L_vv^T L_vv is M_ab[c,d] = g_acbd; kept for b <= a and written as split bf16 at
+// G = L_vv^T L_vv is M_ab[c,d] = g_acbd; kept for b <= a and written as np bf16 planes at
 // pair row ab = a(a+1)/2 + b, K position c + nv*d.
 struct EpiPairs {
+    static constexpr bool kChunked = false;
     __nv_bfloat16 *out;
     size_t plane;
     long long ldk;
-    int nv, a0, M, N;
+    int nv, a0, M, N, np;
     int a, c;
     __device__ __forceinline__ void tile_setup(int) {}
     __device__ __forceinline__ void row_setup(int row) {
         a = a0 + row / nv;
         c = row - (row / nv) * nv;
     }
-    __device__ __forceinline__ void operator()(int row, int col, float v) const {
+    // the pair epilogue stores bf16 planes, so it takes the whole K range as one chunk
+    __device__ __forceinline__ void apply16(int row, int col0, const float (&v)[16], bool) const {
+#pragma unroll
+        for (int j = 0; j < 16; j++) store(row, col0 + j, v[j]);
+    }
+    __device__ __forceinline__ void store(int row, int col, float v) const {
         if (row >= M || col >= N) return;
         const int b = col / nv, d = col - b * nv;
         if (b > a) return;
         const size_t idx = (size_t)((long long)a * (a + 1) / 2 + b) * ldk + c + (long long)nv * d;
         __nv_bfloat16 hi = __float2bfloat16(v);
+        const float r = v - __bfloat162float(hi);   // exact in FP32
+        __nv_bfloat16 mid = __float2bfloat16(r);
         out[idx] = hi;
-        out[plane + idx] = __float2bfloat16(v - __bfloat162float(hi));
+        out[plane + idx] = mid;
+        if (np == 3) out[2 * plane + idx] = __float2bfloat16(r - __bfloat162float(mid));
     }
 };
 
@@ -167,7 +213,8 @@ namespace {
 // one time cover about group_m A panels and 148/group_m B panels, which L2 serves to all of them
 // (instead of every wave streaming the whole of A or B from HBM again).
 struct TileMap {
-    int num_mt, num_nt, nk_all, nks, group_m;
+    int num_mt, num_nt, nk_all, nks, group_m, bn;
+    int kc;   // K blocks accumulated in TMEM before the epilogue takes the partial sum (FP64)
     __device__ __forceinline__ void decode(int t, int &m0, int &n0, int &z, int &kt0, int &nk) const {
         const int per_split = num_mt * num_nt;
         z = t / per_split;
@@ -178,19 +225,22 @@ struct TileMap {
         const int gsz = min(group_m, num_mt - first_m);
         const int mt = first_m + in % gsz, nt = in / gsz;
         m0 = mt * BM;
-        n0 = nt * BN;
+        n0 = nt * bn;
         kt0 = z * nks;
         nk = min(nks, nk_all - kt0);
     }
 };
 
 // Persistent, warp-specialised: warp 0 = TMA producer, warp 1 = MMA issuer (and TMEM owner),
-// warps 2..5 = epilogue.  Two 128 x BN FP32 accumulators in TMEM (512 columns) let the epilogue
-// of one tile overlap the main loop of the next.
-template <class Epi>
+// warps 2..5 = epilogue.  Two 128 x BN FP32 accumulators in TMEM let the epilogue of one
+// accumulation unit overlap the main loop of the next.
+template <class MD, class Epi>
 __global__ void __launch_bounds__(THREADS, 1)
-bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TileMap map,
+split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TileMap map,
                    int num_tiles, Epi epi) {
+    constexpr int NP = MD::NP, BN = MD::BN, A_TILE = MD::A_TILE, B_TILE = MD::B_TILE;
+    constexpr int STAGE_BYTES = MD::STAGE_BYTES;
+    constexpr uint32_t TMEM_COLS = MD::TMEM_COLS;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -244,20 +294,24 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
                     uint8_t *st = smem + s * STAGE_BYTES;
                     mbar_expect_tx(&full[s], STAGE_BYTES);
                     const int k0 = (kt0 + i) * BK;
-                    tma_load_3d(&tmA, &full[s], st, k0, m0, 0);                       // A hi
-                    tma_load_3d(&tmA, &full[s], st + A_TILE, k0, m0, 1);              // A lo
-                    tma_load_3d(&tmB, &full[s], st + 2 * A_TILE, k0, n0, 0);          // B hi
-                    tma_load_3d(&tmB, &full[s], st + 2 * A_TILE + B_TILE, k0, n0, 1); // B lo
+#pragma unroll
+                    for (int p = 0; p < NP; p++) {
+                        tma_load_3d(&tmA, &full[s], st + p * A_TILE, k0, m0, p);
+                        tma_load_3d(&tmB, &full[s], st + NP * A_TILE + p * B_TILE, k0, n0, p);
+                    }
                 }
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {
             // MMA issuer
+            // one accumulation unit = one K chunk of one tile; units alternate between the two
+            // TMEM accumulators
             int g = 0, tc = 0;
-            for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x, tc++) {
+            for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
                 int m0, n0, z, kt0, nk;
                 map.decode(t, m0, n0, z, kt0, nk);
+                for (int c0 = 0; c0 < nk && !*abort_flag; c0 += map.kc, tc++) {
                 const int acc = tc & 1;
                 if (!mbar_wait(&acc_empty[acc], ((tc >> 1) & 1) ^ 1)) {
                     atomicExch(&g_mixed_gemm_error, 4);
@@ -266,7 +320,8 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d = tmem + (uint32_t)(acc * BN);
-                for (int i = 0; i < nk; i++, g++) {
+                const int c1 = min(nk, c0 + map.kc);
+                for (int i = c0; i < c1; i++, g++) {
                     const int s = g % STAGES;
                     if (!mbar_wait(&full[s], (g / STAGES) & 1) || *abort_flag) {
                         atomicExch(&g_mixed_gemm_error, 2);
@@ -275,17 +330,21 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint8_t *st = smem + s * STAGE_BYTES;
-                    const uint8_t *ahi = st, *alo = st + A_TILE, *bhi = st + 2 * A_TILE, *blo = st + 2 * A_TILE + B_TILE;
 #pragma unroll
                     for (int kk = 0; kk < BK / 16; kk++) {
                         const uint32_t ko = kk * 32;   // 16 bf16 = 32 bytes inside the swizzled row
-                        mma_bf16(d, smem_desc(ahi, ko), smem_desc(bhi, ko), (i > 0 || kk > 0) ? 1u : 0u);
-                        mma_bf16(d, smem_desc(ahi, ko), smem_desc(blo, ko), 1u);
-                        mma_bf16(d, smem_desc(alo, ko), smem_desc(bhi, ko), 1u);
+#pragma unroll
+                        for (int p = 0; p < MD::NPROD; p++) {
+                            const uint8_t *ta = st + MD::pa(p) * A_TILE;
+                            const uint8_t *tb = st + NP * A_TILE + MD::pb(p) * B_TILE;
+                            mma_bf16(d, smem_desc(ta, ko), smem_desc(tb, ko), MD::IDESC,
+                                     (i > c0 || kk > 0 || p > 0) ? 1u : 0u);
+                        }
                     }
                     mma_commit(&empty[s]);   // frees the stage once these MMAs have read it
                 }
                 mma_commit(&acc_full[acc]);  // accumulator ready for the epilogue
+                }
             }
             mma_commit(done);                // every MMA of this CTA has completed
         }
@@ -293,15 +352,18 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
         // epilogue: warp w reads TMEM lanes 32*(w % 4) .. +31
         const int quarter = warp & 3;
         int tc = 0;
-        for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, tc++) {
+        bool aborted = false;
+        for (int t = blockIdx.x; t < num_tiles && !aborted; t += gridDim.x) {
             int m0, n0, z, kt0, nk;
             map.decode(t, m0, n0, z, kt0, nk);
+            for (int c0 = 0; c0 < nk; c0 += map.kc, tc++) {
             const int acc = tc & 1;
             bool ok = !*abort_flag && mbar_wait(&acc_full[acc], (tc >> 1) & 1);
             __syncwarp();
             if (!ok || *abort_flag) {
                 atomicExch(&g_mixed_gemm_error, 3);
                 *abort_flag = 1;
+                aborted = true;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -310,14 +372,14 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
             epi.row_setup(row);
             const uint32_t base = tmem + (uint32_t)(acc * BN) + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 16) {
+            for (int cc = 0; cc < BN; cc += 16) {
                 float v[16];
-                tmem_ld16(base + (uint32_t)c0, v);
-#pragma unroll
-                for (int j = 0; j < 16; j++) epi(row, n0 + c0 + j, v[j]);
+                tmem_ld16(base + (uint32_t)cc, v);
+                epi.apply16(row, n0 + cc, v, c0 == 0);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[acc])) : "memory");
+            }
         }
     }
     __syncthreads();
@@ -329,11 +391,12 @@ bf16x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
     }
 }
-// FP64 (strided view of op(X): element (r, k) at src[r*sr + k*sk]) -> bf16 hi/lo planes,
-// K-major [plane][R_pad][K_pad], zero padded.  32x32 smem tile so both sides stay coalesced;
-// blockIdx.x runs over row blocks (up to 2^31), blockIdx.y strides over K blocks.
+// FP64 (strided view of op(X): element (r, k) at src[r*sr + k*sk]) -> np bf16 planes, K-major
+// [plane][R_pad][K_pad], zero padded: plane p holds the bf16 rounding of x minus the planes before
+// it.  32x32 smem tile so both sides stay coalesced; blockIdx.x runs over row blocks (up to
+// 2^31), blockIdx.y strides over K blocks.
 __global__ void split_bf16_kernel(const double *__restrict__ src, long long sr, long long sk, int R, int K, int Rp,
-                                  int Kp, __nv_bfloat16 *__restrict__ out) {
+                                  int Kp, int np, __nv_bfloat16 *__restrict__ out) {
     __shared__ double tile[32][33];
     const int r0 = blockIdx.x * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -358,10 +421,12 @@ __global__ void split_bf16_kernel(const double *__restrict__ src, long long sr, 
             const int r = r0 + i, k = k0 + tx;
             if (r < Rp && k < Kp) {
                 double x = tile[i][tx];
-                __nv_bfloat16 hi = __double2bfloat16(x);
-                __nv_bfloat16 lo = __double2bfloat16(x - (double)__bfloat162float(hi));
-                out[(size_t)r * Kp + k] = hi;
-                out[plane + (size_t)r * Kp + k] = lo;
+                const size_t o = (size_t)r * Kp + k;
+                for (int p = 0; p < np; p++) {
+                    __nv_bfloat16 q = __double2bfloat16(x);
+                    out[p * plane + o] = q;
+                    x -= (double)__bfloat162float(q);
+                }
             }
         }
         __syncthreads();
@@ -400,10 +465,10 @@ EncodeTiledFn encode_fn() {
 }
 
 // planes x rows x K tensor of bf16, box (BK, box_rows, 1); rows beyond `rows` read as zero
-CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t plane_stride) {
+CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t plane_stride, int planes) {
     CUtensorMap m;
     REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, CCSD_GPU_EINVAL, "tensor map base must be 16-byte aligned");
-    cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, 2};
+    cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)planes};
     cuuint64_t strides[2] = {(cuuint64_t)Kp * 2, (cuuint64_t)plane_stride * 2};
     cuuint32_t box[3] = {BK, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
@@ -416,52 +481,77 @@ CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-// A: rows [0, a_rows) of planes with stride a_plane; the grid covers Mp x Np output tiles.
+int sm_count() {
+    static int nsm[128] = {};
+    int dev = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) dev = 0;
+    if (!nsm[dev]) CU_CHECK(cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev));
+    return nsm[dev];
+}
 
-template <class Epi>
-void launch_tc(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t Mp,
-               const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t Np, int64_t Kp, const Epi &epi,
-               double issued_flops, int splits = 1) {
-    REQUIRE(Mp % BM == 0 && Np % BN == 0 && Kp % BK == 0 && Kp > 0, CCSD_GPU_EINVAL, "tc gemm: bad padding");
-    CU_CHECK(cudaFuncSetAttribute(bf16x3_gemm_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane);
-    CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, BN, b_plane);
+// A: a_rows rows of NP planes with stride a_plane; B likewise; the grid covers m_out x n_out output
+// elements (rounded up to the tile); mnk = m * n * k of the product for the FLOP count.
+template <class MD, class Epi>
+void launch_mode(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t m_out,
+                 const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t n_out, int64_t Kp, const Epi &epi,
+                 double mnk, int splits) {
+    const int64_t Mp = round_up(m_out, BM), Np = round_up(n_out, MD::BN);
+    REQUIRE(Kp % BK == 0 && Kp > 0 && Mp > 0 && Np > 0, CCSD_GPU_EINVAL, "tc gemm: bad padding");
+    CU_CHECK(cudaFuncSetAttribute(split_bf16_gemm_kernel<MD, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  MD::SMEM_BYTES));
+    CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane, MD::NP);
+    CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, MD::BN, b_plane, MD::NP);
     TileMap map;
     map.num_mt = (int)(Mp / BM);
-    map.num_nt = (int)(Np / BN);
+    map.num_nt = (int)(Np / MD::BN);
     map.nk_all = (int)(Kp / BK);
     map.nks = (map.nk_all + splits - 1) / splits;
+    map.bn = MD::BN;
     map.group_m = std::min(map.num_mt, 16);
+    map.kc = (Epi::kChunked && ex.k_chunk > 0) ? (int)std::max<int64_t>(1, ex.k_chunk / BK) : map.nks;
     const int num_tiles = map.num_mt * map.num_nt * splits;
-    int nsm = 148;
-    {
-        int dev = 0;
-        CU_CHECK(cudaGetDevice(&dev));
-        CU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    }
-    dim3 grid((unsigned)std::min(num_tiles, nsm));
+    dim3 grid((unsigned)std::min(num_tiles, sm_count()));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ex.prof && ex.prof->on) {
         CU_CHECK(cudaEventCreate(&e0));
         CU_CHECK(cudaEventCreate(&e1));
         CU_CHECK(cudaEventRecord(e0, ex.stream));
     }
-    bf16x3_gemm_kernel<Epi><<<grid, THREADS, SMEM_BYTES, ex.stream>>>(ta, tb, map, num_tiles, epi);
+    split_bf16_gemm_kernel<MD, Epi><<<grid, THREADS, MD::SMEM_BYTES, ex.stream>>>(ta, tb, map, num_tiles, epi);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
     if (e0) {
         CU_CHECK(cudaEventRecord(e1, ex.stream));
         ex.prof->events.emplace_back(e0, e1);
-        ex.prof->flops.push_back(issued_flops);
+        ex.prof->flops.push_back(2.0 * MD::NPROD * mnk);
     }
 }
 
+template <class Epi>
+void launch_tc(Exec &ex, int planes, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t m_out,
+               const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t n_out, int64_t Kp, const Epi &epi,
+               double mnk, int splits = 1) {
+    if (planes == 3)
+        launch_mode<ModeX6>(ex, A, a_rows, a_plane, m_out, B, b_rows, b_plane, n_out, Kp, epi, mnk, splits);
+    else
+        launch_mode<ModeX3>(ex, A, a_rows, a_plane, m_out, B, b_rows, b_plane, n_out, Kp, epi, mnk, splits);
+}
+
+int n_tile(int planes) { return planes == 3 ? ModeX6::BN : ModeX3::BN; }
+
 void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
-           __nv_bfloat16 *out) {
+           int planes, __nv_bfloat16 *out) {
     dim3 grid((unsigned)(Rp / 32), (unsigned)std::min<int64_t>(Kp / 32, 65535));
-    split_bf16_kernel<<<grid, dim3(32, 8), 0, ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, out);
+    split_bf16_kernel<<<grid, dim3(32, 8), 0, ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, planes,
+                                                           out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
+}
+
+int check_planes(int planes) {
+    REQUIRE(planes == 2 || planes == 3, CCSD_GPU_EINVAL, "split-bf16 planes must be 2 or 3");
+    return planes;
 }
 
 }  // namespace
@@ -469,32 +559,34 @@ void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64
 void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
                 int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc) {
     REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "mixed_gemm: size too large");
-    const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, BN);
-    DBuf a(sizeof(__nv_bfloat16) * 2 * Mp * Kp, ex.stream), b(sizeof(__nv_bfloat16) * 2 * Np * Kp, ex.stream);
+    const int np = check_planes(ex.planes);
+    const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, B_ROW_PAD);
+    DBuf a(sizeof(__nv_bfloat16) * np * Mp * Kp, ex.stream), b(sizeof(__nv_bfloat16) * np * Np * Kp, ex.stream);
     // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T)
-    if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, a.as<__nv_bfloat16>());
-    else split(ex, A, lda, 1, m, k, Mp, Kp, a.as<__nv_bfloat16>());
+    if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, np, a.as<__nv_bfloat16>());
+    else split(ex, A, lda, 1, m, k, Mp, Kp, np, a.as<__nv_bfloat16>());
     // B operand rows are output columns: op(B)(kk, c) = B[kk + ldb c] (N) or B[c + ldb kk] (T)
-    if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, b.as<__nv_bfloat16>());
-    else split(ex, B, 1, ldb, n, k, Np, Kp, b.as<__nv_bfloat16>());
-    // split K when the output tiles cannot fill the 148 SMs: deterministic partial products, then a sum
-    const int64_t tiles = (Mp / BM) * (Np / BN), nkt = Kp / BK;
+    if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
+    else split(ex, B, 1, ldb, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
+    // split K when the output tiles cannot fill the SMs: deterministic partial products, then a sum
+    const int64_t tiles = (Mp / BM) * (round_up(n, n_tile(np)) / n_tile(np)), nkt = Kp / BK;
+    const int64_t nsm = sm_count();
     int splits = 1;
-    if (tiles < 148 && nkt >= 16) {
-        int64_t want = std::min<int64_t>((296 + tiles - 1) / tiles, nkt / 8);
+    if (tiles < nsm && nkt >= 16) {
+        int64_t want = std::min<int64_t>((2 * nsm + tiles - 1) / tiles, nkt / 8);
         int64_t per = (nkt + want - 1) / want;
         splits = (int)((nkt + per - 1) / per);
     }
+    const double mnk = double(m) * double(n) * double(k);
     if (splits <= 1) {
         EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
-        launch_tc(ex, a.as<__nv_bfloat16>(), Mp, Mp * Kp, Mp, b.as<__nv_bfloat16>(), Np, Np * Kp, Np, Kp, epi,
-                  6.0 * double(m) * double(n) * double(k));
+        launch_tc(ex, np, a.as<__nv_bfloat16>(), Mp, Mp * Kp, m, b.as<__nv_bfloat16>(), Np, Np * Kp, n, Kp, epi, mnk);
         return;
     }
     DBuf part = dalloc((int64_t)splits * m * n, ex.stream);
     EpiF64 epi{part.d(), (long long)m, (int)m, (int)n, alpha, 0.0, (long long)m * n};
-    launch_tc(ex, a.as<__nv_bfloat16>(), Mp, Mp * Kp, Mp, b.as<__nv_bfloat16>(), Np, Np * Kp, Np, Kp, epi,
-              6.0 * double(m) * double(n) * double(k), splits);
+    launch_tc(ex, np, a.as<__nv_bfloat16>(), Mp, Mp * Kp, m, b.as<__nv_bfloat16>(), Np, Np * Kp, n, Kp, epi, mnk,
+              splits);
     sum_splits_kernel<<<(unsigned)std::min<int64_t>((m * n + 255) / 256, 148 * 64), 256, 0, ex.stream>>>(
         part.d(), splits, m, n, beta, C, ldc);
     ex.launches++;
@@ -502,20 +594,21 @@ void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
 }
 
 int64_t tc_pad_rows_a(int64_t m) { return round_up(m, BM); }
-int64_t tc_pad_rows_b(int64_t n) { return round_up(n, BN); }
+int64_t tc_pad_rows_b(int64_t n) { return round_up(n, B_ROW_PAD); }
 int64_t tc_pad_k(int64_t k) { return round_up(k, BK); }
 
 void split_rows(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
                 __nv_bfloat16 *out) {
     REQUIRE(Rp % 32 == 0 && Kp % 32 == 0, CCSD_GPU_EINVAL, "split_rows: padding must be a multiple of 32");
-    split(ex, src, sr, sk, R, K, Rp, Kp, out);
+    split(ex, src, sr, sk, R, K, Rp, Kp, check_planes(ex.planes), out);
 }
 
 void tc_gemm_f64(Exec &ex, const __nv_bfloat16 *A, int64_t Mp, const __nv_bfloat16 *B, int64_t Np, int64_t Kp,
                  int64_t m, int64_t n, int64_t k_true, double alpha, double beta, double *C, int64_t ldc) {
+    REQUIRE(Mp >= round_up(m, BM) && Np >= round_up(n, B_ROW_PAD), CCSD_GPU_EINVAL, "tc_gemm_f64: bad padding");
     EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
-    launch_tc(ex, A, Mp, Mp * Kp, round_up(m, BM), B, Np, Np * Kp, round_up(n, BN), Kp, epi,
-              6.0 * double(m) * double(n) * double(k_true));
+    launch_tc(ex, check_planes(ex.planes), A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi,
+              double(m) * double(n) * double(k_true));
 }
 
 void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,
@@ -528,9 +621,10 @@ void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp,
     epi.a0 = (int)a0;
     epi.M = (int)(nv * (a1 - a0));
     epi.N = (int)(nv * a1);
+    epi.np = check_planes(ex.planes);
     const int64_t r0 = nv * a0;
-    launch_tc(ex, L + r0 * Kp, l_rows - r0, l_rows * Kp, round_up(epi.M, BM), L, l_rows, l_rows * Kp,
-              round_up(epi.N, BN), Kp, epi, 6.0 * double(epi.M) * double(epi.N) * double(k_true));
+    launch_tc(ex, epi.np, L + r0 * Kp, l_rows - r0, l_rows * Kp, epi.M, L, l_rows, l_rows * Kp, epi.N, Kp, epi,
+              double(epi.M) * double(epi.N) * double(k_true));
 }
 
 int mixed_gemm_error_flag(bool reset) {
@@ -584,7 +678,7 @@ void mixed_gemm_noalloc(bool transA, bool transB, int64_t m, int64_t n, int64_t 
                         cudaStream_t stream) {
     REQUIRE(m > 0 && n > 0 && k > 0 && A && B && C, CCSD_GPU_EINVAL, "bad gemm arguments");
     REQUIRE(lda >= (transA ? k : m) && ldb >= (transB ? n : k) && ldc >= m, CCSD_GPU_EINVAL, "bad leading dimension");
-    const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, BN);
+    const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, B_ROW_PAD);
     const int64_t need = 2 * (Mp + Np) * Kp;
     REQUIRE(need <= NOALLOC_SCRATCH_ELEMS, CCSD_GPU_EINVAL,
             "no-alloc GEMM: 2 x (round_up(m,128) + round_up(n,256)) x round_up(k,64) = " + std::to_string(need) +
@@ -593,12 +687,12 @@ void mixed_gemm_noalloc(bool transA, bool transB, int64_t m, int64_t n, int64_t 
     Exec ex;
     ex.stream = stream;
     __nv_bfloat16 *a = scratch, *b = scratch + 2 * Mp * Kp;
-    if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, a);
-    else split(ex, A, lda, 1, m, k, Mp, Kp, a);
-    if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, b);
-    else split(ex, B, 1, ldb, n, k, Np, Kp, b);
+    if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, 2, a);
+    else split(ex, A, lda, 1, m, k, Mp, Kp, 2, a);
+    if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, 2, b);
+    else split(ex, B, 1, ldb, n, k, Np, Kp, 2, b);
     EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
-    launch_tc(ex, a, Mp, Mp * Kp, Mp, b, Np, Np * Kp, Np, Kp, epi, 6.0 * double(m) * double(n) * double(k));
+    launch_tc(ex, 2, a, Mp, Mp * Kp, m, b, Np, Np * Kp, n, Kp, epi, double(m) * double(n) * double(k));
 }
 
 }  // namespace ccsd

@@ -49,8 +49,8 @@ enum {
 /* arithmetic used by the contractions */
 enum {
     CCSD_GPU_FP64 = 0,           /* FP64 everywhere (DGEMM on the FP64 tensor pipe) */
-    CCSD_GPU_MIXED = 1           /* large contractions as split-BF16 (3 products) tcgen05 GEMMs,
-                                    FP32 accumulation; everything else FP64 */
+    CCSD_GPU_MIXED = 1           /* large contractions as split-BF16 (2 planes, 3 products) tcgen05
+                                    GEMMs, FP32 accumulation; everything else FP64 */
 };
 
 typedef struct ccsd_gpu_options {
@@ -58,7 +58,9 @@ typedef struct ccsd_gpu_options {
     int32_t precision;           /* CCSD_GPU_FP64 or CCSD_GPU_MIXED */
     int64_t ladder_batch;        /* virtual-index batch of the A2 ladder, 0 = automatic */
     int64_t mixed_min_flops;     /* contractions below this many flops stay FP64 (0 = default) */
-    int64_t reserved[5];
+    int64_t mixed_k_chunk;       /* K elements a tensor-core FP32 accumulator sums before the partial
+                                    sum is added in FP64 (0 = default 4096, negative = the whole K) */
+    int64_t reserved[4];
 } ccsd_gpu_options;
 
 typedef struct ccsd_gpu_solver_options {
@@ -66,8 +68,11 @@ typedef struct ccsd_gpu_solver_options {
     int32_t diis_dimension;      /* default 8 */
     double omega_threshold;      /* |Omega| convergence threshold */
     double energy_threshold;     /* |dE| convergence threshold (< 0 disables the energy test) */
-    double refine_threshold;     /* MIXED only: |Omega| at which Omega switches to FP64 */
-    int32_t reserved[8];
+    double refine_threshold;     /* MIXED only: |Omega| of the first FP64 refresh (default 1e-4) */
+    double refine_target;        /* MIXED only: the true residual the refinement aims at; refreshes
+                                    that remove drift happen only while the drift exceeds it
+                                    (0 = omega_threshold) */
+    int32_t reserved[6];
 } ccsd_gpu_solver_options;
 
 /* Creation / teardown.  Replaces the wavefunction set-up that allocates t, Omega and the
@@ -169,7 +174,10 @@ int ccsd_gpu_set_profiling(void *ctx, int32_t on);
 int ccsd_gpu_gemm_profile(void *ctx, int64_t *launches, double *device_ms, double *tensor_flops);
 
 /* Diagnostics: C (m x n, column-major, host) = alpha op(A) op(B) + beta C on the device, through
- * the FP64 DGEMM (mixed = 0) or the split-BF16 tcgen05 GEMM (mixed = 1) that the contractions use. */
+ * the FP64 DGEMM (mixed = 0) or the split-BF16 tcgen05 GEMM that the contractions use (mixed = 1,
+ * two bf16 planes), or the three-plane variant of that GEMM (mixed = 2; 6 products, operand rounding
+ * 2^-24; not used by the contractions because the FP32 accumulation in the tensor cores, not the
+ * operand split, limits their accuracy at CCSD's long K). */
 int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t transB, int64_t m, int64_t n,
                            int64_t k, double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
                            double beta, double *C, int64_t ldc);

@@ -11,6 +11,9 @@ pytestmark = pytest.mark.gpu
 # bf16 hi+lo keeps ~16 significant bits per operand; the dropped lo*lo product and the FP32
 # accumulation leave a relative error of order 1e-5 per dot product.
 GEMM_RTOL = 1e-4
+# three planes keep ~24 bits of each operand; what remains is the FP32 accumulation in TMEM, so
+# the three-plane mode is much tighter than two planes for short K and about as tight for long K.
+GEMM_RTOL_X6 = 1e-5
 
 
 @pytest.fixture(scope="module")
@@ -34,6 +37,25 @@ def test_mixed_gemm_matches_fp64(ctx, m, n, k, tA, tB):
     out = ctx.selftest_gemm(A, B, C0, alpha=0.7, beta=-0.3, transA=tA, transB=tB, mixed=True)
     scale = np.abs(A).max() * np.abs(B).max() * np.sqrt(k)
     assert np.abs(out - ref).max() <= GEMM_RTOL * scale
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 128, 64), (129, 257, 65), (256, 384, 192), (640, 512, 1200),
+                                   (300, 1000, 777), (200, 300, 20000)])
+@pytest.mark.parametrize("tA,tB", [(False, False), (True, True)])
+def test_mixed6_gemm_matches_fp64(ctx, m, n, k, tA, tB):
+    """Three-plane mode (N tile 128): within the bound on every shape, tighter for short K."""
+    rng = np.random.default_rng(m * 5 + n * 11 + k)
+    A = rng.standard_normal((k, m) if tA else (m, k))
+    B = rng.standard_normal((n, k) if tB else (k, n))
+    C0 = rng.standard_normal((m, n))
+    ref = 0.7 * ((A.T if tA else A) @ (B.T if tB else B)) - 0.3 * C0
+    out6 = ctx.selftest_gemm(A, B, C0, alpha=0.7, beta=-0.3, transA=tA, transB=tB, mixed=2)
+    out3 = ctx.selftest_gemm(A, B, C0, alpha=0.7, beta=-0.3, transA=tA, transB=tB, mixed=1)
+    scale = np.abs(A).max() * np.abs(B).max() * np.sqrt(k)
+    err6, err3 = np.abs(out6 - ref).max(), np.abs(out3 - ref).max()
+    assert err6 <= GEMM_RTOL_X6 * scale
+    if k <= 128:                     # accumulation error takes over from K ~ 200 on
+        assert err6 < 0.3 * err3
 
 
 def test_fp64_gemm_path(ctx):
@@ -113,3 +135,24 @@ def test_mixed_ladder_batching(batch):
     om, om_ref = gpu.construct_omega(), ref.omega()
     assert np.linalg.norm(om - om_ref) <= 1e-4 * np.linalg.norm(om_ref)
     gpu.close()
+
+
+def test_chunked_accumulation_beats_whole_k_accumulation():
+    """Long K (no split-K: 16 x 10 output tiles): the tensor cores' FP32 accumulation truncates a
+    little at every step, so summing 4096-wide chunks in FP64 removes most of the drift.  Seen
+    clearly on non-negative operands, where the truncation adds up to a one-sided bias."""
+    from et_b200 import CCSD
+    m, n, k = 2048, 2560, 32768
+    rng = np.random.default_rng(8)
+    A = np.abs(rng.standard_normal((m, k)))
+    B = np.abs(rng.standard_normal((k, n)))
+    ref = A @ B
+    rel = {}
+    for chunk in (0, -1):            # 0: the default 4096-wide chunks; -1: one accumulator for all of K
+        with CCSD(2, 3, 4, mixed_k_chunk=chunk) as c:
+            out = c.selftest_gemm(A, B, mixed=True)
+        rel[chunk] = (out - ref) / ref
+    bias_chunked, bias_whole = abs(rel[0].mean()), abs(rel[-1].mean())
+    assert np.abs(rel[0]).max() < 1e-4
+    assert bias_chunked < 0.5 * bias_whole, (bias_chunked, bias_whole)
+
