@@ -115,6 +115,7 @@ int ccsd_gpu_set_cholesky_mo(void *ctx, const double *L) {
         blk(c.L_vv, no, nv, no, nv);
         CU_CHECK(cudaStreamSynchronize(c.ex.stream));
         c.have_L = true;
+        c.have_gov = false;
         if (c.have_h) c.refresh();
     });
 }
@@ -128,6 +129,7 @@ int ccsd_gpu_set_cholesky_mo_blocks(void *ctx, const double *L_oo, const double 
         h2d(c, c.L_vv.d(), L_vv, c.nJ * c.nv * c.nv);
         CU_CHECK(cudaStreamSynchronize(c.ex.stream));
         c.have_L = true;
+        c.have_gov = false;
         if (c.have_h) c.refresh();
     });
 }

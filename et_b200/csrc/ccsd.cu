@@ -72,7 +72,7 @@ Context::~Context() {
     if (own_stream) cudaStreamSynchronize(own_stream);
     if (ex.stream && ex.stream != own_stream) cudaStreamSynchronize(ex.stream);
     // every device buffer is freed (stream-ordered) while its stream still exists
-    for (DBuf *b : {&L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
+    for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
                     &mbuf, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
         b->release();
     mbuf_bytes = 0;
@@ -188,12 +188,22 @@ DBuf Context::g_ovov() {
     return g;
 }
 
+const double *Context::g_ovov_const() {
+    if (!have_gov) {
+        const Prec keep = ex.prec;
+        ex.prec = Prec::FP64;
+        gov = g_ovov();
+        ex.prec = keep;
+        have_gov = true;
+    }
+    return gov.d();
+}
+
 // calculate_energy_ccsd (src/wavefunctions/ccsd/mean_value_ccsd.F90:36-99), FP64
 double Context::energy() {
     Prec keep = ex.prec;
     ex.prec = Prec::FP64;
-    DBuf g = g_ovov();
-    energy_reduce(ex, t.d(), t.d() + nt1, g.d(), no, nv, e_hf, scal.d());
+    energy_reduce(ex, t.d(), t.d() + nt1, g_ovov_const(), no, nv, e_hf, scal.d());
     ex.prec = keep;
     double e;
     CU_CHECK(cudaMemcpyAsync(&e, scal.d(), sizeof(double), cudaMemcpyDeviceToHost, ex.stream));

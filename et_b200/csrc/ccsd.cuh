@@ -36,6 +36,8 @@ struct Context {
     DBuf scal;               // scalar scratch
     DBuf mbuf;               // split-bf16 ladder integrals M_ab[c,d] for all pairs (mixed precision)
     size_t mbuf_bytes = 0;
+    DBuf gov;                  // g_iajb cache (g_ovov_const)
+    bool have_gov = false;
 
     Context(int64_t no, int64_t nv, int64_t nJ, const ccsd_gpu_options *opt);
     ~Context();
@@ -46,10 +48,14 @@ struct Context {
     void refresh();                        // T1 transformation + Fock at the current t
     void set_precision(int32_t precision);   // CCSD_GPU_FP64 / CCSD_GPU_MIXED
     DBuf g_ovov();
+    // g_iajb = sum_J L_ia L_jb in FP64, kept until the Cholesky vectors change: the ov block is
+    // unchanged by the T1 transformation, so every iteration shares it
+    const double *g_ovov_const();
     double energy();
     void mp2_guess();
     void omega(double *d_omega);
-    OmegaNodes record_omega(Graph &g);
+    // const_ovov: take g_iajb from the cache (no derivative flows into L_ov through it)
+    OmegaNodes record_omega(Graph &g, bool const_ovov = true);
     void record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv_in, int tf);
     void ladder_y(const double *Lvv, const double *tfull, double *Y);
     void jacobian(int64_t nvec, const double *c, double *rho);

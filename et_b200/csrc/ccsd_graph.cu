@@ -64,7 +64,7 @@ __global__ void join_amp_kernel(const double *__restrict__ x1, const double *__r
 // ---------------------------------------------------------------------------
 // Omega on the graph
 // ---------------------------------------------------------------------------
-OmegaNodes Context::record_omega(Graph &g) {
+OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     OmegaNodes n{};
     g.nov = nov;
     const std::vector<int64_t> V4 = {nv, no, nv, no};
@@ -139,8 +139,14 @@ OmegaNodes Context::record_omega(Graph &g) {
     // omega_doubles_c1 (:207-258)
     g.contract(om1, "aibj,jb->ai", 1.0, u, F_ov, true);
 
-    const int G4 = g.zeros("g_ovov", {no, nv, no, nv});               // g_ldkc, shared below
-    g.contract(G4, "Jia,Jjb->iajb", 1.0, Lt_ov, Lt_ov);
+    // g_ldkc, shared below (FP64 cache unless the adjoint into L_ov is wanted)
+    int G4;
+    if (const_ovov) {
+        G4 = g.input("g_ovov", {no, nv, no, nv}, g_ovov_const());
+    } else {
+        G4 = g.zeros("g_ovov", {no, nv, no, nv});
+        g.contract(G4, "Jia,Jjb->iajb", 1.0, Lt_ov, Lt_ov);
+    }
     // omega_ccsd_e2 (omega_ccsd.F90:712-878); Fock parts in FP64
     const int om = g.zeros("omega_aibj", V4);
     {
@@ -343,7 +349,7 @@ void Context::jacobian_transpose(int64_t nvec, const double *b, double *sigma) {
 void Context::adjoint(const double *b, double *dt, double *dL, double *dh) {
     REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
     Graph g(ex);
-    OmegaNodes n = record_omega(g);
+    OmegaNodes n = record_omega(g, dL == nullptr);
     DBuf s1 = dalloc(nt1, ex.stream), s2 = dalloc(nt2, ex.stream);
     split_amp_kernel<<<grid_for(namp, 256), 256, 0, ex.stream>>>(b, nt1, nov, 1, 1.0, s1.d(), s2.d());
     ex.launches++;

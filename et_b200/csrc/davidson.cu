@@ -246,8 +246,7 @@ int Context::davidson(int nstates, int side, const ccsd_gpu_davidson_options *o,
 // eta of the multiplier equation at the current amplitudes (construct_eta_ccsd)
 void Context::eta(double *out) {
     refresh();
-    DBuf g = g_ovov();
-    construct_eta(ex, F.d(), g.d(), no, nv, out);
+    construct_eta(ex, F.d(), g_ovov_const(), no, nv, out);
 }
 
 // Multiplier (Lambda) equations  A^T tbar = -eta  by linear Davidson, restating eT's default
