@@ -156,3 +156,22 @@ def test_chunked_accumulation_beats_whole_k_accumulation():
     assert np.abs(rel[0]).max() < 1e-4
     assert bias_chunked < 0.5 * bias_whole, (bias_chunked, bias_whole)
 
+
+
+def test_mixed_jacobian_and_transpose_close_to_fp64():
+    """Tangent and adjoint contractions through the tensor cores (permuted operands and outputs are
+    read and written in place) against the FP64 transformations."""
+    from et_b200 import CCSD, FP64, MIXED
+    n_o, n_v, n_J = 6, 40, 90
+    s = make_system(n_o, n_v, n_J, seed=31)
+    rng = np.random.default_rng(7)
+    out = {}
+    for prec in (FP64, MIXED):
+        with CCSD(n_o, n_v, n_J, precision=prec, mixed_min_flops=1) as g:
+            g.set_system(s.L_mo, s.h_mo, s.eps)
+            g.set_initial_amplitudes_guess()
+            C = np.random.default_rng(3).standard_normal((g.n_amp, 3))
+            out[prec] = (g.jacobian_transformation(C), g.jacobian_transpose_transformation(C))
+    for k in range(2):
+        ref, mix = out[FP64][k], out[MIXED][k]
+        assert np.linalg.norm(mix - ref) <= 1e-4 * np.linalg.norm(ref)
