@@ -4,6 +4,6 @@
 declared in ``include/ccsd_gpu.h`` and implemented in ``libccsd_gpu.so``.
 """
 
-from .ccsd import CCSD, CCSDGPUError, FP64, MIXED, load_library  # noqa: F401
+from .ccsd import CCSD, CCSDGPUError, FP64, MIXED, load_library, solve_ground_states  # noqa: F401
 
-__all__ = ["CCSD", "CCSDGPUError", "FP64", "MIXED", "load_library"]
+__all__ = ["CCSD", "CCSDGPUError", "FP64", "MIXED", "load_library", "solve_ground_states"]

@@ -57,6 +57,13 @@ class SolverOptions(ctypes.Structure):
                 ("reserved", ctypes.c_int32 * 6)]
 
 
+class BatchSystem(ctypes.Structure):
+    _fields_ = [("n_o", ctypes.c_int64), ("n_v", ctypes.c_int64), ("n_J", ctypes.c_int64),
+                ("L_mo", ctypes.POINTER(ctypes.c_double)), ("h_mo", ctypes.POINTER(ctypes.c_double)),
+                ("eps", ctypes.POINTER(ctypes.c_double)), ("e_hf", ctypes.c_double),
+                ("t_out", ctypes.POINTER(ctypes.c_double))]
+
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -101,6 +108,9 @@ SIGNATURES = {
     "ccsd_gpu_mixed_gemm_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _I64, _I64, _I64, ctypes.c_double,
                                                    _VP, _I64, _VP, _I64, ctypes.c_double, _VP, _I64, _VP]),
     "ccsd_gpu_omega_flops": (ctypes.c_double, [_VP]),
+    "ccsd_gpu_solve_gs_batch": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(BatchSystem), ctypes.POINTER(Options),
+                                               ctypes.POINTER(SolverOptions), ctypes.c_int32, _DP,
+                                               ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
 }
 
 
@@ -368,3 +378,46 @@ class CCSD:
 
     def omega_flops(self) -> float:
         return float(self.lib.ccsd_gpu_omega_flops(self.ctx))
+
+
+
+def solve_ground_states(systems, *, precision=FP64, device=0, workers=8, max_iterations=100, diis_dimension=8,
+                        omega_threshold=1e-5, energy_threshold=1e-5, refine_threshold=1e-4, refine_target=0.0,
+                        mixed_min_flops=0, amplitudes=False):
+    """Ground states of independent systems on `workers` concurrent contexts (ccsd_gpu_solve_gs_batch).
+
+    ``systems``: sequence of (L_mo[J, p, q], h_mo, eps, n_o, e_hf) host arrays and sizes.  Each system
+    starts from its MP2 guess.  Returns (energies, iterations, statuses, amplitudes or None); status
+    -5 means that system did not converge within ``max_iterations``."""
+    lib = load_library()
+    n = len(systems)
+    arr = (BatchSystem * max(n, 1))()
+    keep, t_outs = [], []
+    for k, (L, h, eps, n_o, e_hf) in enumerate(systems):
+        L = np.asarray(L, dtype=np.float64)
+        n_J, n_mo = L.shape[0], L.shape[1]
+        flat = np.ascontiguousarray(L.reshape(-1, order="F"))          # (J, p, q), J fastest
+        hf = np.ascontiguousarray(np.asarray(h, dtype=np.float64).reshape(-1, order="F"))
+        ef = np.ascontiguousarray(np.asarray(eps, dtype=np.float64))
+        keep += [flat, hf, ef]
+        arr[k].n_o, arr[k].n_v, arr[k].n_J = int(n_o), int(n_mo - n_o), int(n_J)
+        arr[k].L_mo, arr[k].h_mo, arr[k].eps = _dp(flat), _dp(hf), _dp(ef)
+        arr[k].e_hf = float(e_hf)
+        if amplitudes:
+            n1 = int(n_o) * int(n_mo - n_o)
+            t = np.zeros(n1 + n1 * (n1 + 1) // 2)
+            t_outs.append(t)
+            arr[k].t_out = _dp(t)
+    opt = Options(device=device, precision=precision, mixed_min_flops=mixed_min_flops)
+    sopt = SolverOptions(max_iterations=max_iterations, diis_dimension=diis_dimension,
+                         omega_threshold=omega_threshold, energy_threshold=energy_threshold,
+                         refine_threshold=refine_threshold, refine_target=refine_target)
+    e = np.zeros(max(n, 1))
+    it = np.zeros(max(n, 1), dtype=np.int32)
+    st = np.zeros(max(n, 1), dtype=np.int32)
+    rc = lib.ccsd_gpu_solve_gs_batch(n, arr, ctypes.byref(opt), ctypes.byref(sopt), int(workers), _dp(e),
+                                     it.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                     st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    if rc not in (0, -5):
+        raise CCSDGPUError(int(rc), "batch solve failed for system %d" % int(np.flatnonzero(st[:n])[0]))
+    return e[:n], it[:n], st[:n], (t_outs if amplitudes else None)

@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "mixed_gemm.cuh"
@@ -482,12 +483,16 @@ CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 int sm_count() {
-    static int nsm[128] = {};
+    static std::atomic<int> nsm[128] = {};   // contexts on several host threads share it
     int dev = 0;
     CU_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 128) dev = 0;
-    if (!nsm[dev]) CU_CHECK(cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev));
-    return nsm[dev];
+    int v = nsm[dev].load(std::memory_order_relaxed);
+    if (!v) {
+        CU_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        nsm[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
 }
 
 // A: a_rows rows of NP planes with stride a_plane; B likewise; the grid covers m_out x n_out output

@@ -202,6 +202,29 @@ int ccsd_gpu_mixed_gemm_noalloc(int32_t transA, int32_t transB, int64_t m, int64
  * call sites (2mnk per DGEMM, n(n+1)k per DSFRK). */
 double ccsd_gpu_omega_flops(void *ctx);
 
+/* One independent system of a batch: host arrays in the layouts of ccsd_gpu_set_cholesky_mo and
+ * ccsd_gpu_set_h_mo. */
+typedef struct ccsd_gpu_batch_system {
+    int64_t n_o, n_v, n_J;
+    const double *L_mo;          /* (J, n_mo, n_mo) column-major */
+    const double *h_mo;          /* n_mo x n_mo */
+    const double *eps;           /* n_mo orbital energies */
+    double e_hf;
+    double *t_out;               /* optional: the final amplitudes (n_t1 + n_t2), or NULL */
+} ccsd_gpu_batch_system;
+
+/* Ground states of many independent systems of uneven size.  eT runs one wavefunction per process
+ * and has no such entry point; this is the batch of the uneven-batch workload.  `workers` host
+ * threads (1..64) each take the next system (largest o^2 v^4 first), create a context on
+ * opt->device with its own stream, start from the MP2 guess, run ccsd_gpu_solve_gs with `sopt` and
+ * release the context, so the kernels of systems in flight overlap on the GPU.  Per system the
+ * energy, iteration count and status are written (arrays of n_systems, each may be NULL); the
+ * return value is CCSD_GPU_OK when every system converged, else the first non-zero status in
+ * system order.  Device memory in use is that of `workers` systems at a time. */
+int ccsd_gpu_solve_gs_batch(int32_t n_systems, const ccsd_gpu_batch_system *systems, const ccsd_gpu_options *opt,
+                            const ccsd_gpu_solver_options *sopt, int32_t workers, double *energies,
+                            int32_t *iterations, int32_t *status);
+
 #ifdef __cplusplus
 }
 #endif
