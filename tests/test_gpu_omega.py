@@ -116,3 +116,25 @@ def test_errors_are_status_codes():
     with pytest.raises(ValueError):
         gpu.set_amplitudes(np.zeros(3))
     gpu.close()
+
+
+@pytest.mark.parametrize("dims", [(1, 1, 2), (1, 4, 5), (4, 1, 6), (2, 3, 1), (1, 70, 40), (9, 2, 30)])
+def test_extreme_shapes_fp64_and_mixed(dims):
+    """Edge shapes: a single occupied or virtual orbital, a single Cholesky vector, and shapes whose
+    padding to the tensor-core tiles dominates (mixed with every GEMM forced onto the tensor cores)."""
+    from et_b200 import CCSD, MIXED
+    n_o, n_v, n_J = dims
+    s = make_system(n_o, n_v, n_J, seed=5)
+    ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
+    ref.set_amplitudes(0.05 * np.random.default_rng(1).standard_normal(ref.n_amp))
+    om_ref = ref.omega()
+    scale = max(1.0, np.abs(om_ref).max())
+    for prec, tol in ((0, 1e-12), (MIXED, 1e-4)):
+        with CCSD(n_o, n_v, n_J, precision=prec, mixed_min_flops=1) as gpu:
+            gpu.set_system(s.L_mo, s.h_mo, s.eps)
+            gpu.set_amplitudes(ref.get_amplitudes())
+            assert abs(gpu.calculate_energy() - ref.energy()) <= tol * max(1.0, abs(ref.energy()))
+            assert np.abs(gpu.construct_omega() - om_ref).max() <= tol * scale
+            c = np.random.default_rng(2).standard_normal(ref.n_amp)
+            rho_ref = ref.jacobian_transformation(c)
+            assert np.abs(gpu.jacobian_transformation(c) - rho_ref).max() <= tol * max(1.0, np.abs(rho_ref).max())
