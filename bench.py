@@ -355,13 +355,17 @@ def run_eom(args):
         out[f"s_per_transform_{name}"] = round(t1, 4)
         out[f"s_per_24_block_{name}"] = round(t24, 4)
     nroots = args.roots
+    # mixed Davidson to residual 1e-5, then one FP64 Davidson iteration restarted from its vectors: a
+    # Rayleigh-Ritz step with FP64 transforms of the mixed eigenvectors.  (Further FP64 Davidson
+    # iterations first move these clustered non-symmetric roots away before converging: after two
+    # the largest error was 2.3e-7 Eh, after five 1.1e-7, and eleven were needed for 3e-9.)
     gpu.set_precision(MIXED)
     t0 = time.perf_counter()
     w_mix, X, it_mix = gpu.excited_states(nroots, block=24, residual_threshold=1e-5, energy_threshold=1e-7,
                                           vectors=True, max_iterations=60)
     gpu.set_precision(FP64)
-    w_ref, _, it_ref = gpu.excited_states(nroots, block=24, residual_threshold=1e-6, energy_threshold=1e-8,
-                                          start=X, max_iterations=60)
+    w_ref, _, it_ref = gpu.excited_states(nroots, block=24, residual_threshold=1e-12, energy_threshold=1e-12,
+                                          start=X, max_iterations=1, raise_on_failure=False)
     t_mixed_path = time.perf_counter() - t0
     t0 = time.perf_counter()
     w64, _, it64 = gpu.excited_states(nroots, block=24, residual_threshold=1e-6, energy_threshold=1e-8,
@@ -369,6 +373,8 @@ def run_eom(args):
     t_fp64_path = time.perf_counter() - t0
     out.update({"roots": nroots, "omega_mixed_refined": list(map(float, w_ref)), "omega_fp64": list(map(float, w64)),
                 "max_abs_domega": float(np.max(np.abs(np.sort(w_ref) - np.sort(w64)))),
+                "max_abs_domega_mixed_only": float(np.max(np.abs(np.sort(w_mix) - np.sort(w64)))),
+                "speedup": round(t_fp64_path / t_mixed_path, 3),
                 "davidson_iterations_mixed_then_fp64": [it_mix, it_ref], "davidson_iterations_fp64": it64,
                 "s_mixed_plus_refinement": round(t_mixed_path, 2), "s_fp64": round(t_fp64_path, 2)})
     gpu.close()

@@ -293,10 +293,13 @@ class CCSD:
         return out[0] if len(out) == 1 else tuple(out)
 
     def excited_states(self, n_states, *, left=False, max_iterations=100, block=0, max_reduced_dim=0,
-                       residual_threshold=1e-6, energy_threshold=1e-6, vectors=False, start=None):
+                       residual_threshold=1e-6, energy_threshold=1e-6, vectors=False, start=None,
+                       raise_on_failure=True):
         """eigen_davidson_solver on the device: (omegas, vectors or None, iterations).
 
-        ``start`` ((n_amp, n_states)) seeds the trial space, e.g. with mixed-precision eigenvectors."""
+        ``start`` ((n_amp, n_states)) seeds the trial space, e.g. with mixed-precision eigenvectors.
+        With ``raise_on_failure=False`` a run that reaches ``max_iterations`` returns its current
+        roots (a fixed number of refinement iterations)."""
         opt = DavidsonOptions(max_iterations=max_iterations, block=block, max_reduced_dim=max_reduced_dim,
                               residual_threshold=residual_threshold, energy_threshold=energy_threshold,
                               start_from_vectors=int(start is not None))
@@ -307,8 +310,10 @@ class CCSD:
         else:
             vec = np.zeros(self.n_amp * n_states) if vectors else None
         it = ctypes.c_int32()
-        self._check(self.lib.ccsd_gpu_eom_davidson(self.ctx, n_states, int(bool(left)), ctypes.byref(opt), _dp(om),
-                                                   _dp(vec) if vectors else None, ctypes.byref(it)))
+        rc = self.lib.ccsd_gpu_eom_davidson(self.ctx, n_states, int(bool(left)), ctypes.byref(opt), _dp(om),
+                                            _dp(vec) if vectors else None, ctypes.byref(it))
+        if rc != 0 and (raise_on_failure or rc != -5):
+            self._check(rc)
         return om, (vec.reshape(self.n_amp, n_states, order="F") if vectors else None), it.value
 
     def construct_eta(self):
