@@ -116,6 +116,7 @@ int ccsd_gpu_set_cholesky_mo(void *ctx, const double *L) {
         CU_CHECK(cudaStreamSynchronize(c.ex.stream));
         c.have_L = true;
         c.have_gov = false;
+        c.l_version++;
         if (c.have_h) c.refresh();
     });
 }
@@ -130,6 +131,7 @@ int ccsd_gpu_set_cholesky_mo_blocks(void *ctx, const double *L_oo, const double 
         CU_CHECK(cudaStreamSynchronize(c.ex.stream));
         c.have_L = true;
         c.have_gov = false;
+        c.l_version++;
         if (c.have_h) c.refresh();
     });
 }

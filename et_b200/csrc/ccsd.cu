@@ -230,16 +230,19 @@ void Context::mp2_guess() {
 // A2 ladder: Omega^ab_ij += sum_cd g_acbd t^cd_ij with the +/- symmetrisation of
 // omega_ccsd_a2 (src/wavefunctions/ccsd/omega_ccsd.F90:113-480), batched over a.
 // ---------------------------------------------------------------------------
-void Context::ladder(const double *Lvv, const double *t2, double *om2) {
+void Context::ladder(const double *Lvv, const double *t2, double *om2, int64_t nvec) {
+    if (nvec <= 0) return;
     if (ex.prec == Prec::MIXED) {
-        ladder_tc(Lvv, t2, om2);
+        ladder_tc(Lvv, t2, om2, nvec, false);
         return;
     }
     cudaStream_t s = ex.stream;
     const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
     const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
-    DBuf tp = dalloc(nop * nvp, s), tm = dalloc(std::max<int64_t>(nom * nvm, 1), s);
-    build_tpm(ex, t2, tp.d(), tm.d(), no, nv);
+    // the nvec vectors side by side: rows [v n_o_p, (v+1) n_o_p) of t+ belong to vector v
+    const int64_t ldp = nvec * nop, ldm = std::max<int64_t>(nvec * nom, 1);
+    DBuf tp = dalloc(ldp * nvp, s), tm = dalloc(ldm * std::max<int64_t>(nvm, 1), s);
+    for (int64_t v = 0; v < nvec; v++) build_tpm(ex, t2 + v * nt2, tp.d() + v * nop, tm.d() + v * nom, no, nv, ldp, ldm);
     // L~_vv as (J, c, a): columns (c, a) of one a-block are contiguous
     DBuf LT = dalloc(nJ * nv * nv, s);
     {
@@ -255,11 +258,11 @@ void Context::ladder(const double *Lvv, const double *t2, double *om2) {
         dst.s[2] = nJ;        // c
         permute_add(ex, 1.0, src, 0.0, dst);
     }
-    // batch length over a: keep G + g+- within the budget
+    // batch length over a: keep G + g+- + w+- within the budget
     int64_t nA = ladder_batch;
     if (nA <= 0) {
         const double budget = 6.0e9;   // bytes
-        double per_a = 8.0 * (double)nv * nv * nv + 16.0 * (double)nvp * nv;
+        double per_a = 8.0 * (double)nv * nv * nv + 16.0 * (double)nvp * nv + 16.0 * (double)ldp * nv;
         nA = std::max<int64_t>(1, std::min<int64_t>(nv, (int64_t)(budget / per_a)));
     }
     int64_t maxab = 0;
@@ -269,19 +272,20 @@ void Context::ladder(const double *Lvv, const double *t2, double *om2) {
     }
     DBuf G = dalloc(nv * nA * nv * nv, s);
     DBuf gp = dalloc(nvp * maxab, s), gm = dalloc(std::max<int64_t>(nvm * maxab, 1), s);
-    DBuf wp = dalloc(nop * maxab, s), wm = dalloc(std::max<int64_t>(nom * maxab, 1), s);
+    DBuf wp = dalloc(ldp * maxab, s), wm = dalloc(ldm * maxab, s);
     for (int64_t a0 = 0; a0 < nv; a0 += nA) {
         int64_t a1 = std::min(nv, a0 + nA);
         int64_t M = nv * (a1 - a0), N = nv * a1;
-        // G[(c,a),(d,b)] = sum_J L_ac L_bd   (eri_t1%get('vvvv') / get_packed('vv'))
+        // G[(c,a),(d,b)] = sum_J L_ac L_bd   (eri_t1%get('vvvv') / get_packed('vv')), once for all vectors
         gemm(ex, true, false, M, N, nJ, 1.0, LT.d() + nJ * nv * a0, nJ, LT.d(), nJ, 0.0, G.d(), M);
         form_gpm(ex, G.d(), M, gp.d(), gm.d(), nv, a0, a1);
         int64_t nabp = a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2;
         int64_t nabm = a1 * (a1 - 1) / 2 - a0 * (a0 - 1) / 2;
-        gemm(ex, false, false, nop, nabp, nvp, 0.5, tp.d(), nop, gp.d(), nvp, 0.0, wp.d(), nop);
+        gemm(ex, false, false, ldp, nabp, nvp, 0.5, tp.d(), ldp, gp.d(), nvp, 0.0, wp.d(), ldp);
         if (nom > 0 && nabm > 0)
-            gemm(ex, false, false, nom, nabm, nvm, 0.5, tm.d(), nom, gm.d(), nvm, 0.0, wm.d(), nom);
-        add_omega_pm(ex, om2, wp.d(), wm.d(), no, nv, a0, a1);
+            gemm(ex, false, false, nvec * nom, nabm, nvm, 0.5, tm.d(), ldm, gm.d(), nvm, 0.0, wm.d(), ldm);
+        for (int64_t v = 0; v < nvec; v++)
+            add_omega_pm(ex, om2 + v * nt2, wp.d() + v * nop, wm.d() + v * nom, no, nv, a0, a1, ldp, ldm);
     }
 }
 
@@ -295,13 +299,19 @@ void Context::set_precision(int32_t precision) {
 //   omega+_ij,ab = sum_cd 1/2 (1 - d_ij/2)(t_cidj + t_cjdi) M_ab[c,d]
 //   omega-_ij,ab = sum_cd 1/2 (t_cidj - t_cjdi) M_ab[c,d]
 // so the split-bf16 integrals M_ab (written by the G GEMM epilogue, all pairs b <= a resident
-// in HBM) meet [T+; T-] in one GEMM of N = n_o^2 and K = n_v^2.
-void Context::ladder_tc(const double *Lvv, const double *t2, double *om2) {
-    cudaStream_t s = ex.stream;
-    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
-    const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
+// in HBM) meet [T+; T-] of all vectors in one GEMM of N = nvec n_o^2 and K = n_v^2.
+//
+// ladder_pairs fills mbuf with M_ab from the given L_vv.  The integrals of the untransformed L_vv
+// (untransformed = true) stay valid until the Cholesky vectors change, so the mixed residual forms
+// them once per Cholesky set; any other L_vv (T1-transformed, or transposed for the adjoint) is
+// formed once per call and shared by all vectors of that call.
+void Context::ladder_pairs(const double *Lvv, bool untransformed) {
     const int np = ex.planes;
-    // split L~_vv rows r = c + nv a (K = J): source element (r, J) = L~[J, a, c] at J + nJ (a + nv c)
+    if (untransformed && mbuf_kind == 1 && mbuf_version == l_version && mbuf_planes == np) return;
+    cudaStream_t s = ex.stream;
+    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2;
+    const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
+    // split L_vv rows r = c + nv a (K = J): source element (r, J) = L[J, a, c] at J + nJ (a + nv c)
     const int64_t l_rows = tc_pad_rows_a(nv2);
     DBuf LS(sizeof(__nv_bfloat16) * np * l_rows * Jp, s);
     {
@@ -320,27 +330,77 @@ void Context::ladder_tc(const double *Lvv, const double *t2, double *om2) {
         permute_add(ex, 1.0, src, 0.0, dst);
         split_rows(ex, LT.d(), nJ, 1, nv2, nJ, l_rows, Jp, LS.as<__nv_bfloat16>());
     }
-    const int64_t rows_T = tc_pad_rows_b(nrow);
-    DBuf TS(sizeof(__nv_bfloat16) * np * rows_T * Kq, s);
-    build_T(ex, t2, no, nv, rows_T, Kq, np, TS.as<__nv_bfloat16>());
     // all pair integrals, resident: [np][mrows][Kq] (padding rows / K positions are never written, so
     // they stay zero when the plane count changes)
     const int64_t mrows = tc_pad_rows_a(nab);
     if (mbuf_bytes < sizeof(__nv_bfloat16) * np * (size_t)mrows * Kq) {
         mbuf = DBuf(sizeof(__nv_bfloat16) * np * (size_t)mrows * Kq, s);
         mbuf_bytes = mbuf.bytes();
-        CU_CHECK(cudaMemsetAsync(mbuf.as<void>(), 0, mbuf_bytes, s));   // padding rows / K stay zero
+        CU_CHECK(cudaMemsetAsync(mbuf.as<void>(), 0, mbuf_bytes, s));
     }
     int64_t nA = ladder_batch > 0 ? ladder_batch : 16;
     for (int64_t a0 = 0; a0 < nv; a0 += nA) {
         int64_t a1 = std::min(nv, a0 + nA);
         tc_gemm_pairs(ex, LS.as<__nv_bfloat16>(), l_rows, Jp, nv, a0, a1, mbuf.as<__nv_bfloat16>(), mrows, Kq, nJ);
     }
-    DBuf W = dalloc(nab * nrow, s);
-    tc_gemm_f64(ex, mbuf.as<__nv_bfloat16>(), mrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nab, nrow, nv2, 1.0, 0.0,
-                W.d(), nab);
-    add_omega_T(ex, om2, W.d(), nab, no, nv);
-    ex.flops += double(nv2) * double(nv2 + 1) * double(nJ) + 2.0 * double(nab) * double(nrow) * double(nv2);
+    ex.flops += double(nv2) * double(nv2 + 1) * double(nJ);
+    mbuf_kind = untransformed ? 1 : 2;
+    mbuf_version = l_version;
+    mbuf_planes = np;
+}
+
+// om2[v] += ladder(pair integrals in mbuf, t2[v]) for nvec packed vectors
+void Context::ladder_tc_apply(const double *t2, double *om2, int64_t nvec) {
+    cudaStream_t s = ex.stream;
+    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
+    const int64_t Kq = tc_pad_k(nv2), mrows = tc_pad_rows_a(nab);
+    const int64_t rows_T = tc_pad_rows_b(nvec * nrow);
+    DBuf TS(sizeof(__nv_bfloat16) * ex.planes * rows_T * Kq, s);
+    build_T(ex, t2, nvec, no, nv, rows_T, Kq, ex.planes, TS.as<__nv_bfloat16>());
+    DBuf W = dalloc(nab * nvec * nrow, s);
+    tc_gemm_f64(ex, mbuf.as<__nv_bfloat16>(), mrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nab, nvec * nrow, nv2, 1.0,
+                0.0, W.d(), nab);
+    for (int64_t v = 0; v < nvec; v++) add_omega_T(ex, om2 + v * nt2, W.d() + v * nrow * nab, nab, no, nv);
+    ex.flops += 2.0 * double(nab) * double(nvec * nrow) * double(nv2);
+}
+
+void Context::ladder_tc(const double *Lvv, const double *t2, double *om2, int64_t nvec, bool untransformed) {
+    ladder_pairs(Lvv, untransformed);
+    ladder_tc_apply(t2, om2, nvec);
+}
+
+// The A2 ladder of the residual on the tensor cores, without forming T1-transformed integrals.
+// With L~_vv = L_vv - t1 L_ov (the T1 transformation of the vv block),
+//   g~_acbd = g_acbd - sum_k t_ak g_kcbd - sum_l t_bl g_acld + sum_kl t_ak t_bl g_kcld,
+// so X_aibj = sum_cd g~_acbd t_cidj (symmetric in ai <-> bj) is
+//   X = sum_cd g_acbd t_cidj - (A + A^T) + T4,   A_aibj = sum_k t_ak Y_kibj,
+//   Y_kibj = sum_cd g_kcbd t_cidj,   T4_aibj = sum_kl t_ak t_bl Q_kilj,   Q_kilj = sum_cd g_kcld t_cidj,
+// (the A^T term uses sum_cd g_acld t_cidj = Y_ljai), all with untransformed integrals: the v^4
+// integrals are formed once per Cholesky set instead of every iteration, the corrections cost
+// o^2 v^3 N_J + o^3 v^3.  The ladder adds pack(X) with the doubles diagonal halved to om2.
+void Context::ladder_residual_mixed(const double *t1, const double *tf, const double *t2, double *om2) {
+    cudaStream_t s = ex.stream;
+    ladder_tc(L_vv.d(), t2, om2, 1, true);
+    DBuf Y = dalloc(no * no * nv * no, s);
+    ladder_y(L_vv.d(), tf, Y.d());
+    DBuf S = dalloc(nov * nov, s), A = dalloc(nov * nov, s);
+    contract(ex, "ak,kibj->aibj", -1.0, tv(t1, {nv, no}), tv(Y.d(), {no, no, nv, no}), 0.0,
+             tv(A.d(), {nv, no, nv, no}));
+    permute_add(ex, 1.0, tv(A.d(), {nv, no, nv, no}), 0.0, tv(S.d(), {nv, no, nv, no}));
+    TV At = tv(A.d(), {nv, no, nv, no});
+    std::swap(At.s[0], At.s[2]);
+    std::swap(At.s[1], At.s[3]);
+    permute_add(ex, 1.0, At, 1.0, tv(S.d(), {nv, no, nv, no}));
+    {
+        DBuf Q = dalloc(no * no * no * no, s), B = dalloc(nv * no * no * no, s);
+        contract(ex, "kcld,cidj->kilj", 1.0, tv(g_ovov_const(), {no, nv, no, nv}), tv(tf, {nv, no, nv, no}), 0.0,
+                 tv(Q.d(), {no, no, no, no}));
+        contract(ex, "ak,kilj->ailj", 1.0, tv(t1, {nv, no}), tv(Q.d(), {no, no, no, no}), 0.0,
+                 tv(B.d(), {nv, no, no, no}));
+        contract(ex, "bl,ailj->aibj", 1.0, tv(t1, {nv, no}), tv(B.d(), {nv, no, no, no}), 1.0,
+                 tv(S.d(), {nv, no, nv, no}));
+    }
+    pack_half_diag_add(ex, 1.0, S.d(), om2, nov);
 }
 
 // ---------------------------------------------------------------------------

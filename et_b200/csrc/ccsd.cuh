@@ -38,6 +38,10 @@ struct Context {
     size_t mbuf_bytes = 0;
     DBuf gov;                  // g_iajb cache (g_ovov_const)
     bool have_gov = false;
+    int64_t l_version = 0;     // bumped whenever the Cholesky vectors change
+    // what mbuf holds: 0 nothing, 1 untransformed L_vv pairs (valid for mbuf_version), 2 per call
+    int mbuf_kind = 0, mbuf_planes = 0;
+    int64_t mbuf_version = -1;
 
     Context(int64_t no, int64_t nv, int64_t nJ, const ccsd_gpu_options *opt);
     ~Context();
@@ -62,9 +66,14 @@ struct Context {
     void jacobian_transpose(int64_t nvec, const double *b, double *sigma);
     void adjoint(const double *b, double *dt, double *dL, double *dh);
     void set_h_blocks();
-    // A2 ladder: om2 += ladder(L_vv in (J, a, c) layout, packed t2)
-    void ladder(const double *Lvv, const double *t2, double *om2);
-    void ladder_tc(const double *Lvv, const double *t2, double *om2);
+    // A2 ladder: om2[v] += ladder(L_vv in (J, a, c) layout, packed t2[v]) for nvec vectors (stride
+    // n_t2); the integrals are formed once per call
+    void ladder(const double *Lvv, const double *t2, double *om2, int64_t nvec = 1);
+    void ladder_tc(const double *Lvv, const double *t2, double *om2, int64_t nvec, bool untransformed);
+    void ladder_pairs(const double *Lvv, bool untransformed);
+    void ladder_tc_apply(const double *t2, double *om2, int64_t nvec);
+    // the residual's ladder in mixed precision from untransformed integrals plus t1 corrections
+    void ladder_residual_mixed(const double *t1, const double *tf, const double *t2, double *om2);
     int davidson(int nstates, int side, const ccsd_gpu_davidson_options *o, double *omega_out, double *vectors_out,
                  int32_t *iters_out, const double *start = nullptr);
     void eta(double *out);

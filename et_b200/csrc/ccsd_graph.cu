@@ -237,14 +237,19 @@ void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv
         return LTcache->d();
     };
     CustomOp op;
-    op.forward = [this, &g, om2, Lvv, t2]() { ladder(g.value(Lvv), g.value(t2), g.node(om2).v); };
+    op.forward = [this, &g, om2, Lvv, t2, t1, tf]() {
+        if (ex.prec == Prec::MIXED)
+            ladder_residual_mixed(g.value(t1), g.value(tf), g.value(t2), g.node(om2).v);
+        else
+            ladder(g.value(Lvv), g.value(t2), g.node(om2).v);
+    };
     op.tangent = [this, &g, om2, Lvv, t2, t1, getY](int nvec) {
         REQUIRE(!g.node(Lvv).active || g.node(t1).active, CCSD_GPU_EINVAL,
                 "ladder tangent: L_vv directions are not supported");
         double *out = g.tangent(om2, nvec);
         if (g.node(t2).active) {
             const double *c2 = g.tangent(t2, nvec);
-            for (int n = 0; n < nvec; n++) ladder(g.value(Lvv), c2 + n * nt2, out + n * nt2);
+            ladder(g.value(Lvv), c2, out, nvec);
         }
         if (g.node(t1).active) {
             // d L~_ac = -sum_k c_ak L_kc: term -P(sum_k c_ak Y_kibj + (ai <-> bj))
@@ -272,7 +277,7 @@ void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv
             // the transpose of the packed ladder is the same ladder with L~_vv transposed
             const double *LT = getLT();
             double *t2bar = g.adjoint(t2, nvec);
-            for (int n = 0; n < nvec; n++) ladder(LT, pbar + n * nt2, t2bar + n * nt2);
+            ladder(LT, pbar, t2bar, nvec);
         }
         if (g.node(t1).active || dense) {
             DBuf B = dalloc(nov * nov, ex.stream);

@@ -35,8 +35,8 @@ inline int grid_for(int64_t total, int block) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (total); i += (int64_t)gridDim.x * blockDim.x)
 
 __global__ void build_tpm_kernel(const double *__restrict__ t2, double *__restrict__ tp, double *__restrict__ tm,
-                                 int64_t no, int64_t nv) {
-    const int64_t nop = no * (no + 1) / 2, nvp = nv * (nv + 1) / 2, nom = no * (no - 1) / 2;
+                                 int64_t no, int64_t nv, int64_t ldp, int64_t ldm) {
+    const int64_t nop = no * (no + 1) / 2, nvp = nv * (nv + 1) / 2;
     GRID_STRIDE(idx, nop * nvp) {
         int64_t ij = idx % nop, cd = idx / nop, i, j, c, d;
         untri(ij, i, j);
@@ -44,10 +44,10 @@ __global__ void build_tpm_kernel(const double *__restrict__ t2, double *__restri
         double a = t2[pk(c + nv * i, d + nv * j)];
         double b = t2[pk(c + nv * j, d + nv * i)];
         double f = (c == d ? 0.5 : 1.0) * (i == j ? 0.5 : 1.0);
-        tp[idx] = f * (a + b);
+        tp[ij + ldp * cd] = f * (a + b);
         if (i > j && c > d) {
             int64_t ijm = i * (i - 1) / 2 + j, cdm = c * (c - 1) / 2 + d;
-            tm[ijm + nom * cdm] = a - b;
+            tm[ijm + ldm * cdm] = a - b;
         }
     }
 }
@@ -73,19 +73,20 @@ __global__ void form_gpm_kernel(const double *__restrict__ G, int64_t ldg, doubl
 }
 
 __global__ void add_omega_pm_kernel(double *__restrict__ om2, const double *__restrict__ wp,
-                                    const double *__restrict__ wm, int64_t no, int64_t nv, int64_t a0, int64_t a1) {
-    const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
+                                    const double *__restrict__ wm, int64_t no, int64_t nv, int64_t a0, int64_t a1,
+                                    int64_t ldwp, int64_t ldwm) {
+    const int64_t nop = no * (no + 1) / 2;
     const int64_t abp0 = a0 * (a0 + 1) / 2, nabp = a1 * (a1 + 1) / 2 - abp0;
     const int64_t abm0 = a0 * (a0 - 1) / 2;
     GRID_STRIDE(idx, nop * nabp) {
         int64_t ij = idx % nop, loc = idx / nop, i, j, a, b;
         untri(ij, i, j);
         untri(abp0 + loc, a, b);
-        double p = wp[idx] * (a == b ? 0.5 : 1.0);
+        double p = wp[ij + ldwp * loc] * (a == b ? 0.5 : 1.0);
         double x1 = p, x2 = p;
         if (i != j && a != b) {
             int64_t ijm = i * (i - 1) / 2 + j, locm = a * (a - 1) / 2 + b - abm0;
-            double m = wm[ijm + nom * locm];
+            double m = wm[ijm + ldwm * locm];
             x1 = p + m;
             x2 = p - m;
         }
@@ -102,14 +103,16 @@ __global__ void add_omega_pm_kernel(double *__restrict__ om2, const double *__re
 // T+ and T- of the full-(c,d) ladder as split bf16 rows: row ij_p (i >= j) carries
 // 1/2 (1 - d_ij/2)(t_cidj + t_cjdi), row n_o_p + ij_m (i > j) carries 1/2 (t_cidj - t_cjdi),
 // both at K position c + nv*d; padding rows/columns are zero.
-__global__ void build_T_kernel(const double *__restrict__ t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq,
-                               int np, __nv_bfloat16 *__restrict__ out) {
-    const int64_t nop = no * (no + 1) / 2, nrow = no * no, nv2 = nv * nv;
+__global__ void build_T_kernel(const double *__restrict__ t2s, int64_t nvec, int64_t no, int64_t nv, int64_t rows_pad,
+                               int64_t Kq, int np, __nv_bfloat16 *__restrict__ out) {
+    const int64_t nop = no * (no + 1) / 2, nrow = no * no, nv2 = nv * nv, nt2 = nv * no * (nv * no + 1) / 2;
     const size_t plane = (size_t)rows_pad * Kq;
     GRID_STRIDE(idx, rows_pad * Kq) {
-        int64_t row = idx / Kq, k = idx - (idx / Kq) * Kq;
+        int64_t rr = idx / Kq, k = idx - (idx / Kq) * Kq;
+        const int64_t vec = rr / nrow, row = rr - vec * nrow;   // vector vec owns rows [vec nrow, (vec+1) nrow)
+        const double *t2 = t2s + vec * nt2;
         double val = 0.0;
-        if (row < nrow && k < nv2) {
+        if (vec < nvec && k < nv2) {
             int64_t c = k % nv, d = k / nv, i, j;
             bool plus = row < nop;
             if (plus) untri(row, i, j);
@@ -373,9 +376,9 @@ __global__ void diis_solve_kernel(double *__restrict__ Gslot, int maxdim, const 
 
 }  // namespace
 
-void build_tpm(Exec &ex, const double *t2, double *tp, double *tm, int64_t no, int64_t nv) {
+void build_tpm(Exec &ex, const double *t2, double *tp, double *tm, int64_t no, int64_t nv, int64_t ldp, int64_t ldm) {
     int64_t total = (no * (no + 1) / 2) * (nv * (nv + 1) / 2);
-    build_tpm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(t2, tp, tm, no, nv);
+    build_tpm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(t2, tp, tm, no, nv, ldp, ldm);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }
@@ -388,16 +391,16 @@ void form_gpm(Exec &ex, const double *G, int64_t ldg, double *gp, double *gm, in
 }
 
 void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int64_t no, int64_t nv, int64_t a0,
-                  int64_t a1) {
+                  int64_t a1, int64_t ldwp, int64_t ldwm) {
     int64_t total = (no * (no + 1) / 2) * (a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2);
-    add_omega_pm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, wp, wm, no, nv, a0, a1);
+    add_omega_pm_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, wp, wm, no, nv, a0, a1, ldwp, ldwm);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }
 
-void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
+void build_T(Exec &ex, const double *t2s, int64_t nvec, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
              __nv_bfloat16 *out) {
-    build_T_kernel<<<grid_for(rows_pad * Kq, 256), 256, 0, ex.stream>>>(t2, no, nv, rows_pad, Kq, np, out);
+    build_T_kernel<<<grid_for(rows_pad * Kq, 256), 256, 0, ex.stream>>>(t2s, nvec, no, nv, rows_pad, Kq, np, out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }

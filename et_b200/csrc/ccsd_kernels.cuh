@@ -14,16 +14,17 @@ struct DiisOrder {
 
 // t+ (n_o_p x n_v_p) and t- (n_o_m x n_v_m) of the A2 ladder (construct_plus_minus_2413_from_packed
 // followed by scale_double_packed_blocks(1/2, 1/2); packed_array_utilities_r.F90:140-197, 99-136)
-void build_tpm(Exec &ex, const double *t2, double *tp, double *tm, int64_t no, int64_t nv);
+// (tp leading dimension ldp >= n_o_p, tm leading dimension ldm >= n_o_m: several vectors side by side)
+void build_tpm(Exec &ex, const double *t2, double *tp, double *tm, int64_t no, int64_t nv, int64_t ldp, int64_t ldm);
 // g+- columns for the pairs a in [a0,a1), b <= a from G = g_acbd (construct_plus_minus_1324_from_full)
 void form_gpm(Exec &ex, const double *G, int64_t ldg, double *gp, double *gm, int64_t nv, int64_t a0, int64_t a1);
 // add_double/single_packed_plus_minus with the omega+ (a == b) half scaling
 void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int64_t no, int64_t nv, int64_t a0,
-                  int64_t a1);
+                  int64_t a1, int64_t ldwp, int64_t ldwm);
 
-// T+/T- rows of the tensor-core ladder (np split-bf16 planes, [np][rows_pad][Kq]) and the scatter of
-// its result
-void build_T(Exec &ex, const double *t2, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
+// T+/T- rows of the tensor-core ladder (np split-bf16 planes, [np][rows_pad][Kq]) for nvec packed
+// vectors (stride n_t2; vector v owns rows [v n_o^2, (v+1) n_o^2)) and the scatter of its result
+void build_T(Exec &ex, const double *t2s, int64_t nvec, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
              __nv_bfloat16 *out);
 void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv);
 
