@@ -108,6 +108,7 @@ SIGNATURES = {
     "ccsd_gpu_mixed_gemm_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _I64, _I64, _I64, ctypes.c_double,
                                                    _VP, _I64, _VP, _I64, ctypes.c_double, _VP, _I64, _VP]),
     "ccsd_gpu_omega_flops": (ctypes.c_double, [_VP]),
+    "ccsd_gpu_one_electron_density": (ctypes.c_int, [_VP, _DP, _DP]),
     "ccsd_gpu_solve_gs_batch": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(BatchSystem), ctypes.POINTER(Options),
                                                ctypes.POINTER(SolverOptions), ctypes.c_int32, _DP,
                                                ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
@@ -315,6 +316,14 @@ class CCSD:
         if rc != 0 and (raise_on_failure or rc != -5):
             self._check(rc)
         return om, (vec.reshape(self.n_amp, n_states, order="F") if vectors else None), it.value
+
+    def one_electron_density(self, tbar):
+        """Unrelaxed CCSD one-electron density in the MO basis (n_mo x n_mo): d(E + tbar^T Omega)/dh
+        at the current amplitudes (eT: construct_gs_density_doubles, in the T1 basis)."""
+        tb = _f64(tbar, self.n_amp)
+        D = np.zeros(self.n_mo * self.n_mo)
+        self._check(self.lib.ccsd_gpu_one_electron_density(self.ctx, _dp(tb), _dp(D)))
+        return D.reshape(self.n_mo, self.n_mo, order="F")
 
     def construct_eta(self):
         out = np.empty(self.n_amp)

@@ -249,6 +249,18 @@ int ccsd_gpu_vjp(void *ctx, const double *b, double *dt, double *dL, double *dh)
     });
 }
 
+int ccsd_gpu_one_electron_density(void *ctx, const double *tbar, double *D) {
+    return guarded(ctx, [&](Context &x) {
+        REQUIRE(tbar != nullptr && D != nullptr, CCSD_GPU_EINVAL, "null multipliers or density");
+        cudaStream_t s = x.ex.stream;
+        ccsd::DBuf db = ccsd::dalloc(x.namp, s), dD = ccsd::dalloc(x.nmo * x.nmo, s);
+        h2d(x, db.d(), tbar, x.namp);
+        x.adjoint(db.d(), nullptr, nullptr, dD.d());                   // tbar^T dOmega/dh
+        ccsd::density_energy_part(x.ex, dD.d(), x.t.d(), x.no, x.nv);   // + dE/dh
+        d2h(x, D, dD.d(), x.nmo * x.nmo);
+    });
+}
+
 int ccsd_gpu_eom_davidson(void *ctx, int32_t n_states, int32_t side, const ccsd_gpu_davidson_options *opt,
                           double *omega, double *vectors, int32_t *iterations) {
     int status = CCSD_GPU_OK;

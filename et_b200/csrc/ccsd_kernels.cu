@@ -158,6 +158,21 @@ __global__ void add_omega_T_kernel(double *__restrict__ om2, const double *__res
     }
 }
 
+// D += the h-derivative of the energy at fixed amplitudes: 2 on the occupied diagonal (reference)
+// and 2 t_ai at (i, n_o + a) (the singles term through h~_ii = h_ii + sum_a h_ia t_ai)
+__global__ void density_energy_part_kernel(double *__restrict__ D, const double *__restrict__ t1, int64_t no,
+                                           int64_t nv) {
+    const int64_t nmo = no + nv;
+    GRID_STRIDE(idx, no * nv + no) {
+        if (idx < no) {
+            D[idx + nmo * idx] += 2.0;
+        } else {
+            const int64_t k = idx - no, a = k % nv, i = k / nv;   // t1 (v, o): t_ai at a + nv i
+            D[i + nmo * (no + a)] += 2.0 * t1[a + nv * i];
+        }
+    }
+}
+
 // eta_ai = 2 F_ia, eta_aibj = 4 g_iajb - 2 g_ibja packed (construct_eta_ccsd); F is n_mo x n_mo,
 // g is (o, v, o, v)
 __global__ void eta_kernel(const double *__restrict__ F, const double *__restrict__ g, int64_t no, int64_t nv,
@@ -408,6 +423,12 @@ void build_T(Exec &ex, const double *t2s, int64_t nvec, int64_t no, int64_t nv, 
 void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv) {
     int64_t total = (nv * (nv + 1) / 2) * (no * (no + 1) / 2);
     add_omega_T_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, W, ldw, no, nv);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void density_energy_part(Exec &ex, double *D, const double *t1, int64_t no, int64_t nv) {
+    density_energy_part_kernel<<<grid_for(no * nv + no, 256), 256, 0, ex.stream>>>(D, t1, no, nv);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }

@@ -30,6 +30,8 @@ void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no
 
 // eta of the multiplier equation (construct_eta_ccsd, multiplier_equation_ccsd.F90:50-113) and the
 // initial multipliers (t1, packed contravariant t2; ccsd_class.F90:411-475)
+// D (n_mo x n_mo) += dE/dh at fixed amplitudes (reference 2 on the occupied diagonal, 2 t_ai at (i, a))
+void density_energy_part(Exec &ex, double *D, const double *t1, int64_t no, int64_t nv);
 void construct_eta(Exec &ex, const double *F, const double *g_ovov, int64_t no, int64_t nv, double *eta);
 void multiplier_guess(Exec &ex, const double *t, int64_t no, int64_t nv, double *out);
 

@@ -1,6 +1,8 @@
 // Tensor primitives: strided permutations (smem-tiled when the fastest index changes),
 // GEMM-backed contractions, packed-doubles conversions and deterministic reductions.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 
@@ -84,8 +86,32 @@ int grid_for(int64_t total, int block) {
 
 }  // namespace
 
+namespace {
+// CCSD_GPU_TRACE=2: every permutation on stderr, tagged with the contraction that asked for it
+thread_local const char *g_perm_tag = nullptr;
+int trace_level() {
+    static const int level = [] {
+        const char *e = std::getenv("CCSD_GPU_TRACE");
+        return e ? std::atoi(e) : 0;
+    }();
+    return level;
+}
+struct PermTag {
+    const char *prev;
+    explicit PermTag(const char *t) : prev(g_perm_tag) { g_perm_tag = t; }
+    ~PermTag() { g_perm_tag = prev; }
+};
+}  // namespace
+
 void permute_add(Exec &ex, double alpha, const TV &in, double beta, const TV &out) {
     REQUIRE(in.nd == out.nd, CCSD_GPU_EINVAL, "permute_add: rank mismatch");
+    if (trace_level() >= 2) {
+        std::string d;
+        for (int k = 0; k < in.nd; k++)
+            d += " " + std::to_string(in.n[k]) + ":" + std::to_string(in.s[k]) + "->" + std::to_string(out.s[k]);
+        std::fprintf(stderr, "ccsd_gpu permute [%s] %.1f MB beta %g dims%s\n", g_perm_tag ? g_perm_tag : "direct",
+                     8e-6 * (double)in.size(), beta, d.c_str());
+    }
     // drop unit dims
     std::vector<int> dims;
     for (int d = 0; d < in.nd; d++) {
@@ -144,8 +170,12 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
     double fl = 2.0 * double(m) * double(n) * double(k);
     ex.flops += fl;
     // the tensor-core tile is 128 x 256 x 64: skinny products stay on the FP64 pipe
-    if (allow_mixed && ex.prec == Prec::MIXED && fl >= ex.mixed_min_flops && k >= 16 &&
-        (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64))) {
+    const bool mixed = allow_mixed && ex.prec == Prec::MIXED && fl >= ex.mixed_min_flops && k >= 16 &&
+                       (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64));
+    if (trace_level() >= 2)
+        std::fprintf(stderr, "ccsd_gpu gemm [%s] %s m %lld n %lld k %lld  %.3g flop\n", g_perm_tag ? g_perm_tag : "direct",
+                     mixed ? "bf16x3" : "fp64", (long long)m, (long long)n, (long long)k, fl);
+    if (mixed) {
         mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
         return;
     }
@@ -239,6 +269,7 @@ TV make_contiguous(Exec &ex, const TV &v, const std::vector<int> &g1, const std:
 }  // namespace
 
 void contract(Exec &ex, const char *spec, double alpha, const TV &A, const TV &B, double beta, const TV &C) {
+    PermTag tag(spec);
     std::string s(spec);
     size_t comma = s.find(','), arrow = s.find("->");
     REQUIRE(comma != std::string::npos && arrow != std::string::npos, CCSD_GPU_EINVAL, "contract: bad spec");

@@ -132,6 +132,15 @@ int ccsd_gpu_jacobian_transpose_device(void *ctx, int64_t n_vec, const double *d
  * No eT routine returns the L and h parts; they are the density-like contributions of the adjoint. */
 int ccsd_gpu_vjp(void *ctx, const double *b, double *dt, double *dL, double *dh);
 
+/* Unrelaxed CCSD one-electron density in the MO basis of h (n_mo x n_mo, column-major):
+ *   D_pq = d(E + tbar^T Omega)/dh_pq  at the current amplitudes, orbitals held fixed,
+ * i.e. the reference part, the singles part 2 t_ai and tbar^T dOmega/dh (ccsd_gpu_vjp).  With t
+ * converged and tbar from ccsd_gpu_solve_multipliers, sum_pq V_pq D_pq is the first-order energy
+ * response to h -> h + V (a dipole moment for V = the dipole integrals).  eT builds the same
+ * density in the T1 basis (construct_gs_density_doubles, mean_value_doubles.F90:78-114):
+ * D_T1 = (1 + t1^T) D (1 - t1^T), with t1 placed in the (virtual, occupied) block. */
+int ccsd_gpu_one_electron_density(void *ctx, const double *tbar, double *D);
+
 typedef struct ccsd_gpu_davidson_options {
     int32_t max_iterations;      /* default 100 */
     int32_t block;               /* trial vectors per batched transformation (0 = by memory) */

@@ -190,7 +190,7 @@ def omega_ccsd(t1, t2p, L_mo, L_t1, F, n_o, *, ladder="dense"):
     nov = n_v * n_o
     o = slice(0, n_o)
     v = slice(n_o, None)
-    dt = np.result_type(t1, t2p, L_t1)
+    dt = np.result_type(t1, t2p, L_t1, F)
 
     # omega_ccs_a1 (omega_ccs.F90:62): Omega_ai += F_ai
     om1 = np.array(F[v, o], dtype=dt, copy=True)
@@ -446,6 +446,32 @@ class CCSDSystem:
             e[k] = 1.0
             A[:, k] = self.jacobian_transformation(e)
         return A
+
+
+def one_electron_density(sysm, tbar, h=1e-30):
+    """Unrelaxed CCSD one-electron density in the MO basis of h:
+    D_pq = d(E + tbar^T Omega)/dh_pq at fixed amplitudes and orbitals.
+
+    eT forms the same density in the T1 basis (construct_gs_density_doubles,
+    src/wavefunctions/doubles/mean_value_doubles.F90:78-114: D = <Lambda| E_pq |CC>); with
+    h~ = (1 - t1) h (1 + t1) the two are related by D_T1 = (1 + t1^T) D (1 - t1^T).  The energy
+    depends on h through the reference (2 on the occupied diagonal) and through the singles term
+    2 sum_ai F_ia t_ai (F_ia = h_ia + ...; it vanishes at a Hartree-Fock reference but not its
+    derivative); tbar^T dOmega/dh is taken by complex-step differentiation."""
+    n_o, n_v = sysm.n_o, sysm.n_v
+    n = n_o + n_v
+    D = np.zeros((n, n))
+    D[:n_o, :n_o] += 2.0 * np.eye(n_o)
+    D[:n_o, n_o:] += 2.0 * sysm.t1.T
+    L_t1 = construct_t1_cholesky(sysm.L_mo, sysm.t1, n_o)
+    for p in range(n):
+        for q in range(n):
+            hc = sysm.h_mo.astype(np.complex128)
+            hc[p, q] += 1j * h
+            F = construct_fock(hc, L_t1, sysm.t1, n_o)
+            om = omega_ccsd(sysm.t1, sysm.t2, sysm.L_mo, L_t1, F, n_o)
+            D[p, q] += tbar @ (np.imag(om) / h)
+    return D
 
 
 def construct_eta(F, L_t1, n_o):

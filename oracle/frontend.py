@@ -33,6 +33,7 @@ def _lib():
     dp = ctypes.POINTER(ctypes.c_double)
     ip = ctypes.POINTER(ctypes.c_int)
     lib.one_electron.argtypes = [ctypes.c_int, ip, dp, dp, ctypes.c_int, dp, dp, dp, dp, dp]
+    lib.dipole.argtypes = [ctypes.c_int, ip, dp, dp, dp, dp, dp, dp]
     lib.eri_all.argtypes = [ctypes.c_int, ip, dp, dp, dp]
     return lib
 
@@ -51,11 +52,13 @@ def parse_g94(text: str, elements) -> dict:
             while not lines[i].startswith("****"):
                 head = lines[i].split()
                 kind, nprim = head[0].upper(), int(head[1])
-                prims = []
-                for k in range(nprim):
-                    a, c = lines[i + 1 + k].replace("D", "E").split()[:2]
-                    prims.append((float(a), float(c)))
-                shells.append((L_OF[kind], prims))
+                rows = [lines[i + 1 + k].replace("D", "E").split() for k in range(nprim)]
+                if kind == "SP":
+                    # an s and a p shell sharing exponents (s first, as the basis lists them)
+                    shells.append((0, [(float(r[0]), float(r[1])) for r in rows]))
+                    shells.append((1, [(float(r[0]), float(r[2])) for r in rows]))
+                else:
+                    shells.append((L_OF[kind], [(float(r[0]), float(r[1])) for r in rows]))
                 i += nprim + 1
             out[el] = shells
         i += 1
@@ -100,8 +103,8 @@ def molecule_from_angstrom(symbols, coords):
     return Molecule(list(symbols), np.asarray(coords, dtype=float) * BOHR_PER_ANGSTROM)
 
 
-def ao_integrals(mol: Molecule, basis: dict):
-    """S, T, V and the AO ERI tensor over spherical, normalised contracted functions."""
+def _contracted(mol: Molecule, basis: dict):
+    """Primitive Cartesian shells and the (unnormalised) map T from them to the contracted spherical AOs."""
     prim_l, prim_a, prim_c = [], [], []
     rows = []          # contracted spherical AO -> list of (prim cart index, coefficient)
     ncart_off = 0
@@ -129,16 +132,44 @@ def ao_integrals(mol: Molecule, basis: dict):
                         if sph[m, k] != 0.0:
                             row[off + k] = row.get(off + k, 0.0) + c * norm * sph[m, k]
                 rows.append(row)
-    n_prim = ncart_off
-    T = np.zeros((len(rows), n_prim))
+    T = np.zeros((len(rows), ncart_off))
     for r, row in enumerate(rows):
         for k, val in row.items():
             T[r, k] = val
+    return (np.array(prim_l, dtype=np.int32), np.array(prim_a, dtype=np.float64),
+            np.ascontiguousarray(np.array(prim_c, dtype=np.float64)), T)
+
+
+def ao_dipole(mol: Molecule, basis: dict, origin=(0.0, 0.0, 0.0)):
+    """<mu| r - origin |nu> over the normalised contracted AOs of ao_integrals: array (3, n_ao, n_ao), bohr."""
+    l_arr, a_arr, c_arr, T = _contracted(mol, basis)
+    n_prim = T.shape[1]
     lib = _lib()
-    nsh = len(prim_l)
-    l_arr = np.array(prim_l, dtype=np.int32)
-    a_arr = np.array(prim_a, dtype=np.float64)
-    c_arr = np.ascontiguousarray(np.array(prim_c, dtype=np.float64))
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    S = np.zeros((n_prim, n_prim))
+    Tk = np.zeros((n_prim, n_prim))
+    V = np.zeros((n_prim, n_prim))
+    Z = np.zeros(1)
+    cpos = np.zeros(3)
+    lib.one_electron(len(l_arr), l_arr.ctypes.data_as(ip), a_arr.ctypes.data_as(dp), c_arr.ctypes.data_as(dp),
+                     0, Z.ctypes.data_as(dp), cpos.ctypes.data_as(dp), S.ctypes.data_as(dp), Tk.ctypes.data_as(dp),
+                     V.ctypes.data_as(dp))
+    M = [np.zeros((n_prim, n_prim)) for _ in range(3)]
+    o = np.ascontiguousarray(np.asarray(origin, dtype=np.float64))
+    lib.dipole(len(l_arr), l_arr.ctypes.data_as(ip), a_arr.ctypes.data_as(dp), c_arr.ctypes.data_as(dp),
+               o.ctypes.data_as(dp), M[0].ctypes.data_as(dp), M[1].ctypes.data_as(dp), M[2].ctypes.data_as(dp))
+    nrm = 1.0 / np.sqrt(np.diag(T @ S @ T.T))
+    Tn = T * nrm[:, None]
+    return np.stack([Tn @ m @ Tn.T for m in M])
+
+
+def ao_integrals(mol: Molecule, basis: dict):
+    """S, T, V and the AO ERI tensor over spherical, normalised contracted functions."""
+    l_arr, a_arr, c_arr, T = _contracted(mol, basis)
+    n_prim = T.shape[1]
+    lib = _lib()
+    nsh = len(l_arr)
     dp = ctypes.POINTER(ctypes.c_double)
     ip = ctypes.POINTER(ctypes.c_int)
     S = np.zeros((n_prim, n_prim))
@@ -257,9 +288,9 @@ def golden_values() -> dict:
         return json.load(f)
 
 
-def golden_basis() -> dict:
+def golden_basis(name: str = "cc-pvdz") -> dict:
     import json
-    with open(os.path.join(GOLDEN, "basis_cc-pvdz.json")) as f:
+    with open(os.path.join(GOLDEN, f"basis_{name}.json")) as f:
         shells = json.load(f)["shells"]
     return {el: [(int(l), [tuple(p) for p in prims]) for l, prims in sh] for el, sh in shells.items()}
 
@@ -297,6 +328,27 @@ def et_restart_system() -> dict:
     return dict(L_mo=L_mo, h_mo=h_mo, eps=z["eps"].copy(), n_o=n_o, e_hf=e_hf, e_nuc=e_nuc, C=C, S=S,
                 t=z["t"].copy(), tbar=z["tbar"].copy(), r=z["r"].copy(), l=z["l"].copy(),
                 omega=z["omega"].copy(), e_ccsd=v["e_ccsd"])
+
+
+def et_dipole_system() -> dict:
+    """eT's tests/ccsd_dipole molecule (H2O and He, STO-3G, Cholesky threshold 1e-11): MO data plus
+    the dipole integrals <p| r |q> in the MO basis (origin 0, bohr) and the nuclear dipole."""
+    v = golden_values()["ccsd_dipole"]
+    sym = [a[0] for a in v["atoms"]]
+    xyz = [a[1:] for a in v["atoms"]]
+    basis = golden_basis(v["basis"])
+    mol = molecule_from_angstrom(sym, xyz)
+    S, Tk, V, eri = ao_integrals(mol, basis)
+    n_o = int(round(mol.charges.sum())) // 2
+    e_nuc = mol.nuclear_repulsion()
+    E_hf, C, eps = rhf(S, Tk + V, eri, n_o, e_nuc)
+    L_ao = pivoted_cholesky(eri, v["cd_threshold"])
+    L_mo = np.einsum("mp,Jmn,nq->Jpq", C, L_ao, C, optimize=True)
+    h_mo = C.T @ (Tk + V) @ C
+    mu_mo = np.einsum("mp,xmn,nq->xpq", C, ao_dipole(mol, basis), C, optimize=True)
+    nuc = (mol.charges[:, None] * mol.coords_bohr).sum(axis=0)
+    return dict(L_mo=L_mo, h_mo=h_mo, eps=eps, n_o=n_o, e_hf=E_hf, e_nuc=e_nuc, mu_mo=mu_mo, nuclear_dipole=nuc,
+                reference=v)
 
 
 # H2O at O (0,0,0), H (0, +-0.757, 0.587) Angstrom, cc-pVDZ, Cholesky threshold 1e-8:

@@ -185,6 +185,42 @@ void one_electron(int nsh, const int *l, const double *alpha, const double *ctr,
     free(off);
 }
 
+/* electric dipole integrals <a| r_d - origin_d |b>, d = x, y, z, over primitive Cartesian functions:
+ * per direction (E^{ij}_1 + (P_d - O_d) E^{ij}_0) sqrt(pi/p), times the overlaps of the other two */
+void dipole(int nsh, const int *l, const double *alpha, const double *ctr, const double *origin,
+            double *Mx, double *My, double *Mz) {
+    int n;
+    int *off = shell_offsets(nsh, l, &n);
+    double *M[3] = {Mx, My, Mz};
+    for (int sa = 0; sa < nsh; sa++)
+        for (int sb = 0; sb < nsh; sb++) {
+            int la = l[sa], lb = l[sb];
+            double a = alpha[sa], b = alpha[sb], p = a + b;
+            const double *A = ctr + 3 * sa, *B = ctr + 3 * sb;
+            double E[3][MAXL + 1][EJ][ET];
+            for (int d = 0; d < 3; d++) hermite_E(la, lb, a, b, A[d], B[d], E[d]);
+            int ca[6][3], cb[6][3];
+            cart_components(la, ca);
+            cart_components(lb, cb);
+            double sq = sqrt(M_PI / p);
+            for (int ia = 0; ia < ncart(la); ia++)
+                for (int ib = 0; ib < ncart(lb); ib++) {
+                    double s1[3], m1[3];
+                    for (int d = 0; d < 3; d++) {
+                        int i = ca[ia][d], j = cb[ib][d];
+                        double P = (a * A[d] + b * B[d]) / p;
+                        s1[d] = E[d][i][j][0] * sq;
+                        m1[d] = (E[d][i][j][1] + (P - origin[d]) * E[d][i][j][0]) * sq;
+                    }
+                    int row = off[sa] + ia, col = off[sb] + ib;
+                    M[0][row * n + col] = m1[0] * s1[1] * s1[2];
+                    M[1][row * n + col] = s1[0] * m1[1] * s1[2];
+                    M[2][row * n + col] = s1[0] * s1[1] * m1[2];
+                }
+        }
+    free(off);
+}
+
 /* (ab|cd) over all primitive Cartesian functions, dense n^4 output */
 void eri_all(int nsh, const int *l, const double *alpha, const double *ctr, double *out) {
     int n;

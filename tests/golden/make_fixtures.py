@@ -6,8 +6,9 @@ Run in a container that has the eT sources mounted (read-only is fine):
 
 It writes
 
-* ``basis_cc-pvdz.json`` - the cc-pVDZ shells of H, He and O, taken from
-  ``ao_basis/cc-pvdz.g94`` (published Dunning basis data), so the oracle's
+* ``basis_cc-pvdz.json``, ``basis_sto-3g.json`` - the cc-pVDZ and STO-3G shells of H, He and O,
+  taken from ``ao_basis/*.g94`` (published basis data; STO-3G's SP shells split into an s and a p
+  shell), so the oracle's
   integral front end can rebuild eT's test molecules without the eT tree;
 * ``et_reference_values.json`` - numbers parsed from eT's committed
   regression outputs (``tests/*/result/*.out``): geometries, HF energies,
@@ -85,6 +86,18 @@ def _test(root, name):
     return inp, out
 
 
+def _dipole(out: str):
+    """The CC dipole table of a mean-value run: electronic / nuclear / total per component, Debye."""
+    block = out[out.index("Dipole moment in [Debye]"):]
+    conv = float(re.search(r"Conversion factor from Debye a\.u\.:\s+(\S+)", block).group(1))
+    rows = {}
+    for comp in ("x", "y", "z"):
+        m = re.search(r"\n\s+%s\s+(-?\d+\.\d+)\s+(-?\d+\.\d+)\s+(-?\d+\.\d+)" % comp, block)
+        rows[comp] = [float(m.group(k)) for k in (1, 2, 3)]
+    return dict(debye_per_au=1.0 / conv, au_per_debye=conv, electronic=[rows[c][0] for c in "xyz"],
+                nuclear=[rows[c][1] for c in "xyz"], total=[rows[c][2] for c in "xyz"])
+
+
 def _restart_vectors(d: str) -> None:
     import numpy as np
     from et_b200 import restart as rs
@@ -123,16 +136,23 @@ def main(root: str) -> None:
     values[name] = dict(source=f"tests/{name}/result/{name}.out", basis=basis, atoms=atoms,
                         cd_threshold=_cd_threshold(inp), e_ccsd=_final_cc(out),
                         excitation_energies=_excitations(out))
+    name = "ccsd_dipole"
+    inp, out = _test(root, name)
+    basis, atoms = _geometry(inp)
+    values[name] = dict(source=f"tests/{name}/result/{name}.out", basis=basis, atoms=atoms,
+                        cd_threshold=_cd_threshold(inp), e_hf=_scf_energy(out), e_ccsd=_final_cc(out),
+                        n_cholesky=_n_cholesky(out), dipole_debye=_dipole(out))
     with open(os.path.join(HERE, "et_reference_values.json"), "w") as f:
         json.dump(values, f, indent=1)
 
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
-    _restart_vectors(os.path.join(root, "tests", name, "old_restart_files"))
+    _restart_vectors(os.path.join(root, "tests", "restart_ccsd_v1.0", "old_restart_files"))
     from oracle.frontend import parse_g94
-    text = open(os.path.join(root, "ao_basis", "cc-pvdz.g94")).read()
-    basis = parse_g94(text, {"H", "He", "O"})
-    with open(os.path.join(HERE, "basis_cc-pvdz.json"), "w") as f:
-        json.dump({"source": "ao_basis/cc-pvdz.g94", "shells": basis}, f, indent=1)
+    for bname in ("cc-pvdz", "sto-3g"):
+        text = open(os.path.join(root, "ao_basis", bname + ".g94")).read()
+        basis = parse_g94(text, {"H", "He", "O"})
+        with open(os.path.join(HERE, f"basis_{bname}.json"), "w") as f:
+            json.dump({"source": f"ao_basis/{bname}.g94", "shells": basis}, f, indent=1)
 
 
 if __name__ == "__main__":
