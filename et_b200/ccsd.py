@@ -79,6 +79,7 @@ SIGNATURES = {
     "ccsd_gpu_synchronize": (ctypes.c_int, [_VP]),
     "ccsd_gpu_set_cholesky_mo": (ctypes.c_int, [_VP, _DP]),
     "ccsd_gpu_set_cholesky_mo_blocks": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
+    "ccsd_gpu_set_cholesky_ao": (ctypes.c_int, [_VP, _I64, _DP, _DP, _DP]),
     "ccsd_gpu_set_h_mo": (ctypes.c_int, [_VP, _DP, _DP, ctypes.c_double]),
     "ccsd_gpu_set_amplitudes": (ctypes.c_int, [_VP, _DP]),
     "ccsd_gpu_get_amplitudes": (ctypes.c_int, [_VP, _DP]),
@@ -200,6 +201,17 @@ class CCSD:
         assert L.shape == (self.n_J, self.n_mo, self.n_mo)
         flat = np.ascontiguousarray(L.reshape(-1, order="F") if not L.flags.f_contiguous else L.ravel(order="K"))
         self._check(self.lib.ccsd_gpu_set_cholesky_mo(self.ctx, _dp(flat)))
+
+    def set_cholesky_ao(self, W_ao, S, C):
+        """MO Cholesky vectors built on the device (construct_cholesky_mo_vectors): W_ao[w, x, K] =
+        (wx|K) over the Cholesky basis, S[K, L] = (K|L), C[w, p] the n_mo orbital coefficients."""
+        W = np.asarray(W_ao, dtype=np.float64)
+        n_ao = W.shape[0]
+        assert W.shape == (n_ao, n_ao, self.n_J)
+        Wf = np.ascontiguousarray(W.reshape(-1, order="F"))
+        Sf = _f64(np.asarray(S, dtype=np.float64).reshape(-1, order="F"), self.n_J * self.n_J)
+        Cf = _f64(np.asarray(C, dtype=np.float64)[:, : self.n_mo].reshape(-1, order="F"), n_ao * self.n_mo)
+        self._check(self.lib.ccsd_gpu_set_cholesky_ao(self.ctx, n_ao, _dp(Wf), _dp(Sf), _dp(Cf)))
 
     def set_h_mo(self, h, eps, e_hf=0.0):
         h = _f64(np.asarray(h, dtype=np.float64).reshape(-1, order="F"), self.n_mo * self.n_mo)

@@ -93,6 +93,14 @@ int ccsd_gpu_set_cholesky_mo(void *ctx, const double *L);
  * (src/eri_tool/abstract_eri_cholesky_class.F90:290-327). */
 int ccsd_gpu_set_cholesky_mo_blocks(void *ctx, const double *L_oo, const double *L_ov,
                                     const double *L_vo, const double *L_vv);
+/* MO Cholesky vectors built on the device from the three-index AO integrals of the Cholesky basis,
+ * as construct_cholesky_mo_vectors (src/solvers/cholesky/eri_cd_class.F90:3132-3472) does:
+ *   L_Jpq = sum_wx C_wp C_xq sum_K (wx|K) [Q^{-T}]_KJ,   S_KL = (K|L) = Q Q^T (Q lower triangular).
+ * W_ao: (wx|K) as (n_ao, n_ao, n_J) column-major for the n_J elements K of the Cholesky basis;
+ * S: (K|L), n_J x n_J; C: n_ao x n_mo orbital coefficients (occupied first).  Replaces
+ * ccsd_gpu_set_cholesky_mo; the factorisation of S, the triangular solve and both transformation
+ * products run on the device. */
+int ccsd_gpu_set_cholesky_ao(void *ctx, int64_t n_ao, const double *W_ao, const double *S, const double *C);
 /* MO one-electron Hamiltonian h (n_mo x n_mo), orbital energies (n_mo) and E_HF
  * (get_t1_oei, src/wavefunctions/ccs/oei_ccs.F90:35-95; wf%orbital_energies; wf%hf_energy). */
 int ccsd_gpu_set_h_mo(void *ctx, const double *h, const double *eps, double e_hf);

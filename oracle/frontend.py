@@ -240,16 +240,18 @@ def rhf(S, H, eri, n_occ, e_nuc, *, conv=1e-12, max_iter=200):
     return E, C, e
 
 
-def pivoted_cholesky(eri, threshold):
-    """Pivoted Cholesky of the (n^2 x n^2) ERI matrix: returns L[J, mu, nu]."""
+def pivoted_cholesky(eri, threshold, pivots=False):
+    """Pivoted Cholesky of the (n^2 x n^2) ERI matrix: returns L[J, mu, nu] (and, with pivots=True,
+    the pivot pairs as indices of the flattened (mu, nu) index, in selection order)."""
     n = eri.shape[0]
     M = eri.reshape(n * n, n * n)
     diag = np.diag(M).copy()
-    vecs = []
+    vecs, piv = [], []
     while True:
         p = int(np.argmax(diag))
         if diag[p] <= threshold:
             break
+        piv.append(p)
         col = M[:, p].copy()
         for v in vecs:
             col -= v * v[p]
@@ -257,7 +259,8 @@ def pivoted_cholesky(eri, threshold):
         vecs.append(v)
         diag -= v * v
         diag[p] = 0.0
-    return np.array(vecs).reshape(len(vecs), n, n)
+    L = np.array(vecs).reshape(len(vecs), n, n)
+    return (L, np.array(piv)) if pivots else L
 
 
 def build_system(symbols, coords_angstrom, basis, *, cd_threshold=1e-12):
