@@ -73,9 +73,10 @@ Context::~Context() {
     if (ex.stream && ex.stream != own_stream) cudaStreamSynchronize(ex.stream);
     // every device buffer is freed (stream-ordered) while its stream still exists
     for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
-                    &mbuf, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
+                    &mbuf, &ybuf, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
         b->release();
     mbuf_bytes = 0;
+    ybuf_bytes = 0;
     if (ex.stream) cudaStreamSynchronize(ex.stream);
     prof.clear();
     if (blas) cublasDestroy(blas);
@@ -369,6 +370,102 @@ void Context::ladder_tc(const double *Lvv, const double *t2, double *om2, int64_
     ladder_tc_apply(t2, om2, nvec);
 }
 
+// Mixed precision keeps the ovvv integrals of the untransformed Cholesky vectors resident as split
+// bf16, ybuf[plane][k + no*b][c + nv*d] = g_kcbd (o v^3 elements per plane: 4.2 GB for both planes
+// at o = 32, v = 320), formed once per Cholesky set by one tensor-core GEMM whose epilogue writes
+// the planes.  The ladder's Y intermediates then cost one GEMM of o^2 x o v x v^2 per call instead
+// of re-forming g_kcbd in batches (and permuting and splitting it) every time.
+bool Context::ovvv_resident() {
+    const size_t need = sizeof(__nv_bfloat16) * (size_t)ex.planes * (size_t)tc_pad_rows_a(nov) * tc_pad_k(nv * nv);
+    if (ybuf_bytes >= need) return true;
+    size_t free_b = 0, total_b = 0;
+    CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    return need < free_b / 4;
+}
+
+void Context::ovvv_pairs() {
+    const int np = ex.planes;
+    if (ybuf_version == l_version && ybuf_planes == np) return;
+    cudaStream_t s = ex.stream;
+    const int64_t nv2 = nv * nv, Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
+    // L_ov split rows c + nv*k: L_ov[J, k, c] sits at J + nJ*(k + no*c); copy to (J, c, k) first
+    const int64_t o_rows = tc_pad_rows_a(nov);
+    DBuf LOS(sizeof(__nv_bfloat16) * np * o_rows * Jp, s);
+    {
+        DBuf LO = dalloc(nJ * nov, s);
+        TV dst = tv(LO.d(), {nJ, no, nv});   // [J, k, c] at J + nJ*(c + nv*k)
+        dst.s[1] = nJ * nv;
+        dst.s[2] = nJ;
+        permute_add(ex, 1.0, tv(L_ov.d(), {nJ, no, nv}), 0.0, dst);
+        split_rows(ex, LO.d(), nJ, 1, nov, nJ, o_rows, Jp, LOS.as<__nv_bfloat16>());
+    }
+    // L_vv split rows d + nv*b: L_vv[J, b, d] sits at J + nJ*(b + nv*d); copy to (J, d, b)
+    const int64_t v_rows = tc_pad_rows_b(nv2);
+    DBuf LVS(sizeof(__nv_bfloat16) * np * v_rows * Jp, s);
+    {
+        DBuf LV = dalloc(nJ * nv2, s);
+        TV dst = tv(LV.d(), {nJ, nv, nv});   // [J, b, d] at J + nJ*(d + nv*b)
+        dst.s[1] = nJ * nv;
+        dst.s[2] = nJ;
+        permute_add(ex, 1.0, tv(L_vv.d(), {nJ, nv, nv}), 0.0, dst);
+        split_rows(ex, LV.d(), nJ, 1, nv2, nJ, v_rows, Jp, LVS.as<__nv_bfloat16>());
+    }
+    const int64_t yrows = tc_pad_rows_a(nov);
+    const size_t need = sizeof(__nv_bfloat16) * (size_t)np * (size_t)yrows * Kq;
+    if (ybuf_bytes < need) {
+        ybuf = DBuf();
+        ybuf = DBuf(need, s);
+        ybuf_bytes = need;
+        // padding rows and K positions are never written and must read as zero
+        CU_CHECK(cudaMemsetAsync(ybuf.as<void>(), 0, need, s));
+    }
+    tc_gemm_ovvv(ex, LOS.as<__nv_bfloat16>(), o_rows, LVS.as<__nv_bfloat16>(), v_rows, Jp, no, nv,
+                 ybuf.as<__nv_bfloat16>(), yrows, Kq, nJ);
+    ybuf_version = l_version;
+    ybuf_planes = np;
+}
+
+void Context::ladder_y0(const double *tf, double *Y) {
+    ovvv_pairs();
+    cudaStream_t s = ex.stream;
+    const int64_t nv2 = nv * nv, oo = no * no, Kq = tc_pad_k(nv2), yrows = tc_pad_rows_a(nov);
+    const int64_t rows_T = tc_pad_rows_b(oo);
+    DBuf TS(sizeof(__nv_bfloat16) * ex.planes * rows_T * Kq, s);
+    {
+        // tau split rows i + no*j, K position c + nv*d: copy tau[c, i, d, j] to (c, d, i, j)
+        DBuf TT = dalloc(oo * nv2, s);
+        TV dst = tv(TT.d(), {nv, no, nv, no});
+        dst.s[1] = nv2;        // i
+        dst.s[2] = nv;         // d
+        dst.s[3] = nv2 * no;   // j
+        permute_add(ex, 1.0, tv(tf, {nv, no, nv, no}), 0.0, dst);
+        split_rows(ex, TT.d(), nv2, 1, oo, nv2, rows_T, Kq, TS.as<__nv_bfloat16>());
+    }
+    // Yt[(k + no*b) + nov*(i + no*j)], then Y[k, i, b, j]
+    DBuf Yt = dalloc(nov * oo, s);
+    tc_gemm_f64(ex, ybuf.as<__nv_bfloat16>(), yrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nov, oo, nv2, 1.0, 0.0,
+                Yt.d(), nov, 0);
+    TV src = tv(Yt.d(), {no, no, nv, no});   // (k, i, b, j)
+    src.s[1] = nov;
+    src.s[2] = no;
+    src.s[3] = nov * no;
+    permute_add(ex, 1.0, src, 0.0, tv(Y, {no, no, nv, no}));
+}
+
+void Context::ladder_y_t1(const double *t1, const double *Ltvv, const double *tf, double *Y) {
+    if (!(ex.prec == Prec::MIXED && ovvv_resident())) {
+        ladder_y(Ltvv, tf, Y);
+        return;
+    }
+    ladder_y0(tf, Y);
+    // L~_bd = L_bd - sum_l t_bl L_ld, so g_kc~bd = g_kcbd - sum_l t_bl g_kcld
+    DBuf Q = dalloc(no * no * no * no, ex.stream);
+    contract(ex, "kcld,cidj->kilj", 1.0, tv(g_ovov_const(), {no, nv, no, nv}), tv(tf, {nv, no, nv, no}), 0.0,
+             tv(Q.d(), {no, no, no, no}));
+    contract(ex, "bl,kilj->kibj", -1.0, tv(t1, {nv, no}), tv(Q.d(), {no, no, no, no}), 1.0,
+             tv(Y, {no, no, nv, no}));
+}
+
 // The A2 ladder of the residual on the tensor cores, without forming T1-transformed integrals.
 // With L~_vv = L_vv - t1 L_ov (the T1 transformation of the vv block),
 //   g~_acbd = g_acbd - sum_k t_ak g_kcbd - sum_l t_bl g_acld + sum_kl t_ak t_bl g_kcld,
@@ -382,7 +479,8 @@ void Context::ladder_residual_mixed(const double *t1, const double *tf, const do
     cudaStream_t s = ex.stream;
     ladder_tc(L_vv.d(), t2, om2, 1, true);
     DBuf Y = dalloc(no * no * nv * no, s);
-    ladder_y(L_vv.d(), tf, Y.d());
+    if (ovvv_resident()) ladder_y0(tf, Y.d());
+    else ladder_y(L_vv.d(), tf, Y.d());
     DBuf S = dalloc(nov * nov, s), A = dalloc(nov * nov, s);
     contract(ex, "ak,kibj->aibj", -1.0, tv(t1, {nv, no}), tv(Y.d(), {no, no, nv, no}), 0.0,
              tv(A.d(), {nv, no, nv, no}));

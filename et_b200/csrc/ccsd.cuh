@@ -26,6 +26,8 @@ struct Context {
     bool have_L = false, have_h = false, have_t = false;
     std::string err;
 
+    // Device buffers are stream-ordered allocations on the context's stream: ~Context() releases
+    // each of them before it destroys that stream, so a new resident buffer joins its list.
     // MO Cholesky blocks (J, p, q) and their T1-transformed counterparts
     DBuf L_oo, L_ov, L_vo, L_vv;
     DBuf Lt_oo, Lt_ov, Lt_vo, Lt_vv;
@@ -42,6 +44,12 @@ struct Context {
     // what mbuf holds: 0 nothing, 1 untransformed L_vv pairs (valid for mbuf_version), 2 per call
     int mbuf_kind = 0, mbuf_planes = 0;
     int64_t mbuf_version = -1;
+    // split-bf16 ovvv integrals g_kcbd of the untransformed vectors at [plane][k + no*b][c + nv*d]
+    // (mixed precision; valid for ybuf_version)
+    DBuf ybuf;
+    size_t ybuf_bytes = 0;
+    int ybuf_planes = 0;
+    int64_t ybuf_version = -1;
 
     Context(int64_t no, int64_t nv, int64_t nJ, const ccsd_gpu_options *opt);
     ~Context();
@@ -62,6 +70,14 @@ struct Context {
     OmegaNodes record_omega(Graph &g, bool const_ovov = true);
     void record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv_in, int tf);
     void ladder_y(const double *Lvv, const double *tfull, double *Y);
+    // mixed precision: whether the resident ovvv planes fit, their construction, and
+    // Y0_kibj = sum_cd g_kcbd tau_cidj from them
+    bool ovvv_resident();
+    void ovvv_pairs();
+    void ladder_y0(const double *tfull, double *Y);
+    // Y with the T1-transformed vv block Ltvv, sum_cd g_kc~bd tau_cidj: in mixed precision
+    // Y0_kibj - sum_l t_bl Q_kilj (Q_kilj = sum_cd g_kcld tau_cidj), else ladder_y(Ltvv)
+    void ladder_y_t1(const double *t1, const double *Ltvv, const double *tfull, double *Y);
     void jacobian(int64_t nvec, const double *c, double *rho);
     void jacobian_transpose(int64_t nvec, const double *b, double *sigma);
     void adjoint(const double *b, double *dt, double *dL, double *dh);

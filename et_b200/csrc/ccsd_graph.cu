@@ -195,7 +195,8 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     return n;
 }
 
-// Y[k,i,b,j] = sum_cd g_kcbd t_cidj with g_kcbd = sum_J L_kc L~_bd (batched over b)
+// Y[k,i,b,j] = sum_cd g_kcbd t_cidj with g_kcbd = sum_J L_kc L~_bd (batched over b; in mixed
+// precision the residual and the derivatives take Y from the resident ovvv planes instead)
 void Context::ladder_y(const double *Lvv, const double *tfull, double *Y) {
     cudaStream_t s = ex.stream;
     const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(nv, (int64_t)(2.0e9 / (8.0 * no * nv * nv))));
@@ -218,10 +219,10 @@ void Context::ladder_y(const double *Lvv, const double *tfull, double *Y) {
 void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv_in, int tf) {
     auto Ycache = std::make_shared<DBuf>();
     auto LTcache = std::make_shared<DBuf>();
-    auto getY = [this, &g, Lvv, tf, Ycache]() -> const double * {
+    auto getY = [this, &g, Lvv, t1, tf, Ycache]() -> const double * {
         if (!*Ycache) {
             *Ycache = dalloc(no * no * nv * no, ex.stream);
-            ladder_y(g.value(Lvv), g.value(tf), Ycache->d());
+            ladder_y_t1(g.value(t1), g.value(Lvv), g.value(tf), Ycache->d());
         }
         return Ycache->d();
     };

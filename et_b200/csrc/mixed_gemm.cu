@@ -173,6 +173,17 @@ struct EpiF64 {
     }
 };
 
+// v as np bf16 planes at out[idx], out[plane + idx], ...: each plane is the bf16 rounding of what
+// the planes before it leave over (the differences are exact in FP32)
+__device__ __forceinline__ void store_split_planes(__nv_bfloat16 *out, size_t plane, size_t idx, float v, int np) {
+    __nv_bfloat16 hi = __float2bfloat16(v);
+    const float r = v - __bfloat162float(hi);
+    __nv_bfloat16 mid = __float2bfloat16(r);
+    out[idx] = hi;
+    out[plane + idx] = mid;
+    if (np == 3) out[2 * plane + idx] = __float2bfloat16(r - __bfloat162float(mid));
+}
+
 // A2 ladder integrals: row (c, a) = c + nv*(a - a0), column (d, b) = d + nv*b of
 // G = L_vv^T L_vv is M_ab[c,d] = g_acbd; kept for b <= a and written as np bf16 planes at
 // pair row ab = a(a+1)/2 + b, K position c + nv*d.
@@ -198,12 +209,36 @@ struct EpiPairs {
         const int b = col / nv, d = col - b * nv;
         if (b > a) return;
         const size_t idx = (size_t)((long long)a * (a + 1) / 2 + b) * ldk + c + (long long)nv * d;
-        __nv_bfloat16 hi = __float2bfloat16(v);
-        const float r = v - __bfloat162float(hi);   // exact in FP32
-        __nv_bfloat16 mid = __float2bfloat16(r);
-        out[idx] = hi;
-        out[plane + idx] = mid;
-        if (np == 3) out[2 * plane + idx] = __float2bfloat16(r - __bfloat162float(mid));
+        store_split_planes(out, plane, idx, v, np);
+    }
+};
+
+// ovvv integrals of the untransformed Cholesky vectors for the ladder's Y intermediate: row
+// (c, k) = c + nv*k of L_ov, column (d, b) = d + nv*b of L_vv, so G = L_ov^T L_vv holds
+// g_kcbd; written as np bf16 planes at row k + no*b, K position c + nv*d (the 32 lanes of a warp
+// take consecutive c and store to consecutive addresses).
+struct EpiOvvv {
+    static constexpr bool kChunked = false;
+    __nv_bfloat16 *out;
+    size_t plane;
+    long long ldk;
+    int no, nv, M, N, np;
+    int k, c;
+    __device__ __forceinline__ void tile_setup(int) {}
+    __device__ __forceinline__ void row_setup(int row) {
+        k = row / nv;
+        c = row - k * nv;
+    }
+    __device__ __forceinline__ void apply16(int row, int col0, const float (&v)[16], bool) const {
+        if (row >= M) return;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int col = col0 + j;
+            if (col >= N) return;
+            const int b = col / nv, d = col - b * nv;
+            const size_t idx = (size_t)(k + (long long)no * b) * ldk + c + (long long)nv * d;
+            store_split_planes(out, plane, idx, v[j], np);
+        }
     }
 };
 
@@ -559,6 +594,27 @@ int check_planes(int planes) {
     return planes;
 }
 
+// K splits for an output of `tiles` tiles over nkt K blocks: the count (up to 4, at least 16 K
+// blocks per split) that fills the last wave of the persistent grid best; a split must gain at
+// least 10 % of wave efficiency to pay for its partial-sum pass.
+int wave_splits(int64_t tiles, int64_t nkt) {
+    const int64_t nsm = sm_count();
+    auto eff = [&](int64_t s) {
+        const int64_t units = tiles * s;
+        return double(units) / double((units + nsm - 1) / nsm * nsm);
+    };
+    int best = 1;
+    double best_eff = eff(1);
+    for (int s = 2; s <= 4; s++) {
+        if (nkt / s < 16) break;
+        if (eff(s) > best_eff * 1.10) {
+            best = s;
+            best_eff = eff(s);
+        }
+    }
+    return best;
+}
+
 }  // namespace
 
 void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
@@ -609,11 +665,43 @@ void split_rows(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, 
 }
 
 void tc_gemm_f64(Exec &ex, const __nv_bfloat16 *A, int64_t Mp, const __nv_bfloat16 *B, int64_t Np, int64_t Kp,
-                 int64_t m, int64_t n, int64_t k_true, double alpha, double beta, double *C, int64_t ldc) {
+                 int64_t m, int64_t n, int64_t k_true, double alpha, double beta, double *C, int64_t ldc,
+                 int splits) {
     REQUIRE(Mp >= round_up(m, BM) && Np >= round_up(n, B_ROW_PAD), CCSD_GPU_EINVAL, "tc_gemm_f64: bad padding");
-    EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
-    launch_tc(ex, check_planes(ex.planes), A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi,
-              double(m) * double(n) * double(k_true));
+    const int np = check_planes(ex.planes);
+    const double mnk = double(m) * double(n) * double(k_true);
+    if (splits <= 0) splits = wave_splits(Mp / BM * (round_up(n, n_tile(np)) / n_tile(np)), Kp / BK);
+    splits = std::max(1, std::min<int>(splits, (int)(Kp / BK)));
+    if (splits == 1) {
+        EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
+        launch_tc(ex, np, A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi, mnk);
+        return;
+    }
+    DBuf part = dalloc((int64_t)splits * m * n, ex.stream);
+    EpiF64 epi{part.d(), (long long)m, (int)m, (int)n, alpha, 0.0, (long long)m * n};
+    launch_tc(ex, np, A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi, mnk, splits);
+    sum_splits_kernel<<<(unsigned)std::min<int64_t>((m * n + 255) / 256, 148 * 64), 256, 0, ex.stream>>>(
+        part.d(), splits, m, n, beta, C, ldc);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+void tc_gemm_ovvv(Exec &ex, const __nv_bfloat16 *Lov, int64_t ov_rows, const __nv_bfloat16 *Lvv, int64_t vv_rows,
+                  int64_t Kp, int64_t no, int64_t nv, __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld,
+                  int64_t k_true) {
+    REQUIRE(out_rows_pad >= no * nv && out_ld >= nv * nv && ov_rows >= no * nv && vv_rows >= nv * nv,
+            CCSD_GPU_EINVAL, "tc_gemm_ovvv: bad padding");
+    EpiOvvv epi{};
+    epi.out = out;
+    epi.plane = (size_t)out_rows_pad * (size_t)out_ld;
+    epi.ldk = out_ld;
+    epi.no = (int)no;
+    epi.nv = (int)nv;
+    epi.M = (int)(no * nv);
+    epi.N = (int)(nv * nv);
+    epi.np = check_planes(ex.planes);
+    launch_tc(ex, epi.np, Lov, ov_rows, ov_rows * Kp, epi.M, Lvv, vv_rows, vv_rows * Kp, epi.N, Kp, epi,
+              double(epi.M) * double(epi.N) * double(k_true));
 }
 
 void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,

@@ -22,9 +22,18 @@ void split_rows(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, 
                 __nv_bfloat16 *out);
 
 // Tensor-core GEMM on pre-split operands A [2][Mp][Kp], B [2][Np][Kp]:
-// C (m x n, col-major, FP64) = alpha A B^T + beta C.
+// C (m x n, col-major, FP64) = alpha A B^T + beta C.  splits > 1 divides K into that many
+// deterministic partial products summed afterwards; 0 chooses the count from the tile waves.
 void tc_gemm_f64(Exec &ex, const __nv_bfloat16 *A, int64_t Mp, const __nv_bfloat16 *B, int64_t Np, int64_t Kp,
-                 int64_t m, int64_t n, int64_t k_true, double alpha, double beta, double *C, int64_t ldc);
+                 int64_t m, int64_t n, int64_t k_true, double alpha, double beta, double *C, int64_t ldc,
+                 int splits = 1);
+
+// ovvv integrals g_kcbd = sum_J L_kc L_bd of the untransformed Cholesky vectors as split bf16:
+// Lov holds split rows c + nv*k (K = N_J padded to Kp), Lvv split rows d + nv*b; the result goes
+// to out[plane][k + no*b][c + nv*d] (row stride out_ld, plane stride out_rows_pad * out_ld).
+void tc_gemm_ovvv(Exec &ex, const __nv_bfloat16 *Lov, int64_t ov_rows, const __nv_bfloat16 *Lvv, int64_t vv_rows,
+                  int64_t Kp, int64_t no, int64_t nv, __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld,
+                  int64_t k_true);
 
 // A2 ladder integrals for a in [a0,a1).  L holds split rows r = c + nv*a (l_rows rows per plane,
 // K = N_J padded to Kp): M_ab[c,d] = sum_J L[c + nv a] L[d + nv b] for b < a1; pairs b <= a are

@@ -175,3 +175,41 @@ def test_mixed_jacobian_and_transpose_close_to_fp64():
     for k in range(2):
         ref, mix = out[FP64][k], out[MIXED][k]
         assert np.linalg.norm(mix - ref) <= 1e-4 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("dims", [(5, 19, 33), (6, 32, 70)])
+def test_mixed_singles_jacobian_with_t1_matches_fp64(dims):
+    """Singles trial vectors at amplitudes with sizeable t1: the ladder's t1 tangent takes Y from the
+    resident untransformed ovvv integrals plus the correction -sum_l t_bl Q_kilj for the
+    T1-transformed vv block.  The mixed result must agree with FP64 far more closely than the size
+    of that ladder term (a missing or wrong correction shows up at ~20 % of it)."""
+    from et_b200 import CCSD, FP64, MIXED
+    n_o, n_v, n_J = dims
+    s = make_system(n_o, n_v, n_J, seed=41)
+    ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
+    amp = 0.05 * np.random.default_rng(5).standard_normal(ref.n_amp)
+    amp[: ref.n_t1] *= 3.0
+    ref.set_amplitudes(amp)
+    C = np.zeros((ref.n_amp, 2))
+    C[: ref.n_t1] = np.random.default_rng(6).standard_normal((ref.n_t1, 2))
+    out = {}
+    for prec in (FP64, MIXED):
+        with CCSD(n_o, n_v, n_J, precision=prec, mixed_min_flops=1) as g:
+            g.set_system(s.L_mo, s.h_mo, s.eps)
+            g.set_amplitudes(amp)
+            out[prec] = (g.jacobian_transformation(C), g.jacobian_transpose_transformation(C))
+    # the ladder's t1 tangent, -sum_k c_ak Y_kibj with Y_kibj = sum_cd g_kc~bd t_cidj
+    o = n_o
+    Lt = ref.L_t1
+    g_ovvv = np.einsum("Jkc,Jbd->kcbd", Lt[:, :o, o:], Lt[:, o:, o:])
+    tf = oc.squareup(ref.t2, ref.n_v, ref.n_o)
+    Y = np.einsum("kcbd,cidj->kibj", g_ovvv, tf)
+    for k in range(2):
+        c1 = C[: ref.n_t1, k].reshape(n_v, n_o, order="F")
+        ladder_t1 = np.linalg.norm(np.einsum("ak,kibj->aibj", c1, Y))
+        for which in range(2):
+            r64, rmx = out[FP64][which][:, k], out[MIXED][which][:, k]
+            err = np.linalg.norm(rmx - r64)
+            assert err <= 1e-4 * np.linalg.norm(r64)
+            if which == 0:
+                assert err <= 1e-3 * ladder_t1, (err, ladder_t1)
