@@ -41,7 +41,7 @@ class CCSDGPUError(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("ladder_batch", ctypes.c_int64),
                 ("mixed_min_flops", ctypes.c_int64), ("mixed_k_chunk", ctypes.c_int64),
-                ("reserved", ctypes.c_int64 * 4)]
+                ("autotune", ctypes.c_int64), ("reserved", ctypes.c_int64 * 3)]
 
 
 class DavidsonOptions(ctypes.Structure):
@@ -148,7 +148,7 @@ class CCSD:
     """One Cholesky-factored closed-shell CCSD system resident on one GPU."""
 
     def __init__(self, n_o, n_v, n_J, *, precision=FP64, device=0, ladder_batch=0, mixed_min_flops=0,
-                 mixed_k_chunk=0):
+                 mixed_k_chunk=0, autotune=0):
         self.lib = load_library()
         self.n_o, self.n_v, self.n_J = int(n_o), int(n_v), int(n_J)
         self.n_mo = self.n_o + self.n_v
@@ -156,7 +156,7 @@ class CCSD:
         self.n_t2 = self.n_t1 * (self.n_t1 + 1) // 2
         self.n_amp = self.n_t1 + self.n_t2
         opt = Options(device=device, precision=precision, ladder_batch=ladder_batch,
-                      mixed_min_flops=mixed_min_flops, mixed_k_chunk=mixed_k_chunk)
+                      mixed_min_flops=mixed_min_flops, mixed_k_chunk=mixed_k_chunk, autotune=autotune)
         ctx = _VP()
         rc = self.lib.ccsd_gpu_create(self.n_o, self.n_v, self.n_J, ctypes.byref(opt), ctypes.byref(ctx))
         if rc != 0:
@@ -409,7 +409,7 @@ class CCSD:
 
 def solve_ground_states(systems, *, precision=FP64, device=0, workers=8, max_iterations=100, diis_dimension=8,
                         omega_threshold=1e-5, energy_threshold=1e-5, refine_threshold=1e-4, refine_target=0.0,
-                        mixed_min_flops=0, amplitudes=False):
+                        mixed_min_flops=0, autotune=0, amplitudes=False):
     """Ground states of independent systems on `workers` concurrent contexts (ccsd_gpu_solve_gs_batch).
 
     ``systems``: sequence of (L_mo[J, p, q], h_mo, eps, n_o, e_hf) host arrays and sizes.  Each system
@@ -422,7 +422,9 @@ def solve_ground_states(systems, *, precision=FP64, device=0, workers=8, max_ite
     for k, (L, h, eps, n_o, e_hf) in enumerate(systems):
         L = np.asarray(L, dtype=np.float64)
         n_J, n_mo = L.shape[0], L.shape[1]
-        flat = np.ascontiguousarray(L.reshape(-1, order="F"))          # (J, p, q), J fastest
+        flat = L.reshape(-1, order="F")                                   # (J, p, q), J fastest
+        if not flat.flags.c_contiguous:
+            flat = np.ascontiguousarray(flat)
         hf = np.ascontiguousarray(np.asarray(h, dtype=np.float64).reshape(-1, order="F"))
         ef = np.ascontiguousarray(np.asarray(eps, dtype=np.float64))
         keep += [flat, hf, ef]
@@ -434,7 +436,7 @@ def solve_ground_states(systems, *, precision=FP64, device=0, workers=8, max_ite
             t = np.zeros(n1 + n1 * (n1 + 1) // 2)
             t_outs.append(t)
             arr[k].t_out = _dp(t)
-    opt = Options(device=device, precision=precision, mixed_min_flops=mixed_min_flops)
+    opt = Options(device=device, precision=precision, mixed_min_flops=mixed_min_flops, autotune=autotune)
     sopt = SolverOptions(max_iterations=max_iterations, diis_dimension=diis_dimension,
                          omega_threshold=omega_threshold, energy_threshold=energy_threshold,
                          refine_threshold=refine_threshold, refine_target=refine_target)

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <memory>
 
+#include "autotune.cuh"
 #include "ccsd.cuh"
 #include "ccsd_kernels.cuh"
 #include "mixed_gemm.cuh"
@@ -48,6 +49,11 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     set_precision(opt ? opt->precision : CCSD_GPU_FP64);
     if (opt && opt->mixed_min_flops > 0) ex.mixed_min_flops = (double)opt->mixed_min_flops;
     if (opt && opt->mixed_k_chunk != 0) ex.k_chunk = opt->mixed_k_chunk;
+    {
+        const char *env = std::getenv("CCSD_GPU_AUTOTUNE");
+        const int64_t at = opt ? opt->autotune : 0;
+        ex.autotune = at > 0 || (at == 0 && !(opt && opt->mixed_min_flops > 0) && !(env && env[0] == '0'));
+    }
     ladder_batch = opt ? opt->ladder_batch : 0;
     cudaStream_t s = ex.stream;
     for (auto *b : {&L_oo, &Lt_oo}) *b = dalloc(nJ * no * no, s);
@@ -359,8 +365,8 @@ void Context::ladder_tc_apply(const double *t2, double *om2, int64_t nvec) {
     DBuf TS(sizeof(__nv_bfloat16) * ex.planes * rows_T * Kq, s);
     build_T(ex, t2, nvec, no, nv, rows_T, Kq, ex.planes, TS.as<__nv_bfloat16>());
     DBuf W = dalloc(nab * nvec * nrow, s);
-    tc_gemm_f64(ex, mbuf.as<__nv_bfloat16>(), mrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nab, nvec * nrow, nv2, 1.0,
-                0.0, W.d(), nab);
+    tc_gemm_f64_tuned(ex, mbuf.as<__nv_bfloat16>(), mrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nab, nvec * nrow, nv2,
+                      1.0, 0.0, W.d(), nab, 1);
     for (int64_t v = 0; v < nvec; v++) add_omega_T(ex, om2 + v * nt2, W.d() + v * nrow * nab, nab, no, nv);
     ex.flops += 2.0 * double(nab) * double(nvec * nrow) * double(nv2);
 }
@@ -443,8 +449,8 @@ void Context::ladder_y0(const double *tf, double *Y) {
     }
     // Yt[(k + no*b) + nov*(i + no*j)], then Y[k, i, b, j]
     DBuf Yt = dalloc(nov * oo, s);
-    tc_gemm_f64(ex, ybuf.as<__nv_bfloat16>(), yrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nov, oo, nv2, 1.0, 0.0,
-                Yt.d(), nov, 0);
+    tc_gemm_f64_tuned(ex, ybuf.as<__nv_bfloat16>(), yrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nov, oo, nv2, 1.0, 0.0,
+                      Yt.d(), nov, 0);
     TV src = tv(Yt.d(), {no, no, nv, no});   // (k, i, b, j)
     src.s[1] = nov;
     src.s[2] = no;

@@ -138,6 +138,7 @@ struct Exec {
     double mixed_min_flops = 2e9;
     int planes = 2;              // split-bf16 planes of a mixed GEMM: 2 = bf16x3, 3 = bf16x6
     int64_t k_chunk = 4096;      // K elements a tensor-core accumulator sums before FP64 takes over (<= 0: all)
+    bool autotune = false;       // mixed GEMM routes (DGEMM or tensor cores, K splits) from measurement
     double flops = 0.0;          // algorithmic flops issued (counted by contract())
     int64_t launches = 0;        // kernels of this library launched
     GemmProfile *prof = nullptr;

@@ -617,8 +617,36 @@ int wave_splits(int64_t tiles, int64_t nkt) {
 
 }  // namespace
 
+int tc_default_splits(int64_t m, int64_t n, int64_t k, int planes) {
+    // split K when the output tiles cannot fill the SMs: deterministic partial products, then a sum
+    const int64_t tiles = (round_up(m, BM) / BM) * (round_up(n, n_tile(planes)) / n_tile(planes));
+    const int64_t nkt = round_up(k, BK) / BK, nsm = sm_count();
+    if (!(tiles < nsm && nkt >= 16)) return 1;
+    const int64_t want = std::min<int64_t>((2 * nsm + tiles - 1) / tiles, nkt / 8);
+    const int64_t per = (nkt + want - 1) / want;
+    return (int)((nkt + per - 1) / per);
+}
+
+std::vector<int> tc_split_candidates(int64_t m, int64_t n, int64_t k, int planes) {
+    const int64_t tiles = (round_up(m, BM) / BM) * (round_up(n, n_tile(planes)) / n_tile(planes));
+    const int64_t nkt = round_up(k, BK) / BK, nsm = sm_count();
+    std::vector<int> out{1};
+    auto add = [&](int64_t s, int64_t min_blocks) {
+        if (s < 2 || s > 64 || nkt / s < min_blocks) return;
+        if (std::find(out.begin(), out.end(), (int)s) == out.end()) out.push_back((int)s);
+    };
+    add(tc_default_splits(m, n, k, planes), 1);
+    if (tiles >= nsm) {
+        for (int s = 2; s <= 4; s++) add(s, 16);
+    } else {
+        // counts whose units fill about j waves of the persistent grid
+        for (int j = 1; j <= 4; j++) add(j * nsm / tiles, 4);
+    }
+    return out;
+}
+
 void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
-                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc) {
+                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, int splits) {
     REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "mixed_gemm: size too large");
     const int np = check_planes(ex.planes);
     const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, B_ROW_PAD);
@@ -629,15 +657,8 @@ void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     // B operand rows are output columns: op(B)(kk, c) = B[kk + ldb c] (N) or B[c + ldb kk] (T)
     if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
     else split(ex, B, 1, ldb, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
-    // split K when the output tiles cannot fill the SMs: deterministic partial products, then a sum
-    const int64_t tiles = (Mp / BM) * (round_up(n, n_tile(np)) / n_tile(np)), nkt = Kp / BK;
-    const int64_t nsm = sm_count();
-    int splits = 1;
-    if (tiles < nsm && nkt >= 16) {
-        int64_t want = std::min<int64_t>((2 * nsm + tiles - 1) / tiles, nkt / 8);
-        int64_t per = (nkt + want - 1) / want;
-        splits = (int)((nkt + per - 1) / per);
-    }
+    if (splits <= 0) splits = tc_default_splits(m, n, k, np);
+    splits = std::max(1, std::min<int>(splits, (int)(Kp / BK)));
     const double mnk = double(m) * double(n) * double(k);
     if (splits <= 1) {
         EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};

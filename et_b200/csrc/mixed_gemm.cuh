@@ -3,14 +3,24 @@
 
 #include <cuda_bf16.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace ccsd {
 
 // C (m x n, col-major, ldc) = alpha op(A) op(B) + beta C with FP64 operands split into
 // bf16 hi + lo parts; the three products hi*hi + hi*lo + lo*hi accumulate in FP32.
+// splits: K-split count (<= 0: tc_default_splits).
 void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha,
-                const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc);
+                const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc,
+                int splits = -1);
+
+// K-split count of the fixed rule: split only when the output tiles cannot fill the SMs.
+int tc_default_splits(int64_t m, int64_t n, int64_t k, int planes);
+// K-split counts worth timing for an m x n x k product: 1, the fixed rule's count, and counts whose
+// tile units fill whole waves of the persistent grid.
+std::vector<int> tc_split_candidates(int64_t m, int64_t n, int64_t k, int planes);
 
 // Row / K padding of pre-split operands (A rows to 128, B rows to 256, K to 64).
 int64_t tc_pad_rows_a(int64_t m);

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <map>
 
+#include "autotune.cuh"
 #include "mixed_gemm.cuh"
 #include "tensor_ops.cuh"
 
@@ -169,14 +170,44 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
     if (m == 0 || n == 0) return;
     double fl = 2.0 * double(m) * double(n) * double(k);
     ex.flops += fl;
-    // the tensor-core tile is 128 x 256 x 64: skinny products stay on the FP64 pipe
-    const bool mixed = allow_mixed && ex.prec == Prec::MIXED && fl >= ex.mixed_min_flops && k >= 16 &&
-                       (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64));
+    const bool tc_ok = allow_mixed && ex.prec == Prec::MIXED && k >= 16;
+    // measured route (0 = DGEMM, s >= 1 = tensor cores with s K-splits) for products big enough to
+    // be worth timing; -1 = the fixed rule below
+    int route = -1;
+    if (tc_ok && ex.autotune) {
+        if (fl < 5e7 || m < 16 || n < 16) {
+            route = 0;
+        } else {
+            const std::string key = tune_key('g', m, n, k, transA, transB, ex);
+            route = tune_lookup(key);
+            if (route < 0) {
+                std::vector<int> routes;
+                if (fl <= 4e11) routes.push_back(0);   // larger products never favour FP64
+                for (int sp : tc_split_candidates(m, n, k, ex.planes)) routes.push_back(sp);
+                DBuf scratch = dalloc(m * n, ex.stream);
+                route = tune_measure(ex, key, routes, [&](int r) {
+                    if (r == 0) {
+                        const double zero = 0.0;
+                        BLAS_CHECK(cublasDgemm_64(ex.blas, transA ? CUBLAS_OP_T : CUBLAS_OP_N,
+                                                  transB ? CUBLAS_OP_T : CUBLAS_OP_N, m, n, k, &alpha, A, lda, B, ldb,
+                                                  &zero, scratch.d(), m));
+                    } else {
+                        mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, 0.0, scratch.d(), m, r);
+                    }
+                });
+            }
+        }
+    }
+    // fixed rule: the tensor-core tile is 128 x 256 x 64, so skinny products stay on the FP64 pipe
+    const bool mixed = route >= 0 ? route > 0
+                                  : tc_ok && fl >= ex.mixed_min_flops &&
+                                        (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64));
     if (trace_level() >= 2)
-        std::fprintf(stderr, "ccsd_gpu gemm [%s] %s m %lld n %lld k %lld  %.3g flop\n", g_perm_tag ? g_perm_tag : "direct",
-                     mixed ? "bf16x3" : "fp64", (long long)m, (long long)n, (long long)k, fl);
+        std::fprintf(stderr, "ccsd_gpu gemm [%s] %s m %lld n %lld k %lld  %.3g flop  splits %d\n",
+                     g_perm_tag ? g_perm_tag : "direct", mixed ? "bf16x3" : "fp64", (long long)m, (long long)n,
+                     (long long)k, fl, route);
     if (mixed) {
-        mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, route);
         return;
     }
     BLAS_CHECK(cublasDgemm_64(ex.blas, transA ? CUBLAS_OP_T : CUBLAS_OP_N, transB ? CUBLAS_OP_T : CUBLAS_OP_N, m,

@@ -48,7 +48,9 @@ DEFAULT_COUPLING = 0.15
 def make_system(n_o: int, n_v: int, n_J: int, seed: int = 2026, coupling: float = DEFAULT_COUPLING) -> System:
     rng = np.random.Generator(np.random.PCG64(seed))
     n_mo = n_o + n_v
-    L = np.empty((n_J, n_mo, n_mo), dtype=np.float64)
+    # eT's layout of the MO Cholesky vectors, L(J, pq) with J fastest (Fortran order), so that the
+    # host arrays go to the library without a reordering copy
+    L = np.empty((n_J, n_mo, n_mo), dtype=np.float64, order="F")
     scale = coupling / np.sqrt(n_o + n_v)
     for J in range(n_J):
         X = rng.standard_normal((n_mo, n_mo)) * scale

@@ -60,7 +60,11 @@ typedef struct ccsd_gpu_options {
     int64_t mixed_min_flops;     /* contractions below this many flops stay FP64 (0 = default) */
     int64_t mixed_k_chunk;       /* K elements a tensor-core FP32 accumulator sums before the partial
                                     sum is added in FP64 (0 = default 4096, negative = the whole K) */
-    int64_t reserved[4];
+    int64_t autotune;            /* MIXED only: route of each GEMM shape (FP64 DGEMM or tensor cores,
+                                    K-split count) timed once per process: 1 on, -1 off (fixed flop
+                                    threshold and split rule), 0 = on unless mixed_min_flops is given
+                                    or the environment sets CCSD_GPU_AUTOTUNE=0 */
+    int64_t reserved[3];
 } ccsd_gpu_options;
 
 typedef struct ccsd_gpu_solver_options {
