@@ -101,6 +101,8 @@ SIGNATURES = {
     "ccsd_gpu_solve_gs": (ctypes.c_int, [_VP, ctypes.POINTER(SolverOptions), _DP,
                                          ctypes.POINTER(ctypes.c_int32), _DP]),
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
+    "ccsd_gpu_set_graphs": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "ccsd_gpu_graph_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     "ccsd_gpu_set_profiling": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_gemm_profile": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP, _DP]),
     "ccsd_gpu_selftest_gemm": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I64, _I64,
@@ -368,6 +370,16 @@ class CCSD:
         if rc != 0 and (raise_on_failure or rc != -5):
             self._check(rc)
         return e.value, it.value, hist[: 2 * it.value].reshape(-1, 2), rc
+
+    def set_graphs(self, on: bool):
+        """Residual evaluations as captured CUDA graphs (off by default; CCSD_GPU_GRAPHS=1)."""
+        self._check(self.lib.ccsd_gpu_set_graphs(self.ctx, 1 if on else 0))
+
+    def graph_stats(self):
+        """(residual evaluations served by a graph launch, GEMM routes held by the process)."""
+        r, n = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.ccsd_gpu_graph_stats(self.ctx, ctypes.byref(r), ctypes.byref(n)))
+        return int(r.value), int(n.value)
 
     def stats(self):
         """(kernel launches of this library, GEMM flops issued) since creation."""

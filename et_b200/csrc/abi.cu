@@ -3,6 +3,7 @@
 #include <cstring>
 #include <new>
 
+#include "autotune.cuh"
 #include "ccsd.cuh"
 #include "mixed_gemm.cuh"
 #include "ccsd_kernels.cuh"
@@ -313,6 +314,22 @@ int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops) {
     return guarded(ctx, [&](Context &c) {
         if (kernel_launches) *kernel_launches = c.ex.launches;
         if (gemm_flops) *gemm_flops = c.ex.flops;
+    });
+}
+
+int ccsd_gpu_set_graphs(void *ctx, int32_t on) {
+    return guarded(ctx, [&](Context &c) {
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        c.use_graphs = on != 0;
+        if (!c.use_graphs)
+            for (auto &G : c.rgraph) G.reset();
+    });
+}
+
+int ccsd_gpu_graph_stats(void *ctx, int64_t *residual_replays, int64_t *tuned_routes) {
+    return guarded(ctx, [&](Context &c) {
+        if (residual_replays) *residual_replays = c.graph_replays;
+        if (tuned_routes) *tuned_routes = ccsd::tune_entries();
     });
 }
 

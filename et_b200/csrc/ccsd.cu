@@ -44,6 +44,15 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     CU_CHECK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     BLAS_CHECK(cublasCreate(&blas));
     set_stream(nullptr);
+    {
+        // cuBLAS works in a buffer it is given, so its calls can be captured into a graph
+        const size_t ws = size_t(32) << 20;
+        blas_ws = DBuf(ws, own_stream);
+        CU_CHECK(cudaStreamSynchronize(own_stream));
+        BLAS_CHECK(cublasSetWorkspace(blas, blas_ws.as<void>(), ws));
+        const char *g = std::getenv("CCSD_GPU_GRAPHS");
+        use_graphs = g && g[0] == '1';
+    }
     ex.blas = blas;
     ex.prof = &prof;
     set_precision(opt ? opt->precision : CCSD_GPU_FP64);
@@ -78,9 +87,15 @@ Context::~Context() {
     if (own_stream) cudaStreamSynchronize(own_stream);
     if (ex.stream && ex.stream != own_stream) cudaStreamSynchronize(ex.stream);
     // every device buffer is freed (stream-ordered) while its stream still exists
+    for (auto &G : rgraph) G.reset();
+    if (ex.stream) cudaStreamSynchronize(ex.stream);
+    if (graphs_captured) cudaDeviceGraphMemTrim(device);   // the physical memory the residual graphs held
     for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
-                    &mbuf, &ybuf, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
+                    &mbuf, &ybuf, &om_stage, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
         b->release();
+    if (blas) cublasDestroy(blas);
+    blas = nullptr;
+    blas_ws.release();
     mbuf_bytes = 0;
     ybuf_bytes = 0;
     if (ex.stream) cudaStreamSynchronize(ex.stream);
@@ -202,6 +217,7 @@ const double *Context::g_ovov_const() {
         gov = g_ovov();
         ex.prec = keep;
         have_gov = true;
+        cache_epoch++;
     }
     return gov.d();
 }
@@ -354,6 +370,7 @@ void Context::ladder_pairs(const double *Lvv, bool untransformed) {
     mbuf_kind = untransformed ? 1 : 2;
     mbuf_version = l_version;
     mbuf_planes = np;
+    cache_epoch++;
 }
 
 // om2[v] += ladder(pair integrals in mbuf, t2[v]) for nvec packed vectors
@@ -384,9 +401,14 @@ void Context::ladder_tc(const double *Lvv, const double *t2, double *om2, int64_
 bool Context::ovvv_resident() {
     const size_t need = sizeof(__nv_bfloat16) * (size_t)ex.planes * (size_t)tc_pad_rows_a(nov) * tc_pad_k(nv * nv);
     if (ybuf_bytes >= need) return true;
-    size_t free_b = 0, total_b = 0;
-    CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
-    return need < free_b / 4;
+    if (ybuf_fit < 0 || ybuf_fit_version != l_version || ybuf_fit_planes != ex.planes) {
+        size_t free_b = 0, total_b = 0;
+        CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
+        ybuf_fit = need < free_b / 4 ? 1 : 0;
+        ybuf_fit_version = l_version;
+        ybuf_fit_planes = ex.planes;
+    }
+    return ybuf_fit == 1;
 }
 
 void Context::ovvv_pairs() {
@@ -429,6 +451,7 @@ void Context::ovvv_pairs() {
                  ybuf.as<__nv_bfloat16>(), yrows, Kq, nJ);
     ybuf_version = l_version;
     ybuf_planes = np;
+    cache_epoch++;
 }
 
 void Context::ladder_y0(const double *tf, double *Y) {

@@ -50,6 +50,34 @@ struct Context {
     size_t ybuf_bytes = 0;
     int ybuf_planes = 0;
     int64_t ybuf_version = -1;
+    int ybuf_fit = -1;              // residency decision for (ybuf_fit_version, ybuf_fit_planes)
+    int64_t ybuf_fit_version = -1;
+    int ybuf_fit_planes = 0;
+    // bumped whenever a resident cache (g_iajb, ladder pair integrals, ovvv planes) is (re)built, so
+    // a captured residual that points into the old one is not replayed
+    int64_t cache_epoch = 0;
+    DBuf blas_ws;                   // cuBLAS workspace (no allocation inside stream capture)
+
+    // The residual evaluation captured as a CUDA graph, one per precision.  The first evaluation in
+    // a precision runs eagerly (it builds the caches and times the GEMM routes); later ones replay
+    // a graph captured for the same Cholesky set, caches and GEMM settings, which writes om_stage.
+    struct ResidualGraph {
+        cudaGraphExec_t exec = nullptr;
+        bool warm = false;
+        int64_t l_version = -1, cache_epoch = -1, k_chunk = 0;
+        int planes = 0;
+        int64_t launches = 0;
+        double flops = 0.0;
+        void reset() {
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+    };
+    ResidualGraph rgraph[2];        // [0] FP64, [1] MIXED
+    DBuf om_stage;                  // the residual graphs' output
+    bool use_graphs = false;        // ccsd_gpu_set_graphs or CCSD_GPU_GRAPHS=1 turns capture on
+    int64_t graph_replays = 0;      // residual evaluations served by a graph launch
+    bool graphs_captured = false;
 
     Context(int64_t no, int64_t nv, int64_t nJ, const ccsd_gpu_options *opt);
     ~Context();
@@ -66,6 +94,9 @@ struct Context {
     double energy();
     void mp2_guess();
     void omega(double *d_omega);
+    void omega_eager(double *d_omega);       // record + evaluate the residual on ex.stream
+    void prepare_residual_caches();          // builds what a captured residual only reads
+    void capture_residual(ResidualGraph &G, double *d_omega);
     // const_ovov: take g_iajb from the cache (no derivative flows into L_ov through it)
     OmegaNodes record_omega(Graph &g, bool const_ovov = true);
     void record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv_in, int tf);

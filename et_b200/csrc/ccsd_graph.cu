@@ -2,6 +2,8 @@
 // it: rho = A c = (dOmega/dt) D c (forward mode) and sigma = b^T A = D (dOmega/dt)^T b (reverse
 // mode), D = 2 on the packed doubles diagonal (jacobian_ccsd.F90:74-176).  Every term restates
 // the routine of the eT file cited beside it.
+#include <cstdio>
+#include <cstdlib>
 #include <memory>
 
 #include "ccsd.cuh"
@@ -305,12 +307,90 @@ void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv
     g.custom(std::move(op), om2, {Lvv, t2, t1, tf});
 }
 
-void Context::omega(double *om_out) {
-    REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+void Context::omega_eager(double *om_out) {
     Graph g(ex);
     OmegaNodes n = record_omega(g);
     CU_CHECK(cudaMemcpyAsync(om_out, g.value(n.om1), sizeof(double) * nt1, cudaMemcpyDeviceToDevice, ex.stream));
     CU_CHECK(cudaMemcpyAsync(om_out + nt1, g.value(n.om2), sizeof(double) * nt2, cudaMemcpyDeviceToDevice, ex.stream));
+}
+
+void Context::prepare_residual_caches() {
+    g_ovov_const();
+    if (ex.prec == Prec::MIXED) {
+        ladder_pairs(L_vv.d(), true);
+        if (ovvv_resident()) ovvv_pairs();
+    }
+}
+
+// Records the residual on ex.stream into G.  A capture that fails (a call that cannot be captured)
+// leaves G empty and turns graphs off for this context; the caller then evaluates eagerly.
+void Context::capture_residual(ResidualGraph &G, double *om_out) {
+    G.reset();
+    graphs_captured = true;
+    const double flops0 = ex.flops;
+    const int64_t launches0 = ex.launches;
+    cudaGraph_t graph = nullptr;
+    std::string why;
+    CU_CHECK(cudaStreamBeginCapture(ex.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        omega_eager(om_out);
+    } catch (const std::exception &e) {
+        why = e.what();
+    }
+    cudaError_t rc = cudaStreamEndCapture(ex.stream, &graph);
+    if (why.empty() && rc == cudaSuccess && graph) {
+        rc = cudaGraphInstantiate(&G.exec, graph, 0);
+        if (rc != cudaSuccess) G.exec = nullptr;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (!G.exec) {
+        if (why.empty()) why = cudaGetErrorString(rc);
+        cudaGetLastError();
+        use_graphs = false;
+        if (std::getenv("CCSD_GPU_TRACE"))
+            std::fprintf(stderr, "ccsd_gpu residual graph capture failed (%s); evaluating eagerly\n", why.c_str());
+    }
+    G.flops = ex.flops - flops0;
+    G.launches = ex.launches - launches0;
+    ex.flops = flops0;
+    ex.launches = launches0;
+    G.l_version = l_version;
+    G.cache_epoch = cache_epoch;
+    G.planes = ex.planes;
+    G.k_chunk = ex.k_chunk;
+}
+
+void Context::omega(double *om_out) {
+    REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CU_CHECK(cudaStreamIsCapturing(ex.stream, &cap));
+    const bool graphs = use_graphs && !(ex.prof && ex.prof->on) && cap == cudaStreamCaptureStatusNone;
+    if (!graphs) {
+        omega_eager(om_out);
+    } else {
+        prepare_residual_caches();
+        ResidualGraph &G = rgraph[ex.prec == Prec::MIXED ? 1 : 0];
+        if (!G.warm) {
+            omega_eager(om_out);
+            G.warm = true;
+        } else {
+            // the graph writes a buffer of its own, so callers may pass any output
+            if (!om_stage) om_stage = dalloc(namp, ex.stream);
+            const bool match = G.exec && G.l_version == l_version && G.cache_epoch == cache_epoch &&
+                               G.planes == ex.planes && G.k_chunk == ex.k_chunk;
+            if (!match) capture_residual(G, om_stage.d());
+            if (G.exec) {
+                CU_CHECK(cudaGraphLaunch(G.exec, ex.stream));
+                CU_CHECK(cudaMemcpyAsync(om_out, om_stage.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice,
+                                         ex.stream));
+                ex.flops += G.flops;
+                ex.launches += G.launches;
+                graph_replays++;
+            } else {
+                omega_eager(om_out);
+            }
+        }
+    }
     if (ex.prec == Prec::MIXED) {
         CU_CHECK(cudaStreamSynchronize(ex.stream));
         REQUIRE(mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM barrier wait timed out");

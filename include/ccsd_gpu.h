@@ -188,6 +188,18 @@ int ccsd_gpu_solve_gs(void *ctx, const ccsd_gpu_solver_options *opt, double *ene
 /* Counters since creation: kernels of this library launched and GEMM flops issued. */
 int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops);
 
+/* Residual evaluations (construct_omega and the solver's) as CUDA graphs: the first evaluation in a
+ * precision runs eagerly, later ones replay a graph captured for the same Cholesky vectors, caches
+ * and GEMM settings.  Off by default (on when the environment sets CCSD_GPU_GRAPHS=1): capture,
+ * instantiation and the graph's own memory cost 5-50 ms per context on a B200, which a solve of
+ * 5-16 iterations does not win back except for the smallest systems.  Switching off releases the
+ * captured graphs.  No counterpart in eT, which calls BLAS per contraction. */
+int ccsd_gpu_set_graphs(void *ctx, int32_t on);
+
+/* Residual evaluations served by a graph launch since creation, and the number of GEMM routes the
+ * process holds (timed, or loaded from CCSD_GPU_TUNE_FILE). */
+int ccsd_gpu_graph_stats(void *ctx, int64_t *residual_replays, int64_t *tuned_routes);
+
 /* Kernel timing: when enabled, every tensor-core GEMM launch is bracketed by CUDA events on the
  * context's stream.  ccsd_gpu_gemm_profile returns the launches recorded since it was enabled,
  * their summed device time (ms) and the tensor flops they issued (3 products x 2mnk). */
