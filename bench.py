@@ -159,10 +159,14 @@ def gemm_traffic(n_o, n_v, n_J):
     return None
 
 
-def converged_solve(gpu, stream, refine, thr=1e-9, ethr=1e-11):
+def converged_solve(gpu, stream, refine, thr=1e-9, ethr=1e-11, L=None):
     """From the MP2 start to |Omega| < thr and |dE| < ethr between iterations (certified by an FP64
-    evaluation in mixed precision): (seconds by CUDA events, iterations, energy, converged)."""
+    evaluation in mixed precision): (seconds by CUDA events, iterations, energy, converged).  With L
+    the Cholesky vectors are set again first (untimed), so every integral kept on the device for a
+    Cholesky set is formed inside the timed solve, as in a calculation that solves once."""
     import torch
+    if L is not None:
+        gpu.set_cholesky_mo(L)
     gpu.set_initial_amplitudes_guess()
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -222,6 +226,14 @@ def run_gpu(args):
     gpu.set_system(sysd.L_mo, sysd.h_mo, sysd.eps, sysd.e_hf)
     flops_iter, flops_omega = iteration_flops(n_o, n_v, n_J)
 
+    # the integrals kept for a Cholesky set (ladder pairs and ovvv planes in split bf16, and the FP64
+    # ones of the refinement evaluations) are formed at set-up, outside the timed window; the solves to
+    # a threshold below form them inside their timed region
+    if prec == MIXED:
+        gpu.set_precision(FP64)
+        gpu.set_initial_amplitudes_guess()
+        gpu.construct_omega()
+        gpu.set_precision(MIXED)
     # warm-up iterations, then exactly K timed iterations from the MP2 start
     timed_solve(gpu, stream, args.warmup, args.refine, world)
     launches0, _ = gpu.stats()
@@ -285,18 +297,39 @@ def run_gpu(args):
         # by an FP64 evaluation).  The reference energy is the tightly converged FP64 one; the target
         # thresholds (|Omega| < 1e-6, |dE| < 1e-8 between iterations) are those that put both paths
         # within 1e-8 Eh of it; the tight ones (1e-9, 1e-11) are reported beside them.
+        # Two FP64 paths: eT's algorithm (the T1-transformed ladder integrals formed in every call,
+        # omega_ccsd_a2) and the same residual from FP64 integrals of the untransformed vectors kept
+        # for the Cholesky set (the algorithm of the mixed path's ladder, in FP64).  Solves to a
+        # threshold set the Cholesky vectors again first, so integrals kept for a Cholesky set are
+        # formed inside their timed region.
+        L = sysd.L_mo
         gpu.set_precision(FP64)
+        gpu.set_fp64_integrals(False)
         ms64, _, it64, _, _ = timed_solve(gpu, stream, 3, args.refine, world)
         s64 = ms64 / 1e3 / it64
         t64, n64, e_ref, ok64 = converged_solve(gpu, stream, args.refine, 1e-9, 1e-11)
         t64b, n64b, e64b, ok64b = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8)
+        gpu.set_fp64_integrals(True)
+        gpu.construct_omega()              # forms the resident integrals before the per-iteration timing
+        ms64r, _, it64r, _, _ = timed_solve(gpu, stream, 3, args.refine, world)
+        s64r = ms64r / 1e3 / it64r
+        t64r, n64r, e64r, ok64r = converged_solve(gpu, stream, args.refine, 1e-9, 1e-11, L=L)
+        t64rb, n64rb, e64rb, ok64rb = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8, L=L)
         gpu.set_precision(MIXED)
-        tmb, itmb, emb, okmb = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8)
-        tm, itm, em, okm = converged_solve(gpu, stream, args.refine, 1e-9, 1e-11)
-        result["fp64_path"] = {"s_per_iter": round(s64, 5), "energy": e_ref, "converged": ok64,
+        tmb, itmb, emb, okmb = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8, L=L)
+        tm, itm, em, okm = converged_solve(gpu, stream, args.refine, 1e-9, 1e-11, L=L)
+        result["fp64_path"] = {"algorithm": "T1-transformed ladder integrals formed in every call (eT)",
+                               "s_per_iter": round(s64, 5), "energy": e_ref, "converged": ok64,
                                "to_1e-9": {"s": round(t64, 3), "iterations": n64},
                                "to_target": {"s": round(t64b, 3), "iterations": n64b, "converged": ok64b,
                                              "dE": abs(e64b - e_ref)}}
+        result["fp64_resident_path"] = {"algorithm": "integrals of the untransformed vectors kept per Cholesky set "
+                                                     "+ T1 corrections (the mixed path's algorithm in FP64)",
+                                        "s_per_iter": round(s64r, 5), "converged": ok64r,
+                                        "dE_vs_fp64": abs(e64r - e_ref),
+                                        "to_1e-9": {"s": round(t64r, 3), "iterations": n64r},
+                                        "to_target": {"s": round(t64rb, 3), "iterations": n64rb,
+                                                      "converged": ok64rb, "dE": abs(e64rb - e_ref)}}
         result["mixed_path"] = {"to_1e-9": {"s": round(tm, 3), "iterations": itm, "converged": okm,
                                             "dE": abs(em - e_ref)},
                                 "to_target": {"s": round(tmb, 3), "iterations": itmb, "converged": okmb,
@@ -305,6 +338,9 @@ def run_gpu(args):
         result["speedup_per_iter_vs_fp64"] = round(s64 / (ms_step / 1e3), 3)
         result["speedup_to_target_vs_fp64"] = round(t64b / tmb, 3)
         result["speedup_to_1e-9_vs_fp64"] = round(t64 / tm, 3)
+        result["speedup_per_iter_vs_fp64_resident"] = round(s64r / (ms_step / 1e3), 3)
+        result["speedup_to_target_vs_fp64_resident"] = round(t64rb / tmb, 3)
+        result["speedup_to_1e-9_vs_fp64_resident"] = round(t64r / tm, 3)
         result["dE_vs_fp64"] = abs(emb - e_ref)
         result["dE_window_vs_fp64"] = abs(e - e_ref)
     gpu.close()

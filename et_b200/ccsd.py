@@ -102,6 +102,7 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_int32), _DP]),
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
     "ccsd_gpu_set_graphs": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "ccsd_gpu_set_fp64_integrals": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_graph_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     "ccsd_gpu_set_profiling": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_gemm_profile": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP, _DP]),
@@ -374,6 +375,11 @@ class CCSD:
     def set_graphs(self, on: bool):
         """Residual evaluations as captured CUDA graphs (off by default; CCSD_GPU_GRAPHS=1)."""
         self._check(self.lib.ccsd_gpu_set_graphs(self.ctx, 1 if on else 0))
+
+    def set_fp64_integrals(self, resident: bool):
+        """FP64 residual from resident integrals of the untransformed vectors (default, when they
+        fit) or from T1-transformed integrals formed in every call (eT's omega_ccsd_a2)."""
+        self._check(self.lib.ccsd_gpu_set_fp64_integrals(self.ctx, 1 if resident else 0))
 
     def graph_stats(self):
         """(residual evaluations served by a graph launch, GEMM routes held by the process)."""

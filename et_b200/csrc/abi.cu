@@ -326,6 +326,20 @@ int ccsd_gpu_set_graphs(void *ctx, int32_t on) {
     });
 }
 
+int ccsd_gpu_set_fp64_integrals(void *ctx, int32_t resident) {
+    return guarded(ctx, [&](Context &c) {
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        c.f64_resident_on = resident != 0;
+        if (!c.f64_resident_on) {
+            c.f64_gp.release();
+            c.f64_gm.release();
+            c.f64_ovvv.release();
+            c.f64_version = -1;
+            c.cache_epoch++;
+        }
+    });
+}
+
 int ccsd_gpu_graph_stats(void *ctx, int64_t *residual_replays, int64_t *tuned_routes) {
     return guarded(ctx, [&](Context &c) {
         if (residual_replays) *residual_replays = c.graph_replays;

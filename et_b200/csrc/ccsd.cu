@@ -52,6 +52,8 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
         BLAS_CHECK(cublasSetWorkspace(blas, blas_ws.as<void>(), ws));
         const char *g = std::getenv("CCSD_GPU_GRAPHS");
         use_graphs = g && g[0] == '1';
+        const char *r = std::getenv("CCSD_GPU_FP64_RESIDENT");
+        f64_resident_on = !(r && r[0] == '0');
     }
     ex.blas = blas;
     ex.prof = &prof;
@@ -91,7 +93,7 @@ Context::~Context() {
     if (ex.stream) cudaStreamSynchronize(ex.stream);
     if (graphs_captured) cudaDeviceGraphMemTrim(device);   // the physical memory the residual graphs held
     for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
-                    &mbuf, &ybuf, &om_stage, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
+                    &mbuf, &ybuf, &om_stage, &f64_gp, &f64_gm, &f64_ovvv, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
         b->release();
     if (blas) cublasDestroy(blas);
     blas = nullptr;
@@ -482,11 +484,16 @@ void Context::ladder_y0(const double *tf, double *Y) {
 }
 
 void Context::ladder_y_t1(const double *t1, const double *Ltvv, const double *tf, double *Y) {
-    if (!(ex.prec == Prec::MIXED && ovvv_resident())) {
+    if (ex.prec == Prec::MIXED && ovvv_resident()) {
+        ladder_y0(tf, Y);
+    } else if (ex.prec != Prec::MIXED && f64_resident()) {
+        f64_integrals();
+        contract(ex, "kbcd,cidj->kibj", 1.0, tv(f64_ovvv.d(), {no, nv, nv, nv}), tv(tf, {nv, no, nv, no}), 0.0,
+                 tv(Y, {no, no, nv, no}));
+    } else {
         ladder_y(Ltvv, tf, Y);
         return;
     }
-    ladder_y0(tf, Y);
     // L~_bd = L_bd - sum_l t_bl L_ld, so g_kc~bd = g_kcbd - sum_l t_bl g_kcld
     DBuf Q = dalloc(no * no * no * no, ex.stream);
     contract(ex, "kcld,cidj->kilj", 1.0, tv(g_ovov_const(), {no, nv, no, nv}), tv(tf, {nv, no, nv, no}), 0.0,
@@ -510,8 +517,13 @@ void Context::ladder_residual_mixed(const double *t1, const double *tf, const do
     DBuf Y = dalloc(no * no * nv * no, s);
     if (ovvv_resident()) ladder_y0(tf, Y.d());
     else ladder_y(L_vv.d(), tf, Y.d());
+    ladder_t1_corrections(t1, tf, Y.d(), om2);
+}
+
+void Context::ladder_t1_corrections(const double *t1, const double *tf, const double *Y0, double *om2) {
+    cudaStream_t s = ex.stream;
     DBuf S = dalloc(nov * nov, s), A = dalloc(nov * nov, s);
-    contract(ex, "ak,kibj->aibj", -1.0, tv(t1, {nv, no}), tv(Y.d(), {no, no, nv, no}), 0.0,
+    contract(ex, "ak,kibj->aibj", -1.0, tv(t1, {nv, no}), tv(Y0, {no, no, nv, no}), 0.0,
              tv(A.d(), {nv, no, nv, no}));
     permute_add(ex, 1.0, tv(A.d(), {nv, no, nv, no}), 0.0, tv(S.d(), {nv, no, nv, no}));
     TV At = tv(A.d(), {nv, no, nv, no});
@@ -528,6 +540,86 @@ void Context::ladder_residual_mixed(const double *t1, const double *tf, const do
                  tv(S.d(), {nv, no, nv, no}));
     }
     pack_half_diag_add(ex, 1.0, S.d(), om2, nov);
+}
+
+// FP64 integrals of the untransformed vectors, resident while they fit in half of the free memory
+// (50 GB at o = 32, v = 320): the +/- ladder integrals of all pairs (eT's packing, formed block by
+// block exactly as the per-call ladder forms them) and g_kcbd.
+bool Context::f64_resident() {
+    if (!f64_resident_on) return false;
+    if (f64_version == l_version) return true;
+    const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
+    // buffers of this shape already held (integrals of earlier Cholesky vectors) are reused
+    if (f64_gp.bytes() == sizeof(double) * nvp * nvp && f64_ovvv.bytes() == sizeof(double) * nov * nv * nv)
+        return true;
+    if (f64_fit < 0 || f64_fit_version != l_version) {
+        const double need = 8.0 * (double(nvp) * nvp + double(nvm) * nvm + double(nov) * nv * nv);
+        size_t free_b = 0, total_b = 0;
+        CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
+        f64_fit = need < 0.5 * double(free_b) ? 1 : 0;
+        f64_fit_version = l_version;
+    }
+    return f64_fit == 1;
+}
+
+void Context::f64_integrals() {
+    if (f64_version == l_version) return;
+    cudaStream_t s = ex.stream;
+    const Prec keep = ex.prec;
+    ex.prec = Prec::FP64;
+    const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
+    auto hold = [&](DBuf &b, int64_t n) {
+        if (b.bytes() == sizeof(double) * (size_t)n) return;
+        b = DBuf();
+        b = dalloc(n, s);
+    };
+    hold(f64_gp, nvp * nvp);
+    hold(f64_gm, std::max<int64_t>(nvm * nvm, 1));
+    hold(f64_ovvv, nov * nv * nv);
+    {
+        // L_vv as (J, c, a): columns (c, a) of one a-block are contiguous
+        DBuf LT = dalloc(nJ * nv * nv, s);
+        TV dst = tv(LT.d(), {nJ, nv, nv});
+        dst.s[1] = nJ * nv;
+        dst.s[2] = nJ;
+        permute_add(ex, 1.0, tv(L_vv.d(), {nJ, nv, nv}), 0.0, dst);
+        const int64_t nA = std::max<int64_t>(1, std::min<int64_t>(nv, (int64_t)(4.0e9 / (8.0 * nv * nv * nv))));
+        DBuf G = dalloc(nv * nA * nv * nv, s);
+        for (int64_t a0 = 0; a0 < nv; a0 += nA) {
+            const int64_t a1 = std::min(nv, a0 + nA), M = nv * (a1 - a0), N = nv * a1;
+            gemm(ex, true, false, M, N, nJ, 1.0, LT.d() + nJ * nv * a0, nJ, LT.d(), nJ, 0.0, G.d(), M);
+            form_gpm(ex, G.d(), M, f64_gp.d() + nvp * (a0 * (a0 + 1) / 2),
+                     f64_gm.d() + nvm * std::max<int64_t>(a0 * (a0 - 1) / 2, 0), nv, a0, a1);
+        }
+    }
+    // g_kcbd as [k, b, c, d]
+    contract(ex, "Jkc,Jbd->kbcd", 1.0, tv(L_ov.d(), {nJ, no, nv}), tv(L_vv.d(), {nJ, nv, nv}), 0.0,
+             tv(f64_ovvv.d(), {no, nv, nv, nv}));
+    ex.prec = keep;
+    f64_version = l_version;
+    cache_epoch++;
+}
+
+void Context::ladder_residual_f64(const double *t1, const double *tf, const double *t2, double *om2) {
+    f64_integrals();
+    cudaStream_t s = ex.stream;
+    const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
+    const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
+    const int64_t ldm = std::max<int64_t>(nom, 1);
+    // X0 = sum_cd g_acbd t_cidj of the untransformed integrals, all pairs in two GEMMs
+    {
+        DBuf tp = dalloc(nop * nvp, s), tm = dalloc(ldm * std::max<int64_t>(nvm, 1), s);
+        build_tpm(ex, t2, tp.d(), tm.d(), no, nv, nop, ldm);
+        DBuf wp = dalloc(nop * nvp, s), wm = dalloc(ldm * std::max<int64_t>(nvm, 1), s);
+        gemm(ex, false, false, nop, nvp, nvp, 0.5, tp.d(), nop, f64_gp.d(), nvp, 0.0, wp.d(), nop, false);
+        if (nom > 0 && nvm > 0)
+            gemm(ex, false, false, nom, nvm, nvm, 0.5, tm.d(), ldm, f64_gm.d(), nvm, 0.0, wm.d(), ldm, false);
+        add_omega_pm(ex, om2, wp.d(), wm.d(), no, nv, 0, nv, nop, ldm);
+    }
+    DBuf Y = dalloc(no * no * nv * no, s);
+    contract(ex, "kbcd,cidj->kibj", 1.0, tv(f64_ovvv.d(), {no, nv, nv, nv}), tv(tf, {nv, no, nv, no}), 0.0,
+             tv(Y.d(), {no, no, nv, no}));
+    ladder_t1_corrections(t1, tf, Y.d(), om2);
 }
 
 // ---------------------------------------------------------------------------

@@ -53,6 +53,14 @@ struct Context {
     int ybuf_fit = -1;              // residency decision for (ybuf_fit_version, ybuf_fit_planes)
     int64_t ybuf_fit_version = -1;
     int ybuf_fit_planes = 0;
+    // FP64 residual with resident integrals of the untransformed vectors (when they fit): eT's +/-
+    // ladder integrals g+ [v(v+1)/2 x v(v+1)/2] and g- [v(v-1)/2 x v(v-1)/2] for all pairs, and the
+    // ovvv block g_kcbd as [k, b, c, d]; valid for f64_version
+    DBuf f64_gp, f64_gm, f64_ovvv;
+    int64_t f64_version = -1;
+    int f64_fit = -1;               // residency decision for f64_fit_version
+    int64_t f64_fit_version = -1;
+    bool f64_resident_on = true;    // CCSD_GPU_FP64_RESIDENT=0 keeps eT's per-call integrals
     // bumped whenever a resident cache (g_iajb, ladder pair integrals, ovvv planes) is (re)built, so
     // a captured residual that points into the old one is not replayed
     int64_t cache_epoch = 0;
@@ -121,6 +129,12 @@ struct Context {
     void ladder_tc_apply(const double *t2, double *om2, int64_t nvec);
     // the residual's ladder in mixed precision from untransformed integrals plus t1 corrections
     void ladder_residual_mixed(const double *t1, const double *tf, const double *t2, double *om2);
+    // om2 += pack(-(A + A^T) + T4) with A_aibj = sum_k t_ak Y0_kibj, T4 = sum_kl t_ak t_bl Q_kilj
+    void ladder_t1_corrections(const double *t1, const double *tf, const double *Y0, double *om2);
+    // the same ladder in FP64 from resident FP64 integrals (f64_resident() must hold)
+    bool f64_resident();
+    void f64_integrals();
+    void ladder_residual_f64(const double *t1, const double *tf, const double *t2, double *om2);
     int davidson(int nstates, int side, const ccsd_gpu_davidson_options *o, double *omega_out, double *vectors_out,
                  int32_t *iters_out, const double *start = nullptr);
     void eta(double *out);

@@ -243,6 +243,8 @@ void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv
     op.forward = [this, &g, om2, Lvv, t2, t1, tf]() {
         if (ex.prec == Prec::MIXED)
             ladder_residual_mixed(g.value(t1), g.value(tf), g.value(t2), g.node(om2).v);
+        else if (f64_resident())
+            ladder_residual_f64(g.value(t1), g.value(tf), g.value(t2), g.node(om2).v);
         else
             ladder(g.value(Lvv), g.value(t2), g.node(om2).v);
     };
@@ -319,6 +321,8 @@ void Context::prepare_residual_caches() {
     if (ex.prec == Prec::MIXED) {
         ladder_pairs(L_vv.d(), true);
         if (ovvv_resident()) ovvv_pairs();
+    } else if (f64_resident()) {
+        f64_integrals();
     }
 }
 

@@ -196,6 +196,14 @@ int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops);
  * captured graphs.  No counterpart in eT, which calls BLAS per contraction. */
 int ccsd_gpu_set_graphs(void *ctx, int32_t on);
 
+/* Integrals of the FP64 residual.  resident = 1 (the default unless the environment sets
+ * CCSD_GPU_FP64_RESIDENT=0): the A2 ladder's +/- pair integrals and the ovvv block of the
+ * untransformed Cholesky vectors are formed once per Cholesky set and kept on the device when they
+ * fit in half of the free memory (50 GB at o = 32, v = 320), and the T1 transformation enters
+ * through o^2 v^3 corrections; resident = 0: the T1-transformed integrals are formed in blocks in
+ * every call, as omega_ccsd_a2 does (omega_ccsd.F90:113-480).  Switching off releases them. */
+int ccsd_gpu_set_fp64_integrals(void *ctx, int32_t resident);
+
 /* Residual evaluations served by a graph launch since creation, and the number of GEMM routes the
  * process holds (timed, or loaded from CCSD_GPU_TUNE_FILE). */
 int ccsd_gpu_graph_stats(void *ctx, int64_t *residual_replays, int64_t *tuned_routes);
