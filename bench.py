@@ -343,6 +343,7 @@ def run_gpu(args):
         result["speedup_to_1e-9_vs_fp64_resident"] = round(t64r / tm, 3)
         result["dE_vs_fp64"] = abs(emb - e_ref)
         result["dE_window_vs_fp64"] = abs(e - e_ref)
+        result["per_call"] = per_call_times(gpu, stream)
     gpu.close()
     if world > 1:
         import torch.distributed as dist
@@ -351,6 +352,39 @@ def run_gpu(args):
         if args.cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_sample(args)
         print(json.dumps(result), flush=True)
+
+
+def per_call_times(gpu, stream):
+    """Seconds per residual (construct_omega into a device buffer) and per one-vector Jacobian
+    transform at the converged amplitudes: medians of CUDA-event times after one untimed call, mixed
+    and both FP64 algorithms."""
+    import torch
+    from et_b200 import FP64, MIXED
+    om = torch.empty(gpu.n_amp, dtype=torch.float64, device="cuda")
+    C = 1e-2 * torch.randn(gpu.n_amp, 1, dtype=torch.float64, device="cuda")
+    R = torch.empty_like(C)
+
+    def med(fn, n):
+        fn()
+        ts = sorted(_event_time(fn, stream) for _ in range(n))
+        return round(ts[len(ts) // 2], 4)
+
+    omega = lambda: gpu.construct_omega_device(om.data_ptr())
+    jac = lambda: gpu.jacobian_device(1, C.data_ptr(), R.data_ptr())
+    out = {}
+    gpu.set_precision(MIXED)
+    out["omega_mixed_s"] = med(omega, 5)
+    out["jacobian_mixed_s"] = med(jac, 3)
+    gpu.set_precision(FP64)
+    gpu.set_fp64_integrals(True)
+    out["omega_fp64_resident_s"] = med(omega, 3)
+    out["jacobian_fp64_resident_s"] = med(jac, 1)
+    gpu.set_fp64_integrals(False)
+    out["omega_fp64_s"] = med(omega, 3)
+    out["jacobian_fp64_s"] = med(jac, 1)
+    gpu.set_fp64_integrals(True)
+    gpu.set_precision(MIXED)
+    return out
 
 
 def _event_time(fn, stream):

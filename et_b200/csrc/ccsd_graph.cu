@@ -160,16 +160,16 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
         g.contract(om, "bc,cjai->bjai", 1.0, F_vv, tf, true);
         g.contract(om, "aibk,kj->aibj", -1.0, tf, F_oo, true);
     }
-    const int omS = g.zeros("omega_sym", V4);                         // symmetric_sum (reordering.F90:416)
-    g.permute(omS, "aibj->aibj", 1.0, om);
-    g.permute(omS, "bjai->aibj", 1.0, om);
+    // om collects the terms that eT symmetrises (symmetric_sum, reordering.F90:416): the doubles
+    // residual is pack(om + om^T) with the diagonal halved, formed in one pass at the end.  Terms
+    // that are symmetric already enter with weight 1/2.
     // omega_ccsd_b2 (omega_ccsd.F90:483-583); g_aibj in FP64
-    g.contract(omS, "Jai,Jbj->aibj", 1.0, Lt_vo, Lt_vo, true);
+    g.contract(om, "Jai,Jbj->aibj", 0.5, Lt_vo, Lt_vo, true);
     {
         const int X4 = g.zeros("X_klij", {no, no, no, no});
         g.contract(X4, "Jki,Jlj->klij", 1.0, Lt_oo, Lt_oo);
         g.contract(X4, "kcld,cidj->klij", 1.0, G4, tf);
-        g.contract(omS, "akbl,klij->aibj", 1.0, tf, X4);
+        g.contract(om, "akbl,klij->aibj", 0.5, tf, X4);
     }
     // omega_ccsd_c2_d2 (omega_ccsd.F90:586-709) in contraction form
     {
@@ -180,16 +180,14 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
         g.contract(C, "kcld,djak->claj", -0.5, G4, tf);
         g.contract(D, "lckd,dkaj->claj", 1.0, G4, u);
         g.contract(D, "kcld,dkaj->claj", -0.5, G4, u);
-        const int x = g.zeros("x_c2", V4), w = g.zeros("w_d2", V4);
+        const int x = g.zeros("x_c2", V4);
         g.contract(x, "akci,ckbj->aibj", -1.5, tf, C);
-        g.contract(w, "aick,ckbj->aibj", 0.5, u, D);
-        g.permute(w, "aibj->aibj", 1.0 / 3.0, x);
-        g.permute(w, "ajbi->aibj", 2.0 / 3.0, x);
-        g.permute(omS, "aibj->aibj", 1.0, w);
-        g.permute(omS, "bjai->aibj", 1.0, w);
+        g.contract(om, "aick,ckbj->aibj", 0.5, u, D);
+        g.permute(om, "aibj->aibj", 1.0 / 3.0, x);
+        g.permute(om, "ajbi->aibj", 2.0 / 3.0, x);
     }
     const int om2 = g.zeros("omega2", {nt2});
-    g.pack_half(om2, omS);                                           // scale_diagonal(1/2) + packin
+    g.pack_sym(om2, om);                     // symmetric_sum + scale_diagonal(1/2) + packin
     // omega_ccsd_a2 (omega_ccsd.F90:113-480) as a custom op
     record_ladder(g, om2, Lt_vv, n.t2, t1, n.L_vv, tf);
     n.om1 = om1;

@@ -65,6 +65,21 @@ __global__ void pack_half_batch_kernel(const double *__restrict__ full, double *
     }
 }
 
+// packed[(M, m)] += (F[m, M] + F[M, m]) * (1/2 if M == m): consecutive threads take consecutive m
+// of one M, so the F[m, M] reads are coalesced and the F[M, m] reads of neighbouring M share sectors
+// in L2
+__global__ void pack_sym_batch_kernel(const double *__restrict__ full, double *__restrict__ packed, int64_t nov,
+                                      int64_t nbatch) {
+    const int64_t np = nov * (nov + 1) / 2;
+    GRID_STRIDE(idx, np * nbatch) {
+        int64_t n = idx / np, p = idx - n * np, M, m;
+        untri(p, M, m);
+        const double *F = full + n * nov * nov;
+        const double v = F[m + nov * M] + F[M + nov * m];
+        packed[idx] += M == m ? 0.5 * v : v;
+    }
+}
+
 __global__ void squareup_batch_kernel(const double *__restrict__ packed, double *__restrict__ full, int64_t nov,
                                       int64_t nbatch) {
     const int64_t nf = nov * nov, np = nov * (nov + 1) / 2;
@@ -194,6 +209,11 @@ void Graph::run_forward(const GOp &op) {
             nodes_[op.a].v, nodes_[op.out].v, nov, 1);
         ex_.launches++;
         break;
+    case OpKind::PackSym:
+        pack_sym_batch_kernel<<<grid_for(nov * (nov + 1) / 2, 256), 256, 0, ex_.stream>>>(
+            nodes_[op.a].v, nodes_[op.out].v, nov, 1);
+        ex_.launches++;
+        break;
     case OpKind::Trace: {
         const GNode &a = nodes_[op.a];
         trace_batch_kernel<<<grid_for(a.dims[0], 128), 128, 0, ex_.stream>>>(a.v, nodes_[op.out].v, a.dims[0],
@@ -238,6 +258,16 @@ void Graph::permute(int out, const char *spec, double alpha, int a) {
 void Graph::squareup(int out, int a) {
     GOp op;
     op.kind = OpKind::Squareup;
+    op.out = out;
+    op.a = a;
+    run_forward(op);
+    nodes_[a].last_use = (int)ops_.size();
+    ops_.push_back(op);
+}
+
+void Graph::pack_sym(int out, int a) {
+    GOp op;
+    op.kind = OpKind::PackSym;
     op.out = out;
     op.a = a;
     run_forward(op);
@@ -347,6 +377,12 @@ void Graph::jvp(const std::vector<int> &inputs, const std::vector<const double *
                 tangent(op.a, nvec), tangent(op.out, nvec), nov, nvec);
             ex_.launches++;
             break;
+        case OpKind::PackSym:
+            if (!nodes_[op.a].active) break;
+            pack_sym_batch_kernel<<<grid_for(nov * (nov + 1) / 2 * nvec, 256), 256, 0, ex_.stream>>>(
+                tangent(op.a, nvec), tangent(op.out, nvec), nov, nvec);
+            ex_.launches++;
+            break;
         case OpKind::Trace: {
             if (!nodes_[op.a].active) break;
             const GNode &a = nodes_[op.a];
@@ -425,6 +461,14 @@ void Graph::vjp(const std::vector<int> &outputs, const std::vector<const double 
         case OpKind::PackHalf:
             if (!nodes_[op.a].active) break;
             pack_half_adj_kernel<<<grid_for(nov * (nov + 1) / 2 * nvec, 256), 256, 0, ex_.stream>>>(
+                adjoint(op.out, nvec), adjoint(op.a, nvec), nov, nvec);
+            ex_.launches++;
+            break;
+        case OpKind::PackSym:
+            // d packed[(M, m)] / d F[x, y] = 1 for {x, y} = {M, m} (the diagonal's 1/2 meets two
+            // equal entries): the adjoint is the full symmetric square-up of the packed adjoint
+            if (!nodes_[op.a].active) break;
+            squareup_batch_kernel<<<grid_for(nov * nov * nvec, 256), 256, 0, ex_.stream>>>(
                 adjoint(op.out, nvec), adjoint(op.a, nvec), nov, nvec);
             ex_.launches++;
             break;

@@ -24,7 +24,7 @@ struct GNode {
     int last_use = -1;           // index of the last op reading this node
 };
 
-enum class OpKind { Contract, Permute, Squareup, PackHalf, Trace, Custom };
+enum class OpKind { Contract, Permute, Squareup, PackHalf, PackSym, Trace, Custom };
 
 // A custom op supplies its own forward / tangent / adjoint callbacks.
 struct CustomOp {
@@ -61,6 +61,9 @@ class Graph {
     void squareup(int out, int a);
     // out(packed) += pack with the diagonal halved of a (full; read triangle (m, M))
     void pack_half(int out, int a);
+    // out(packed) += pack with the diagonal halved of a + a^T (a full, not symmetric): eT's
+    // symmetric_sum, scale_diagonal(1/2) and packin in one pass
+    void pack_sym(int out, int a);
     // out[J] += sum_k a[J, k, k]
     void trace(int out, int a);
     // custom op over existing nodes
