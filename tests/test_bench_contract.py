@@ -1,0 +1,45 @@
+"""The benchmark's JSON contract on the CPU: the reference arm (the oracle timed on the host cores)
+prints one line with the metric of BASELINE.json, its own cpu_baseline and an e2e record without
+device copies; the roofline traffic comes from the committed launch list."""
+
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    sys.path.insert(0, ROOT)
+    import bench
+    return bench
+
+
+def test_metric_is_the_baseline_metric():
+    bench = _bench()
+    with open(os.path.join(ROOT, "BASELINE.json")) as f:
+        assert bench.METRIC == json.load(f)["metric"]
+
+
+def test_roofline_traffic_comes_from_the_committed_launch_list():
+    bench = _bench()
+    traffic = bench.gemm_traffic(32, 320, 1200)
+    assert traffic is not None and 1e9 < traffic < 1e11
+    assert bench.gemm_traffic(8, 40, 100) is None
+
+
+def test_reference_arm_prints_one_contract_line():
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--cpu-seconds", "1", "--cpu-o", "4", "--cpu-v", "24", "--cpu-J", "60"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "TFLOP/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["value"] == d["cpu_baseline"]["value"] == d["e2e"]["value"]
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert "workload" in d["config"]
