@@ -15,6 +15,7 @@ raises ``CCSDGPUError``.
 from __future__ import annotations
 
 import ctypes
+import json
 import os
 
 import numpy as np
@@ -103,6 +104,9 @@ SIGNATURES = {
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
     "ccsd_gpu_set_graphs": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_set_fp64_integrals": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "ccsd_gpu_set_term_timing": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "ccsd_gpu_term_timing_report": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int64,
+                                                   ctypes.POINTER(ctypes.c_int64)]),
     "ccsd_gpu_graph_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     "ccsd_gpu_set_profiling": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_gemm_profile": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP, _DP]),
@@ -380,6 +384,18 @@ class CCSD:
         """FP64 residual from resident integrals of the untransformed vectors (default, when they
         fit) or from T1-transformed integrals formed in every call (eT's omega_ccsd_a2)."""
         self._check(self.lib.ccsd_gpu_set_fp64_integrals(self.ctx, 1 if resident else 0))
+
+    def set_term_timing(self, on: bool):
+        """Per-term device times under eT's timing labels; on starts a fresh log."""
+        self._check(self.lib.ccsd_gpu_set_term_timing(self.ctx, 1 if on else 0))
+
+    def term_timings(self) -> dict:
+        """{eT timing label: {"calls": n, "ms": total device ms}} since set_term_timing(True)."""
+        need = ctypes.c_int64()
+        self._check(self.lib.ccsd_gpu_term_timing_report(self.ctx, None, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(int(need.value))
+        self._check(self.lib.ccsd_gpu_term_timing_report(self.ctx, buf, int(need.value), ctypes.byref(need)))
+        return json.loads(buf.value.decode())
 
     def graph_stats(self):
         """(residual evaluations served by a graph launch, GEMM routes held by the process)."""

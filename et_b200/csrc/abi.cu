@@ -1,5 +1,7 @@
 // extern "C" entry points (include/ccsd_gpu.h): argument checks, host<->device staging,
 // and conversion of exceptions into status codes.
+#include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <new>
 
@@ -336,6 +338,47 @@ int ccsd_gpu_set_fp64_integrals(void *ctx, int32_t resident) {
             c.f64_ovvv.release();
             c.f64_version = -1;
             c.cache_epoch++;
+        }
+    });
+}
+
+int ccsd_gpu_set_term_timing(void *ctx, int32_t on) {
+    return guarded(ctx, [&](Context &c) {
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        if (on) c.terms.clear();
+        c.terms.on = on != 0;
+    });
+}
+
+int ccsd_gpu_term_timing_report(void *ctx, char *json, int64_t capacity, int64_t *needed) {
+    return guarded(ctx, [&](Context &c) {
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        std::vector<std::string> order;
+        std::vector<std::pair<int64_t, double>> agg;
+        for (const auto &m : c.terms.marks) {
+            float ms = 0.f;
+            CU_CHECK(cudaEventElapsedTime(&ms, m.e0, m.e1));
+            size_t k = 0;
+            while (k < order.size() && order[k] != m.name) k++;
+            if (k == order.size()) {
+                order.emplace_back(m.name);
+                agg.emplace_back(0, 0.0);
+            }
+            agg[k].first++;
+            agg[k].second += ms;
+        }
+        std::string out = "{";
+        for (size_t k = 0; k < order.size(); k++) {
+            char buf[64];
+            std::snprintf(buf, sizeof buf, "{\"calls\": %lld, \"ms\": %.4f}", (long long)agg[k].first, agg[k].second);
+            out += (k ? ", \"" : "\"") + order[k] + "\": " + buf;
+        }
+        out += "}";
+        if (needed) *needed = (int64_t)out.size() + 1;
+        if (json && capacity > 0) {
+            const size_t n = std::min<size_t>(out.size(), (size_t)capacity - 1);
+            std::memcpy(json, out.data(), n);
+            json[n] = '\0';
         }
     });
 }

@@ -57,6 +57,7 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     }
     ex.blas = blas;
     ex.prof = &prof;
+    ex.terms = &terms;
     set_precision(opt ? opt->precision : CCSD_GPU_FP64);
     if (opt && opt->mixed_min_flops > 0) ex.mixed_min_flops = (double)opt->mixed_min_flops;
     if (opt && opt->mixed_k_chunk != 0) ex.k_chunk = opt->mixed_k_chunk;
@@ -102,6 +103,7 @@ Context::~Context() {
     ybuf_bytes = 0;
     if (ex.stream) cudaStreamSynchronize(ex.stream);
     prof.clear();
+    terms.clear();
     if (blas) cublasDestroy(blas);
     if (own_stream) {
         cudaStreamSynchronize(own_stream);
@@ -199,8 +201,14 @@ void Context::refresh() {
     REQUIRE(have_L && have_h, CCSD_GPU_ESTATE, "Cholesky vectors and h must be set first");
     Prec keep = ex.prec;
     ex.prec = Prec::FP64;      // the T1 transformation and the Fock matrix stay FP64
-    t1_transform_cholesky();
-    construct_fock();
+    {
+        TermTimer tt(ex, "T1 transform cholesky");
+        t1_transform_cholesky();
+    }
+    {
+        TermTimer tt(ex, "Fock matrix construction (T1 basis)");
+        construct_fock();
+    }
     ex.prec = keep;
 }
 
@@ -228,7 +236,11 @@ const double *Context::g_ovov_const() {
 double Context::energy() {
     Prec keep = ex.prec;
     ex.prec = Prec::FP64;
-    energy_reduce(ex, t.d(), t.d() + nt1, g_ovov_const(), no, nv, e_hf, scal.d());
+    const double *gov_p = g_ovov_const();
+    {
+        TermTimer tt(ex, "Calculate energy");
+        energy_reduce(ex, t.d(), t.d() + nt1, gov_p, no, nv, e_hf, scal.d());
+    }
     ex.prec = keep;
     double e;
     CU_CHECK(cudaMemcpyAsync(&e, scal.d(), sizeof(double), cudaMemcpyDeviceToHost, ex.stream));

@@ -21,6 +21,7 @@ struct Context {
     cublasHandle_t blas = nullptr;
     Exec ex;
     GemmProfile prof;
+    TermLog terms;                  // per-term device times under eT's labels (ccsd_gpu_set_term_timing)
     int64_t ladder_batch = 0;
     double e_hf = 0.0;
     bool have_L = false, have_h = false, have_t = false;

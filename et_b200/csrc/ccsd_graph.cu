@@ -83,6 +83,7 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     const int t1 = n.t1;
 
     // construct_t1_cholesky (src/wavefunctions/ccs/t1_ccs.F90:208-499); the ov block is unchanged
+    auto t1_timer = std::make_unique<TermTimer>(ex, "T1 transform cholesky");
     const int Lt_ov = g.alias(n.L_ov);
     const int Lt_oo = g.zeros("Lt_oo", {nJ, no, no});
     g.permute(Lt_oo, "Jij->Jij", 1.0, n.L_oo);
@@ -95,9 +96,11 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     g.permute(Lt_vv, "Jab->Jab", 1.0, n.L_vv);
     g.contract(Lt_vv, "aj,Jjb->Jab", -1.0, t1, n.L_ov, true);
     n.Lt_vv = Lt_vv;
+    t1_timer.reset();
 
     // T1 Fock matrix in blocks (fock_ccs.F90:242-1107): h~ = (1 - t1) h (1 + t1) then
     // F_pq = h~_pq + 2 sum_J L~_pq X_J - sum_Jk L~_pk L~_kq, X_J = sum_k L~_kk
+    auto fock_timer = std::make_unique<TermTimer>(ex, "Fock matrix construction (T1 basis)");
     const int F_oo = g.zeros("F_oo", {no, no}), F_ov = g.zeros("F_ov", {no, nv});
     const int F_vo = g.zeros("F_vo", {nv, no}), F_vv = g.zeros("F_vv", {nv, nv});
     g.permute(F_oo, "ij->ij", 1.0, n.h_oo);
@@ -121,25 +124,38 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     g.contract(F_ov, "Jpk,Jkq->pq", -1.0, Lt_oo, Lt_ov, true);
     g.contract(F_vo, "Jpk,Jkq->pq", -1.0, Lt_vo, Lt_oo, true);
     g.contract(F_vv, "Jpk,Jkq->pq", -1.0, Lt_vo, Lt_ov, true);
+    fock_timer.reset();
 
     // construct_omega_ccsd (src/wavefunctions/ccsd/omega_ccsd.F90:39-110)
     const int om1 = g.zeros("omega1", {nv, no});
     g.permute(om1, "ai->ai", 1.0, F_vo);                            // omega_ccs_a1 (omega_ccs.F90:62)
     const int tf = g.zeros("t_aibj", V4);
-    g.squareup(tf, n.t2);                                            // squareup (reordering.F90:4174)
     const int u = g.zeros("u_aibj", V4);                             // construct_u_aibj (omega_ccsd.F90:881)
-    g.permute(u, "aibj->aibj", 2.0, tf);
-    g.permute(u, "ajbi->aibj", -1.0, tf);
-    // omega_doubles_a1 (src/wavefunctions/doubles/omega_doubles.F90:36-138)
-    const int XJ = g.zeros("X_Jbi", {nJ, nv, no});
-    g.contract(XJ, "Jcj,cjbi->Jbi", 1.0, n.L_vo, u);
-    g.contract(om1, "Jab,Jbi->ai", 1.0, Lt_vv, XJ);
-    // omega_doubles_b1 (:141-204)
-    const int gkbji = g.zeros("g_kbji", {no, nv, no, no});
-    g.contract(gkbji, "Jkb,Jji->kbji", 1.0, Lt_ov, Lt_oo);
-    g.contract(om1, "ajbk,kbji->ai", -1.0, u, gkbji);
-    // omega_doubles_c1 (:207-258)
-    g.contract(om1, "aibj,jb->ai", 1.0, u, F_ov, true);
+    {
+        TermTimer tt(ex, "Construct u_aibj");
+        g.squareup(tf, n.t2);                                        // squareup (reordering.F90:4174)
+        g.permute(u, "aibj->aibj", 2.0, tf);
+        g.permute(u, "ajbi->aibj", -1.0, tf);
+    }
+    {
+        // omega_doubles_a1 (src/wavefunctions/doubles/omega_doubles.F90:36-138)
+        TermTimer tt(ex, "omega doubles a1");
+        const int XJ = g.zeros("X_Jbi", {nJ, nv, no});
+        g.contract(XJ, "Jcj,cjbi->Jbi", 1.0, n.L_vo, u);
+        g.contract(om1, "Jab,Jbi->ai", 1.0, Lt_vv, XJ);
+    }
+    {
+        // omega_doubles_b1 (:141-204)
+        TermTimer tt(ex, "omega doubles b1");
+        const int gkbji = g.zeros("g_kbji", {no, nv, no, no});
+        g.contract(gkbji, "Jkb,Jji->kbji", 1.0, Lt_ov, Lt_oo);
+        g.contract(om1, "ajbk,kbji->ai", -1.0, u, gkbji);
+    }
+    {
+        // omega_doubles_c1 (:207-258)
+        TermTimer tt(ex, "omega doubles c1");
+        g.contract(om1, "aibj,jb->ai", 1.0, u, F_ov, true);
+    }
 
     // g_ldkc, shared below (FP64 cache unless the adjoint into L_ov is wanted)
     int G4;
@@ -152,6 +168,7 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     // omega_ccsd_e2 (omega_ccsd.F90:712-878); Fock parts in FP64
     const int om = g.zeros("omega_aibj", V4);
     {
+        TermTimer tt(ex, "omega ccsd e2");
         const int Xbc = g.zeros("X_bc", {nv, nv}), Ykj = g.zeros("Y_kj", {no, no});
         g.contract(Xbc, "bkdl,ldkc->bc", -1.0, u, G4);
         g.contract(om, "bc,cjai->bjai", 1.0, Xbc, tf);
@@ -164,8 +181,9 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     // residual is pack(om + om^T) with the diagonal halved, formed in one pass at the end.  Terms
     // that are symmetric already enter with weight 1/2.
     // omega_ccsd_b2 (omega_ccsd.F90:483-583); g_aibj in FP64
-    g.contract(om, "Jai,Jbj->aibj", 0.5, Lt_vo, Lt_vo, true);
     {
+        TermTimer tt(ex, "omega ccsd b2");
+        g.contract(om, "Jai,Jbj->aibj", 0.5, Lt_vo, Lt_vo, true);
         const int X4 = g.zeros("X_klij", {no, no, no, no});
         g.contract(X4, "Jki,Jlj->klij", 1.0, Lt_oo, Lt_oo);
         g.contract(X4, "kcld,cidj->klij", 1.0, G4, tf);
@@ -173,6 +191,7 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     }
     // omega_ccsd_c2_d2 (omega_ccsd.F90:586-709) in contraction form
     {
+        TermTimer tt(ex, "omega ccsd c2 and d2");
         const int C = g.zeros("C_term", V4), D = g.zeros("D_term", V4);
         g.contract(C, "Jac,Jkj->ckaj", 1.0, Lt_vv, Lt_oo);
         g.permute(D, "ckaj->ckaj", -1.0, C);
@@ -239,6 +258,7 @@ void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv
     };
     CustomOp op;
     op.forward = [this, &g, om2, Lvv, t2, t1, tf]() {
+        TermTimer tt(ex, "omega ccsd a2");
         if (ex.prec == Prec::MIXED)
             ladder_residual_mixed(g.value(t1), g.value(tf), g.value(t2), g.node(om2).v);
         else if (f64_resident())
@@ -364,6 +384,7 @@ void Context::capture_residual(ResidualGraph &G, double *om_out) {
 
 void Context::omega(double *om_out) {
     REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+    TermTimer tt(ex, "Construct CCSD Omega");
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CU_CHECK(cudaStreamIsCapturing(ex.stream, &cap));
     const bool graphs = use_graphs && !(ex.prof && ex.prof->on) && cap == cudaStreamCaptureStatusNone;
@@ -403,6 +424,7 @@ void Context::omega(double *om_out) {
 // rho_k = A c_k for n_vec device columns [t1 | packed t2]
 void Context::jacobian(int64_t nvec, const double *c, double *rho) {
     REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+    TermTimer tt(ex, "Jacobian CCSD transformation");
     Graph g(ex);
     OmegaNodes n = record_omega(g);
     DBuf s1 = dalloc(nt1 * nvec, ex.stream), s2 = dalloc(nt2 * nvec, ex.stream);
@@ -419,6 +441,7 @@ void Context::jacobian(int64_t nvec, const double *c, double *rho) {
 // sigma_k = b_k^T A = D (dOmega/dt)^T b_k
 void Context::jacobian_transpose(int64_t nvec, const double *b, double *sigma) {
     REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+    TermTimer tt(ex, "Jacobian transpose CCSD");
     Graph g(ex);
     OmegaNodes n = record_omega(g);
     DBuf s1 = dalloc(nt1 * nvec, ex.stream), s2 = dalloc(nt2 * nvec, ex.stream);

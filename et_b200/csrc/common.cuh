@@ -131,6 +131,25 @@ struct GemmProfile {
 };
 
 // Execution environment handed to the tensor kernels.
+// Device time per named term, eT's timing labels (timings_class.F90:20-80 writes them to
+// eT.timing.out): a pair of CUDA events on the context's stream around each term while `on`.
+struct TermLog {
+    bool on = false;
+    struct Mark {
+        const char *name;   // a string literal
+        cudaEvent_t e0, e1;
+    };
+    std::vector<Mark> marks;
+    void clear() {
+        for (auto &m : marks) {
+            cudaEventDestroy(m.e0);
+            cudaEventDestroy(m.e1);
+        }
+        marks.clear();
+    }
+    ~TermLog() { clear(); }
+};
+
 struct Exec {
     cudaStream_t stream = nullptr;
     cublasHandle_t blas = nullptr;
@@ -142,6 +161,38 @@ struct Exec {
     double flops = 0.0;          // algorithmic flops issued (counted by contract())
     int64_t launches = 0;        // kernels of this library launched
     GemmProfile *prof = nullptr;
+    TermLog *terms = nullptr;
+};
+
+// Times the enclosing scope as one term of ex.terms (nothing happens unless the log is on, and
+// nothing is recorded while the stream is being captured into a graph).
+class TermTimer {
+  public:
+    TermTimer(Exec &ex, const char *name) : ex_(ex) {
+        if (!ex.terms || !ex.terms->on) return;
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(ex.stream, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return;
+        mark_.name = name;
+        if (cudaEventCreate(&mark_.e0) != cudaSuccess) return;
+        if (cudaEventCreate(&mark_.e1) != cudaSuccess) {
+            cudaEventDestroy(mark_.e0);
+            return;
+        }
+        cudaEventRecord(mark_.e0, ex.stream);
+        active_ = true;
+    }
+    ~TermTimer() {
+        if (!active_) return;
+        cudaEventRecord(mark_.e1, ex_.stream);
+        ex_.terms->marks.push_back(mark_);
+    }
+    TermTimer(const TermTimer &) = delete;
+    TermTimer &operator=(const TermTimer &) = delete;
+
+  private:
+    Exec &ex_;
+    TermLog::Mark mark_{};
+    bool active_ = false;
 };
 
 }  // namespace ccsd

@@ -204,6 +204,15 @@ int ccsd_gpu_set_graphs(void *ctx, int32_t on);
  * every call, as omega_ccsd_a2 does (omega_ccsd.F90:113-480).  Switching off releases them. */
 int ccsd_gpu_set_fp64_integrals(void *ctx, int32_t resident);
 
+/* Per-term device times under eT's timing labels ('Construct CCSD Omega', 'omega ccsd a2',
+ * 'omega ccsd c2 and d2', 'T1 transform cholesky', 'Jacobian CCSD transformation', ...; eT writes
+ * them to eT.timing.out, timings_class.F90:20-80).  on != 0 starts a fresh log (CUDA events around
+ * each term on the context's stream; nothing is recorded inside a captured graph), 0 stops it.
+ * The report is a JSON object {label: {"calls": n, "ms": total}} written to json (NUL-terminated,
+ * truncated to capacity); *needed receives the full length + 1. */
+int ccsd_gpu_set_term_timing(void *ctx, int32_t on);
+int ccsd_gpu_term_timing_report(void *ctx, char *json, int64_t capacity, int64_t *needed);
+
 /* Residual evaluations served by a graph launch since creation, and the number of GEMM routes the
  * process holds (timed, or loaded from CCSD_GPU_TUNE_FILE). */
 int ccsd_gpu_graph_stats(void *ctx, int64_t *residual_replays, int64_t *tuned_routes);
