@@ -43,3 +43,17 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert "workload" in d["config"]
+
+
+def test_synthetic_cholesky_vectors_in_et_layout():
+    """make_system gives L(J, p, q) with J fastest (eT's layout), symmetric in p, q, seeded, so the
+    host arrays go to the library without a reordering copy and every run sees the same input."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    from et_b200.synthetic import make_system
+    a, b = make_system(3, 9, 20, seed=5), make_system(3, 9, 20, seed=5)
+    assert a.L_mo.flags.f_contiguous and a.L_mo.shape == (20, 12, 12)
+    assert np.array_equal(a.L_mo, b.L_mo) and np.array_equal(a.h_mo, b.h_mo)
+    assert np.abs(a.L_mo - a.L_mo.transpose(0, 2, 1)).max() == 0.0
+    flat = a.L_mo.reshape(-1, order="F")
+    assert np.shares_memory(flat, a.L_mo)
