@@ -589,6 +589,28 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+def run_gemm(args):
+    """The tensor-core GEMM alone on one shape (default 10240^3, the (ov)^3 C2/D2 product at o=32,
+    v=320): per-launch device time from CUDA events around each launch on the launching stream,
+    issued tensor TFLOP/s (3 bf16 products x 2mnk) and FP64-equivalent TFLOP/s (2mnk).  The first
+    launch (256^3) is a warm-up, so profilers skip one launch."""
+    from et_b200 import CCSD
+    m, n, k = args.gemm_m, args.gemm_n, args.gemm_k
+    rng = np.random.default_rng(0)
+    A = np.asfortranarray(rng.standard_normal((m, k)))
+    B = np.asfortranarray(rng.standard_normal((k, n)))
+    with CCSD(2, 3, 4) as ctx:
+        ctx.selftest_gemm(A[:256, :256], B[:256, :256], mixed=True)
+        ctx.set_profiling(True)
+        for _ in range(args.gemm_reps):
+            ctx.selftest_gemm(A, B, mixed=True)
+        nl, ms, fl = ctx.gemm_profile()
+    per = ms / max(nl, 1)
+    print(json.dumps({"workload": "tensor-core GEMM", "m": m, "n": n, "k": k, "launches": nl,
+                      "ms_per_launch": round(per, 4), "issued_tflops": round(fl / nl / (per * 1e-3) / 1e12, 1),
+                      "fp64_equivalent_tflops": round(2.0 * m * n * k / (per * 1e-3) / 1e12, 1)}), flush=True)
+
+
 def cpu_sample(args):
     """The CPU oracle (numpy + threaded BLAS) on a bounded sample: GS iterations at a reduced size."""
     from oracle import ccsd as oc
@@ -631,8 +653,13 @@ def main():
     p.add_argument("--steps", type=int, default=15)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="gs", choices=["gs", "eom", "adjoint", "batch"],
-                   help="gs: the headline ground-state iteration; eom / adjoint / batch: the other workloads")
+    p.add_argument("--workload", default="gs", choices=["gs", "eom", "adjoint", "batch", "gemm"],
+                   help="gs: the headline ground-state iteration; eom / adjoint / batch: the other workloads; "
+                        "gemm: the tensor-core GEMM alone on one shape")
+    p.add_argument("--gemm-m", dest="gemm_m", type=int, default=10240)
+    p.add_argument("--gemm-n", dest="gemm_n", type=int, default=10240)
+    p.add_argument("--gemm-k", dest="gemm_k", type=int, default=10240)
+    p.add_argument("--gemm-reps", dest="gemm_reps", type=int, default=3)
     p.add_argument("--roots", type=int, default=12)
     p.add_argument("--directions", type=int, default=256)
     p.add_argument("--systems", type=int, default=64)
@@ -658,6 +685,8 @@ def main():
         run_adjoint(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "gemm":
+        run_gemm(args)
     else:
         run_gpu(args)
 

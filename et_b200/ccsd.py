@@ -29,7 +29,7 @@ MIXED = 1
 STATUS = {
     0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
     -4: "missing input", -5: "not converged", -6: "non-finite value", -7: "singular system",
-    -8: "no sm_100 device",
+    -8: "no sm_100 device", -9: "tensor-core GEMM wait timed out",
 }
 
 
@@ -91,6 +91,7 @@ SIGNATURES = {
     "ccsd_gpu_omega_device": (ctypes.c_int, [_VP, _VP]),
     "ccsd_gpu_jacobian": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
     "ccsd_gpu_jacobian_transpose": (ctypes.c_int, [_VP, _I64, _DP, _DP]),
+    "ccsd_gpu_prepare_jacobian": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_jacobian_device": (ctypes.c_int, [_VP, _I64, _VP, _VP]),
     "ccsd_gpu_jacobian_transpose_device": (ctypes.c_int, [_VP, _I64, _VP, _VP]),
     "ccsd_gpu_vjp": (ctypes.c_int, [_VP, _DP, _DP, _DP, _DP]),
@@ -113,6 +114,7 @@ SIGNATURES = {
     "ccsd_gpu_selftest_gemm": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I64, _I64,
                                               _I64, ctypes.c_double, _DP, _I64, _DP, _I64, ctypes.c_double, _DP,
                                               _I64]),
+    "ccsd_gpu_selftest_gemm_stall": (ctypes.c_int, [_VP, _I64, _I64, _I64, _I64]),
     "ccsd_gpu_mixed_gemm_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _I64, _I64, _I64, ctypes.c_double,
                                                    _VP, _I64, _VP, _I64, ctypes.c_double, _VP, _I64, _VP]),
     "ccsd_gpu_omega_flops": (ctypes.c_double, [_VP]),
@@ -292,6 +294,12 @@ class CCSD:
         self._check(self.lib.ccsd_gpu_jacobian_transpose(self.ctx, n_vec, _dp(flat), _dp(out)))
         return out if b.ndim == 1 else out.reshape(self.n_amp, n_vec, order="F")
 
+    def prepare_for_jacobian(self, side: int = 0):
+        """prepare_for_jacobian (side 0) / prepare_for_jacobian_transpose (side 1): record the
+        residual once at the current amplitudes for the transformations that follow; side -1
+        releases it.  Dropped automatically when the amplitudes, integrals or precision change."""
+        self._check(self.lib.ccsd_gpu_prepare_jacobian(self.ctx, int(side)))
+
     def jacobian_device(self, n_vec: int, d_c: int, d_rho: int, transpose: bool = False):
         """rho = A c (or sigma = b^T A) on device pointers of (n_amp x n_vec) column blocks."""
         fn = self.lib.ccsd_gpu_jacobian_transpose_device if transpose else self.lib.ccsd_gpu_jacobian_device
@@ -435,6 +443,12 @@ class CCSD:
             self.ctx, int(mixed), int(transA), int(transB), m, n, k, alpha, A.ctypes.data_as(_DP), A.shape[0],
             B.ctypes.data_as(_DP), B.shape[0], beta, Cf.ctypes.data_as(_DP), m))
         return Cf
+
+    def selftest_gemm_stall(self, m=256, n=256, k=256, wait_cycles=20_000_000) -> int:
+        """Failure-path diagnostics: one tensor-core GEMM whose producer withholds a pipeline stage,
+        so a bounded barrier wait runs out by design.  Returns the status code (-9 when the kernel
+        reported the time-out as designed) without raising."""
+        return int(self.lib.ccsd_gpu_selftest_gemm_stall(self.ctx, m, n, k, wait_cycles))
 
     def omega_flops(self) -> float:
         return float(self.lib.ccsd_gpu_omega_flops(self.ctx))

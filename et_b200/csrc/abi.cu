@@ -222,6 +222,14 @@ int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, doubl
     });
 }
 
+int ccsd_gpu_prepare_jacobian(void *ctx, int32_t side) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(side >= -1 && side <= 1, CCSD_GPU_EINVAL, "side must be 0 (right), 1 (left) or -1 (release)");
+        if (side < 0) c.drop_jacobian();
+        else c.prepare_jacobian();
+    });
+}
+
 int ccsd_gpu_jacobian_device(void *ctx, int64_t n_vec, const double *d_c, double *d_rho) {
     return guarded(ctx, [&](Context &x) {
         REQUIRE(n_vec > 0 && d_c && d_rho, CCSD_GPU_EINVAL, "bad jacobian arguments");
@@ -437,7 +445,36 @@ int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t tra
             c.ex.planes = planes;
         } else ccsd::gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc, false);
         d2h(c, C, dC.d(), nc);
-        REQUIRE(ccsd::mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM wait timed out");
+        c.check_gemm();
+    });
+}
+
+int ccsd_gpu_selftest_gemm_stall(void *ctx, int64_t m, int64_t n, int64_t k, int64_t wait_cycles) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(m > 0 && n > 0 && k > 0 && m <= 4096 && n <= 4096 && k <= 4096, CCSD_GPU_EINVAL,
+                "stall test: 0 < m, n, k <= 4096");
+        cudaStream_t s = c.ex.stream;
+        ccsd::DBuf A = ccsd::dalloc(m * k, s), B = ccsd::dalloc(k * n, s), C = ccsd::dalloc(m * n, s);
+        ccsd::fill(c.ex, A.d(), m * k, 1.0);
+        ccsd::fill(c.ex, B.d(), k * n, 1.0);
+        c.check_gemm();   // an earlier time-out is not this test's
+        const int planes = c.ex.planes;
+        c.ex.planes = 2;
+        c.ex.stall_test = 1;
+        c.ex.wait_cycles = wait_cycles;
+        try {
+            ccsd::mixed_gemm(c.ex, false, false, m, n, k, 1.0, A.d(), m, B.d(), k, 0.0, C.d(), m, 1);
+        } catch (...) {
+            c.ex.planes = planes;
+            c.ex.stall_test = 0;
+            c.ex.wait_cycles = 0;
+            throw;
+        }
+        c.ex.planes = planes;
+        c.ex.stall_test = 0;
+        c.ex.wait_cycles = 0;
+        CU_CHECK(cudaStreamSynchronize(s));
+        c.check_gemm();   // CCSD_GPU_ETIMEOUT when the withheld stage made the wait run out
     });
 }
 
@@ -447,8 +484,6 @@ int ccsd_gpu_mixed_gemm_noalloc(int32_t transA, int32_t transB, int64_t m, int64
     try {
         ccsd::mixed_gemm_noalloc(transA != 0, transB != 0, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
                                  static_cast<cudaStream_t>(stream));
-        CU_CHECK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-        REQUIRE(ccsd::mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM wait timed out");
         return CCSD_GPU_OK;
     } catch (const Error &e) {
         g_create_error = e.what();

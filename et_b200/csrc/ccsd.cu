@@ -58,6 +58,9 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     ex.blas = blas;
     ex.prof = &prof;
     ex.terms = &terms;
+    gemm_err = DBuf(sizeof(int), own_stream);
+    CU_CHECK(cudaMemsetAsync(gemm_err.as<void>(), 0, sizeof(int), own_stream));
+    ex.gemm_err = gemm_err.as<int>();
     set_precision(opt ? opt->precision : CCSD_GPU_FP64);
     if (opt && opt->mixed_min_flops > 0) ex.mixed_min_flops = (double)opt->mixed_min_flops;
     if (opt && opt->mixed_k_chunk != 0) ex.k_chunk = opt->mixed_k_chunk;
@@ -90,11 +93,13 @@ Context::~Context() {
     if (own_stream) cudaStreamSynchronize(own_stream);
     if (ex.stream && ex.stream != own_stream) cudaStreamSynchronize(ex.stream);
     // every device buffer is freed (stream-ordered) while its stream still exists
+    prep.reset();
     for (auto &G : rgraph) G.reset();
     if (ex.stream) cudaStreamSynchronize(ex.stream);
     if (graphs_captured) cudaDeviceGraphMemTrim(device);   // the physical memory the residual graphs held
     for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
-                    &mbuf, &ybuf, &om_stage, &f64_gp, &f64_gm, &f64_ovvv, &hb_oo, &hb_ov, &hb_vo, &hb_vv})
+                    &mbuf, &ybuf, &om_stage, &f64_gp, &f64_gm, &f64_ovvv, &hb_oo, &hb_ov, &hb_vo, &hb_vv,
+                    &gemm_err})
         b->release();
     if (blas) cublasDestroy(blas);
     blas = nullptr;
@@ -199,6 +204,7 @@ void Context::set_h_blocks() {
 
 void Context::refresh() {
     REQUIRE(have_L && have_h, CCSD_GPU_ESTATE, "Cholesky vectors and h must be set first");
+    drop_jacobian();   // the amplitudes (or integrals) the prepared transformations were recorded at are gone
     Prec keep = ex.prec;
     ex.prec = Prec::FP64;      // the T1 transformation and the Fock matrix stay FP64
     {
@@ -328,7 +334,9 @@ void Context::ladder(const double *Lvv, const double *t2, double *om2, int64_t n
 
 void Context::set_precision(int32_t precision) {
     REQUIRE(precision == CCSD_GPU_FP64 || precision == CCSD_GPU_MIXED, CCSD_GPU_EINVAL, "unknown precision");
-    ex.prec = precision == CCSD_GPU_FP64 ? Prec::FP64 : Prec::MIXED;
+    const Prec p = precision == CCSD_GPU_FP64 ? Prec::FP64 : Prec::MIXED;
+    if (p != ex.prec) drop_jacobian();
+    ex.prec = p;
 }
 
 // Tensor-core form of the same ladder.  With M_ab[c,d] = g_acbd the +/- sums of
@@ -345,6 +353,11 @@ void Context::set_precision(int32_t precision) {
 void Context::ladder_pairs(const double *Lvv, bool untransformed) {
     const int np = ex.planes;
     if (untransformed && mbuf_kind == 1 && mbuf_version == l_version && mbuf_planes == np) return;
+    // a prepared transformation keeps the integrals of its (T1-transformed or transposed) vectors
+    // for the next transformation of the same preparation
+    if (!untransformed && pairs_reuse_id >= 0 && mbuf_kind == 2 && mbuf_reuse == pairs_reuse_id &&
+        mbuf_src == Lvv && mbuf_version == l_version && mbuf_planes == np)
+        return;
     cudaStream_t s = ex.stream;
     const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2;
     const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
@@ -384,6 +397,8 @@ void Context::ladder_pairs(const double *Lvv, bool untransformed) {
     mbuf_kind = untransformed ? 1 : 2;
     mbuf_version = l_version;
     mbuf_planes = np;
+    mbuf_src = untransformed ? nullptr : Lvv;
+    mbuf_reuse = untransformed ? -1 : pairs_reuse_id;
     cache_epoch++;
 }
 

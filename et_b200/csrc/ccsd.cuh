@@ -1,17 +1,30 @@
 // The per-system context behind the C ABI.
 #pragma once
 
+#include <memory>
 #include <string>
 
 #include "common.cuh"
+#include "graph.cuh"
 
 namespace ccsd {
-
-class Graph;
 
 // node ids of the recorded residual
 struct OmegaNodes {
     int t1, t2, L_oo, L_ov, L_vo, L_vv, h_oo, h_ov, h_vo, h_vv, Lt_vv, om1, om2;
+};
+
+// The residual recorded once at the current amplitudes for all Jacobian transformations of a
+// Davidson run (prepare_for_jacobian, jacobian_ccsd.F90:46-71): its primal values, and through its
+// ladder op the Y intermediate and the transposed vectors; valid for the arithmetic it was
+// recorded with and until the amplitudes, integrals or h change.
+struct PreparedJacobian {
+    std::unique_ptr<Graph> g;
+    OmegaNodes n{};
+    Prec prec = Prec::FP64;
+    int planes = 0;
+    int64_t k_chunk = 0, l_version = -1;
+    int64_t id = -1;
 };
 
 struct Context {
@@ -66,6 +79,14 @@ struct Context {
     // a captured residual that points into the old one is not replayed
     int64_t cache_epoch = 0;
     DBuf blas_ws;                   // cuBLAS workspace (no allocation inside stream capture)
+    DBuf gemm_err;                  // error word of this context's tensor-core GEMMs (ex.gemm_err)
+    // ccsd_gpu_prepare_jacobian: the recorded residual shared by the transformations, and the id
+    // under which the ladder integrals a prepared transformation forms stay in mbuf for the next one
+    std::unique_ptr<PreparedJacobian> prep;
+    int64_t prep_counter = 0;
+    int64_t pairs_reuse_id = -1;    // the prepared id while a prepared transformation runs, else -1
+    const double *mbuf_src = nullptr;   // the L_vv whose pair integrals mbuf holds (mbuf_kind 2)
+    int64_t mbuf_reuse = -1;            // the prepared id they were formed for
 
     // The residual evaluation captured as a CUDA graph, one per precision.  The first evaluation in
     // a precision runs eagerly (it builds the caches and times the GEMM routes); later ones replay
@@ -118,6 +139,14 @@ struct Context {
     // Y with the T1-transformed vv block Ltvv, sum_cd g_kc~bd tau_cidj: in mixed precision
     // Y0_kibj - sum_l t_bl Q_kilj (Q_kilj = sum_cd g_kcld tau_cidj), else ladder_y(Ltvv)
     void ladder_y_t1(const double *t1, const double *Ltvv, const double *tfull, double *Y);
+    // throws CCSD_GPU_ETIMEOUT (and clears the word) when a tensor-core GEMM of this context
+    // reported a bounded wait that ran out
+    void check_gemm();
+    void prepare_jacobian();
+    void drop_jacobian();
+    // the prepared recording when it is valid for the current arithmetic, else a fresh recording
+    // into `local`
+    Graph &transform_graph(std::unique_ptr<Graph> &local, OmegaNodes &n);
     void jacobian(int64_t nvec, const double *c, double *rho);
     void jacobian_transpose(int64_t nvec, const double *b, double *sigma);
     void adjoint(const double *b, double *dt, double *dL, double *dh);

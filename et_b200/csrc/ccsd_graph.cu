@@ -414,19 +414,69 @@ void Context::omega(double *om_out) {
             }
         }
     }
-    if (ex.prec == Prec::MIXED) {
-        CU_CHECK(cudaStreamSynchronize(ex.stream));
-        REQUIRE(mixed_gemm_error_flag(true) == 0, CCSD_GPU_ECUDA, "tensor-core GEMM barrier wait timed out");
-    }
-    CU_CHECK(cudaStreamSynchronize(ex.stream));
+    check_gemm();
 }
+
+void Context::check_gemm() {
+    const int code = gemm_error(ex, true);
+    REQUIRE(code == 0, CCSD_GPU_ETIMEOUT,
+            "tensor-core GEMM barrier wait timed out (code " + std::to_string(code) + ")");
+}
+
+// prepare_for_jacobian (jacobian_ccsd.F90:46-71) / prepare_for_jacobian_transpose
+// (jacobian_transpose_ccsd.F90:44-126): eT computes and stores the t-dependent intermediates of its
+// hand-written terms once per Davidson run; here the whole residual is recorded once at the current
+// amplitudes, so every later transformation runs only its derivative pass over the stored values.
+void Context::prepare_jacobian() {
+    REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+    drop_jacobian();
+    auto p = std::make_unique<PreparedJacobian>();
+    p->g = std::make_unique<Graph>(ex);
+    p->n = record_omega(*p->g);
+    p->prec = ex.prec;
+    p->planes = ex.planes;
+    p->k_chunk = ex.k_chunk;
+    p->l_version = l_version;
+    p->id = ++prep_counter;
+    CU_CHECK(cudaStreamSynchronize(ex.stream));
+    check_gemm();
+    prep = std::move(p);
+}
+
+void Context::drop_jacobian() {
+    if (!prep) return;
+    prep.reset();
+    if (mbuf_kind == 2) mbuf_reuse = -1;
+}
+
+Graph &Context::transform_graph(std::unique_ptr<Graph> &local, OmegaNodes &n) {
+    if (prep && prep->prec == ex.prec && prep->planes == ex.planes && prep->k_chunk == ex.k_chunk &&
+        prep->l_version == l_version) {
+        n = prep->n;
+        pairs_reuse_id = prep->id;
+        return *prep->g;
+    }
+    local = std::make_unique<Graph>(ex);
+    n = record_omega(*local);
+    return *local;
+}
+
+namespace {
+// a prepared transformation's ladder integrals stay reusable only while it runs
+struct ReuseScope {
+    int64_t &id;
+    ~ReuseScope() { id = -1; }
+};
+}  // namespace
 
 // rho_k = A c_k for n_vec device columns [t1 | packed t2]
 void Context::jacobian(int64_t nvec, const double *c, double *rho) {
     REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
     TermTimer tt(ex, "Jacobian CCSD transformation");
-    Graph g(ex);
-    OmegaNodes n = record_omega(g);
+    ReuseScope scope{pairs_reuse_id};
+    std::unique_ptr<Graph> local;
+    OmegaNodes n;
+    Graph &g = transform_graph(local, n);
     DBuf s1 = dalloc(nt1 * nvec, ex.stream), s2 = dalloc(nt2 * nvec, ex.stream);
     split_amp_kernel<<<grid_for(namp * nvec, 256), 256, 0, ex.stream>>>(c, nt1, nov, nvec, 2.0, s1.d(), s2.d());
     ex.launches++;
@@ -435,15 +485,19 @@ void Context::jacobian(int64_t nvec, const double *c, double *rho) {
     join_amp_kernel<<<grid_for(namp * nvec, 256), 256, 0, ex.stream>>>(r1.d(), r2.d(), nt1, nov, nvec, 1.0, rho);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
+    g.clear_derivatives();
     CU_CHECK(cudaStreamSynchronize(ex.stream));
+    check_gemm();
 }
 
 // sigma_k = b_k^T A = D (dOmega/dt)^T b_k
 void Context::jacobian_transpose(int64_t nvec, const double *b, double *sigma) {
     REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
     TermTimer tt(ex, "Jacobian transpose CCSD");
-    Graph g(ex);
-    OmegaNodes n = record_omega(g);
+    ReuseScope scope{pairs_reuse_id};
+    std::unique_ptr<Graph> local;
+    OmegaNodes n;
+    Graph &g = transform_graph(local, n);
     DBuf s1 = dalloc(nt1 * nvec, ex.stream), s2 = dalloc(nt2 * nvec, ex.stream);
     split_amp_kernel<<<grid_for(namp * nvec, 256), 256, 0, ex.stream>>>(b, nt1, nov, nvec, 1.0, s1.d(), s2.d());
     ex.launches++;
@@ -452,7 +506,9 @@ void Context::jacobian_transpose(int64_t nvec, const double *b, double *sigma) {
     join_amp_kernel<<<grid_for(namp * nvec, 256), 256, 0, ex.stream>>>(r1.d(), r2.d(), nt1, nov, nvec, 2.0, sigma);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
+    g.clear_derivatives();
     CU_CHECK(cudaStreamSynchronize(ex.stream));
+    check_gemm();
 }
 
 // b^T dOmega/d(t, L, h): amplitude part without the D scaling, plus the adjoints into the MO
@@ -516,6 +572,7 @@ void Context::adjoint(const double *b, double *dt, double *dL, double *dh) {
     }
     CU_CHECK(cudaGetLastError());
     CU_CHECK(cudaStreamSynchronize(ex.stream));
+    check_gemm();
 }
 
 }  // namespace ccsd

@@ -162,6 +162,9 @@ struct Exec {
     int64_t launches = 0;        // kernels of this library launched
     GemmProfile *prof = nullptr;
     TermLog *terms = nullptr;
+    int *gemm_err = nullptr;     // device error word of this caller's tensor-core GEMMs (one per context)
+    long long wait_cycles = 0;   // bound of the GEMM's barrier waits (<= 0: the default, ~2 s)
+    int stall_test = 0;          // diagnostics only: the next GEMMs withhold one stage of loads
 };
 
 // Times the enclosing scope as one term of ex.terms (nothing happens unless the log is on, and

@@ -18,6 +18,21 @@
 namespace ccsd {
 
 namespace {
+// A Davidson run prepares the transformations once (eT calls prepare_for_jacobian before its
+// solver loop) and drops what it prepared when it ends; a preparation the caller made is kept.
+struct PrepareScope {
+    Context &c;
+    bool own;
+    explicit PrepareScope(Context &ctx) : c(ctx), own(!ctx.prep) {
+        if (own) c.prepare_jacobian();
+    }
+    ~PrepareScope() {
+        if (own) c.drop_jacobian();
+    }
+};
+}  // namespace
+
+namespace {
 
 #define SOLVER_CHECK(x)                                                                        \
     do {                                                                                       \
@@ -125,6 +140,7 @@ int Context::davidson(int nstates, int side, const ccsd_gpu_davidson_options *o,
     }
     nnew = nstates;
     std::vector<double> omega(nstates, 0.0), prev(nstates, 0.0);
+    PrepareScope prepared(*this);
     DBuf G = dalloc(maxdim * maxdim, s), X = dalloc(namp * nstates, s), R = dalloc(namp * nstates, s);
     DBuf proj = dalloc(maxdim * std::max<int64_t>(nstates, 1), s), nrm = dalloc(8, s);
     Geev geev(s);
@@ -262,6 +278,7 @@ int Context::multipliers(const ccsd_gpu_davidson_options *o, double *tbar, int32
     orbital_differences(ex, eps.d(), no, nv, epsdiff.d());
     DBuf et = dalloc(namp, s);
     eta(et.d());
+    PrepareScope prepared(*this);
     DBuf V = dalloc(namp * maxdim, s), AV = dalloc(namp * maxdim, s), x = dalloc(namp, s), r = dalloc(namp, s);
     DBuf cand = dalloc(namp, s), proj = dalloc(maxdim, s), nrm = dalloc(8, s);
     DBuf G = dalloc(maxdim * maxdim, s), rhs = dalloc(maxdim, s);

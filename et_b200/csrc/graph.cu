@@ -322,8 +322,16 @@ void Graph::mark_active(const std::vector<int> &inputs) {
     }
 }
 
+void Graph::clear_derivatives() {
+    for (auto &n : nodes_) {
+        n.tan.release();
+        n.adj.release();
+    }
+}
+
 void Graph::jvp(const std::vector<int> &inputs, const std::vector<const double *> &seeds, int nvec,
                 const std::vector<int> &outputs, const std::vector<double *> &results) {
+    clear_derivatives();
     mark_active(inputs);
     for (size_t k = 0; k < inputs.size(); k++) {
         double *t = tangent(inputs[k], nvec);
@@ -410,6 +418,7 @@ void Graph::jvp(const std::vector<int> &inputs, const std::vector<const double *
 
 void Graph::vjp(const std::vector<int> &outputs, const std::vector<const double *> &seeds, int nvec,
                 const std::vector<int> &inputs, const std::vector<double *> &results) {
+    clear_derivatives();
     mark_active(inputs);
     for (size_t k = 0; k < outputs.size(); k++) {
         double *a = adjoint(outputs[k], nvec);

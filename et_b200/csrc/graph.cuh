@@ -73,8 +73,10 @@ class Graph {
     const double *value(int i) const { return nodes_[i].v; }
     int64_t nov = 0;               // for squareup / pack_half
 
-    // derivative passes; seeds are [size x nvec] device arrays for the listed nodes
+    // derivative passes; seeds are [size x nvec] device arrays for the listed nodes.  Each pass
+    // starts from zero tangents / adjoints, so a recording can serve several passes.
     void mark_active(const std::vector<int> &inputs);
+    void clear_derivatives();
     void jvp(const std::vector<int> &inputs, const std::vector<const double *> &seeds, int nvec,
              const std::vector<int> &outputs, const std::vector<double *> &results);
     void vjp(const std::vector<int> &outputs, const std::vector<const double *> &seeds, int nvec,

@@ -14,7 +14,8 @@
 // (Exec::k_chunk, 4096 by default): each chunk accumulates in one TMEM buffer and the epilogue
 // adds it to the FP64 output while the next chunk accumulates in the other; the same CTA takes
 // the chunks of a tile in order, so the sum is deterministic.  Every mbarrier wait is bounded;
-// on time-out the kernel records an error code, skips its remaining work and frees its TMEM.
+// on time-out the kernel records an error code in the caller's error word (one per context),
+// skips its remaining work, waits (bounded) for the copies it has in flight and frees its TMEM.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -35,6 +36,8 @@ constexpr int B_ROW_PAD = 256;             // B operand rows are padded to 256 i
 constexpr int THREADS = 192;              // producer warp, MMA warp, four epilogue warps
 constexpr int EPI_THREADS = 128;
 constexpr long long WAIT_CYCLES = 4000000000ll;   // ~2 s at 2 GHz: far above any legitimate wait
+// error codes written to the caller's error word when a bounded wait runs out
+constexpr int ERR_PRODUCER = 1, ERR_MMA_FULL = 2, ERR_EPILOGUE = 3, ERR_MMA_ACC = 4, ERR_DONE = 5, ERR_DRAIN = 6;
 
 // plane count and N tile of one mode
 template <int NP_, int BN_>
@@ -59,11 +62,12 @@ using ModeX6 = Mode<3, 128>;
 static_assert(ModeX3::STAGE_BYTES == 96 * 1024 && ModeX6::STAGE_BYTES == 96 * 1024, "stage size");
 static_assert(B_ROW_PAD % ModeX3::BN == 0 && B_ROW_PAD % ModeX6::BN == 0, "B padding");
 
-__device__ int g_mixed_gemm_error = 0;
-
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+
+// the first bounded wait that runs out names the error; later ones keep it
+__device__ __forceinline__ void record_error(int *err, int code) { atomicCAS(err, 0, code); }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
@@ -74,8 +78,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                  : "memory");
 }
 
-// bounded wait for the completion of the phase with the given parity; false on time-out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// bounded wait for the completion of the phase with the given parity; false after `limit` cycles
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
     uint32_t addr = smem_u32(bar);
     const long long t0 = clock64();
     while (true) {
@@ -88,7 +92,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
             : "r"(addr), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > WAIT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -251,6 +255,10 @@ namespace {
 struct TileMap {
     int num_mt, num_nt, nk_all, nks, group_m, bn;
     int kc;   // K blocks accumulated in TMEM before the epilogue takes the partial sum (FP64)
+    int *err;               // the caller's error word (device): a bounded wait that ran out writes its code
+    long long wait_cycles;  // bound of every barrier wait
+    int stall_test;         // diagnostics: the producer withholds the loads of its first stage, so the
+                            // MMA warp's wait for it runs out by design
     __device__ __forceinline__ void decode(int t, int &m0, int &n0, int &z, int &kt0, int &nk) const {
         const int per_split = num_mt * num_nt;
         z = t / per_split;
@@ -317,16 +325,19 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
         if (lane == 0) {
             // TMA producer: one ring of stages across all tiles of this CTA
             int g = 0;
+            int issued[STAGES] = {};   // loads issued per stage (at most the last one is in flight)
             for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
                 int m0, n0, z, kt0, nk;
                 map.decode(t, m0, n0, z, kt0, nk);
                 for (int i = 0; i < nk; i++, g++) {
                     const int s = g % STAGES;
-                    if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1) || *abort_flag) {
-                        atomicExch(&g_mixed_gemm_error, 1);
+                    if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1, map.wait_cycles) || *abort_flag) {
+                        record_error(map.err, ERR_PRODUCER);
                         *abort_flag = 1;
                         break;
                     }
+                    if (map.stall_test && g == 0) continue;   // stage 0's first phase never completes
+                    issued[s]++;
                     uint8_t *st = smem + s * STAGE_BYTES;
                     mbar_expect_tx(&full[s], STAGE_BYTES);
                     const int k0 = (kt0 + i) * BK;
@@ -337,6 +348,12 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
                     }
                 }
             }
+            // the last load issued to each stage may still be landing (the consumers may abort
+            // before they read it): wait for it, so no copy of this CTA is in flight when its
+            // shared memory goes away.  In a normal run these phases complete anyway.
+            for (int s = 0; s < STAGES; s++)
+                if (issued[s] && !mbar_wait(&full[s], (issued[s] - 1) & 1, map.wait_cycles))
+                    record_error(map.err, ERR_DRAIN);
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -349,8 +366,8 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
                 map.decode(t, m0, n0, z, kt0, nk);
                 for (int c0 = 0; c0 < nk && !*abort_flag; c0 += map.kc, tc++) {
                 const int acc = tc & 1;
-                if (!mbar_wait(&acc_empty[acc], ((tc >> 1) & 1) ^ 1)) {
-                    atomicExch(&g_mixed_gemm_error, 4);
+                if (!mbar_wait(&acc_empty[acc], ((tc >> 1) & 1) ^ 1, map.wait_cycles)) {
+                    record_error(map.err, ERR_MMA_ACC);
                     *abort_flag = 1;
                     break;
                 }
@@ -359,8 +376,8 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
                 const int c1 = min(nk, c0 + map.kc);
                 for (int i = c0; i < c1; i++, g++) {
                     const int s = g % STAGES;
-                    if (!mbar_wait(&full[s], (g / STAGES) & 1) || *abort_flag) {
-                        atomicExch(&g_mixed_gemm_error, 2);
+                    if (!mbar_wait(&full[s], (g / STAGES) & 1, map.wait_cycles) || *abort_flag) {
+                        record_error(map.err, ERR_MMA_FULL);
                         *abort_flag = 1;
                         break;
                     }
@@ -394,10 +411,10 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
             map.decode(t, m0, n0, z, kt0, nk);
             for (int c0 = 0; c0 < nk; c0 += map.kc, tc++) {
             const int acc = tc & 1;
-            bool ok = !*abort_flag && mbar_wait(&acc_full[acc], (tc >> 1) & 1);
+            bool ok = !*abort_flag && mbar_wait(&acc_full[acc], (tc >> 1) & 1, map.wait_cycles);
             __syncwarp();
             if (!ok || *abort_flag) {
-                atomicExch(&g_mixed_gemm_error, 3);
+                record_error(map.err, ERR_EPILOGUE);
                 *abort_flag = 1;
                 aborted = true;
                 break;
@@ -420,7 +437,7 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
     }
     __syncthreads();
     // all MMAs complete before the TMEM is released
-    if (!mbar_wait(done, 0)) atomicExch(&g_mixed_gemm_error, 5);
+    if (!mbar_wait(done, 0, map.wait_cycles)) record_error(map.err, ERR_DONE);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 1) {
@@ -550,6 +567,10 @@ void launch_mode(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_pla
     map.bn = MD::BN;
     map.group_m = std::min(map.num_mt, 16);
     map.kc = (Epi::kChunked && ex.k_chunk > 0) ? (int)std::max<int64_t>(1, ex.k_chunk / BK) : map.nks;
+    REQUIRE(ex.gemm_err != nullptr, CCSD_GPU_EINVAL, "tc gemm: no error word");
+    map.err = ex.gemm_err;
+    map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : WAIT_CYCLES;
+    map.stall_test = ex.stall_test;
     const int num_tiles = map.num_mt * map.num_nt * splits;
     dim3 grid((unsigned)std::min(num_tiles, sm_count()));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -741,13 +762,12 @@ void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp,
               double(epi.M) * double(epi.N) * double(k_true));
 }
 
-int mixed_gemm_error_flag(bool reset) {
+int gemm_error(Exec &ex, bool reset) {
+    if (!ex.gemm_err) return 0;
     int v = 0;
-    CU_CHECK(cudaMemcpyFromSymbol(&v, g_mixed_gemm_error, sizeof(int)));
-    if (reset && v) {
-        int z = 0;
-        CU_CHECK(cudaMemcpyToSymbol(g_mixed_gemm_error, &z, sizeof(int)));
-    }
+    CU_CHECK(cudaMemcpyAsync(&v, ex.gemm_err, sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
+    CU_CHECK(cudaStreamSynchronize(ex.stream));
+    if (reset && v) CU_CHECK(cudaMemsetAsync(ex.gemm_err, 0, sizeof(int), ex.stream));
     return v;
 }
 
@@ -764,26 +784,34 @@ int mixed_gemm_error_flag(bool reset) {
 // bf16 elements of the fixed split scratch: hi and lo planes of A (Mp x Kp) and of B (Np x Kp)
 constexpr int64_t NOALLOC_SCRATCH_ELEMS = 8ll << 20;   // 16 MiB, held by every GPU that loads the library
 static __device__ __align__(256) __nv_bfloat16 g_noalloc_split[NOALLOC_SCRATCH_ELEMS];
+// error word of the allocation-free entry point (shared by all its callers, like the scratch)
+static __device__ int g_noalloc_error = 0;
 
 namespace {
 std::mutex g_noalloc_mutex;
 void *g_noalloc_ptr[128] = {};   // device address of g_noalloc_split, per device ordinal
+void *g_noalloc_err[128] = {};   // device address of g_noalloc_error, per device ordinal
 }  // namespace
 
-// Device address of the scratch for the current device (looked up once per device; the first call
-// on a device does this set-up).
-static __nv_bfloat16 *noalloc_scratch() {
+// Device addresses of the scratch and of the error word for the current device (looked up once
+// per device; the first call on a device does this set-up).
+static __nv_bfloat16 *noalloc_scratch(int **err) {
     int dev = 0;
     CU_CHECK(cudaGetDevice(&dev));
     REQUIRE(dev >= 0 && dev < 128, CCSD_GPU_EINVAL, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
+        void *p = nullptr, *e = nullptr;
         cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_split);
         REQUIRE(rc == cudaSuccess && p != nullptr, CCSD_GPU_ECUDA,
                 std::string("cudaGetSymbolAddress of the no-alloc scratch failed: ") + cudaGetErrorString(rc));
+        rc = cudaGetSymbolAddress(&e, g_noalloc_error);
+        REQUIRE(rc == cudaSuccess && e != nullptr, CCSD_GPU_ECUDA,
+                std::string("cudaGetSymbolAddress of the no-alloc error word failed: ") + cudaGetErrorString(rc));
+        g_noalloc_err[dev] = e;
         g_noalloc_ptr[dev] = p;
     }
+    *err = static_cast<int *>(g_noalloc_err[dev]);
     return static_cast<__nv_bfloat16 *>(g_noalloc_ptr[dev]);
 }
 
@@ -791,15 +819,18 @@ void mixed_gemm_noalloc(bool transA, bool transB, int64_t m, int64_t n, int64_t 
                         int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc,
                         cudaStream_t stream) {
     REQUIRE(m > 0 && n > 0 && k > 0 && A && B && C, CCSD_GPU_EINVAL, "bad gemm arguments");
+    REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "no-alloc GEMM: size too large");
     REQUIRE(lda >= (transA ? k : m) && ldb >= (transB ? n : k) && ldc >= m, CCSD_GPU_EINVAL, "bad leading dimension");
     const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, B_ROW_PAD);
     const int64_t need = 2 * (Mp + Np) * Kp;
     REQUIRE(need <= NOALLOC_SCRATCH_ELEMS, CCSD_GPU_EINVAL,
             "no-alloc GEMM: 2 x (round_up(m,128) + round_up(n,256)) x round_up(k,64) = " + std::to_string(need) +
                 " bf16 elements exceeds the fixed scratch of " + std::to_string(NOALLOC_SCRATCH_ELEMS));
-    __nv_bfloat16 *scratch = noalloc_scratch();
+    int *err = nullptr;
+    __nv_bfloat16 *scratch = noalloc_scratch(&err);
     Exec ex;
     ex.stream = stream;
+    ex.gemm_err = err;
     __nv_bfloat16 *a = scratch, *b = scratch + 2 * Mp * Kp;
     if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, 2, a);
     else split(ex, A, lda, 1, m, k, Mp, Kp, 2, a);
@@ -807,6 +838,9 @@ void mixed_gemm_noalloc(bool transA, bool transB, int64_t m, int64_t n, int64_t 
     else split(ex, B, 1, ldb, n, k, Np, Kp, 2, b);
     EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
     launch_tc(ex, 2, a, Mp, Mp * Kp, m, b, Np, Np * Kp, n, Kp, epi, double(m) * double(n) * double(k));
+    // synchronous: the caller learns of a bounded wait that ran out from the return status
+    const int code = gemm_error(ex, true);
+    REQUIRE(code == 0, CCSD_GPU_ETIMEOUT, "tensor-core GEMM barrier wait timed out (code " + std::to_string(code) + ")");
 }
 
 }  // namespace ccsd

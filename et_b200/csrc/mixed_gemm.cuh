@@ -52,12 +52,14 @@ void tc_gemm_ovvv(Exec &ex, const __nv_bfloat16 *Lov, int64_t ov_rows, const __n
 void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,
                    __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld, int64_t k_true);
 
-// The same GEMM with its split scratch in a fixed file-scope device array (no allocation).
+// The same GEMM with its split scratch in a fixed file-scope device array (no allocation);
+// synchronous, throws CCSD_GPU_ETIMEOUT when a bounded wait ran out.
 void mixed_gemm_noalloc(bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
                         int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc,
                         cudaStream_t stream);
 
-// Error code recorded by a tensor-core GEMM whose bounded barrier wait timed out (0 = none).
-int mixed_gemm_error_flag(bool reset);
+// Error code that a tensor-core GEMM on ex's error word recorded when a bounded barrier wait ran
+// out (0 = none); waits for ex.stream first, and clears the word when reset is set.
+int gemm_error(Exec &ex, bool reset);
 
 }  // namespace ccsd

@@ -5,7 +5,7 @@
  * class(ccsd) (paths relative to the eT source tree).  eT's Fortran binds
  * them through an ISO_C_BINDING interface block in the style of
  * src/libint/eri_cdef.F90:25-68 (bind(C), value scalars, real(c_double)
- * arrays); see INTEGRATION.md for the interface block and the shim.
+ * arrays), one interface per function below.
  *
  * Conventions (identical to eT):
  *  - every array is column-major double precision and owned by the caller;
@@ -43,7 +43,9 @@ enum {
     CCSD_GPU_ENOCONV = -5,       /* solver did not converge */
     CCSD_GPU_ENAN = -6,          /* non-finite value detected */
     CCSD_GPU_ESINGULAR = -7,     /* DIIS / reduced-space system singular */
-    CCSD_GPU_ENODEV = -8         /* no sm_100 device available */
+    CCSD_GPU_ENODEV = -8,        /* no sm_100 device available */
+    CCSD_GPU_ETIMEOUT = -9       /* a tensor-core GEMM's bounded barrier wait ran out (the GEMM
+                                    stopped early; the context stays usable) */
 };
 
 /* arithmetic used by the contractions */
@@ -136,6 +138,17 @@ int ccsd_gpu_jacobian_transpose(void *ctx, int64_t n_vec, const double *b, doubl
 /* The same two transformations on device pointers (trial and result blocks stay in HBM). */
 int ccsd_gpu_jacobian_device(void *ctx, int64_t n_vec, const double *d_c, double *d_rho);
 int ccsd_gpu_jacobian_transpose_device(void *ctx, int64_t n_vec, const double *d_b, double *d_sigma);
+
+/* prepare_for_jacobian / prepare_for_jacobian_transpose (src/wavefunctions/ccsd/jacobian_ccsd.F90:46-71,
+ * jacobian_transpose_ccsd.F90:44-126): side 0 (right) or 1 (left) keeps the intermediates of the
+ * current amplitudes that every transformation of a Davidson run reuses (the recorded residual
+ * with its primal values, and the transformations' ladder integrals), so later calls of
+ * ccsd_gpu_jacobian(_transpose)(_device) only run the derivative pass.  Both sides share what is
+ * kept.  Anything that changes the amplitudes, the integrals or the arithmetic (set_amplitudes,
+ * set_cholesky_*, set_h_mo, mp2_guess, set_precision, solve_gs) drops it, and the transformations
+ * then record afresh per call as without preparation; side -1 drops it explicitly.  Costs the device
+ * memory of the recorded residual (about 25 (o v)^2 doubles). */
+int ccsd_gpu_prepare_jacobian(void *ctx, int32_t side);
 
 /* Vector-Jacobian product of the residual: given a cotangent b (n_t1 + n_t2), returns
  *   dt = (dOmega/dt)^T b                      (n_t1 + n_t2; sigma = D dt with D = 2 on the doubles diagonal),
@@ -234,19 +247,29 @@ int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t tra
 
 /* Allocation-free split-BF16 tensor-core GEMM; no counterpart in eT.
  * C (m x n, column-major, device) = alpha op(A) op(B) + beta C with A, B, C device pointers on the
- * current device, run on `stream` (a cudaStream_t as void*, NULL = legacy default stream); returns
- * after the stream has finished the product.  It is for callers that cannot allocate device memory
- * when they call in (a host program that reserved the whole GPU for its own pool, or a code path
- * that must avoid the synchronisation of cudaMalloc/cudaFree): it makes no cudaMalloc/cudaFree or
- * other allocating call.  Its scratch is a fixed 16 MiB device array inside the library (held by
- * every GPU that loads it): 2 x (round_up(m,128) + round_up(n,256)) x round_up(k,64) must not exceed
- * 8388608, larger sizes are rejected with CCSD_GPU_EINVAL.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.  All calls share the
- * array, so calls that overlap on the GPU (e.g. on two streams) race; serialise them.  Errors are
- * reported through ccsd_gpu_last_error(NULL). */
+ * current device, run on `stream` (a cudaStream_t as void*, NULL = legacy default stream).  It is
+ * for callers that cannot allocate device memory when they call in (a host program that reserved
+ * the whole GPU for its own pool, or a code path that must avoid the synchronisation of
+ * cudaMalloc/cudaFree): it makes no cudaMalloc/cudaFree or other allocating call.  Its scratch is a
+ * fixed 16 MiB device array inside the library (held by every GPU that loads it):
+ * 2 x (round_up(m,128) + round_up(n,256)) x round_up(k,64) must not exceed 8388608, and m, n, k
+ * must be below 2^31; larger sizes are rejected with CCSD_GPU_EINVAL.  The call is synchronous: it
+ * waits for `stream` to finish the product and reads the GEMM's error word before it returns
+ * (CCSD_GPU_ETIMEOUT if a bounded wait ran out), so it must not be called while a stream is being
+ * captured into a graph.  The first call on a device looks up the device addresses of the scratch
+ * and of the error word.  All calls share the array, so calls that overlap on the GPU (e.g. from two
+ * host threads on two streams) race; serialise them.  Errors are reported through
+ * ccsd_gpu_last_error(NULL). */
 int ccsd_gpu_mixed_gemm_noalloc(int32_t transA, int32_t transB, int64_t m, int64_t n, int64_t k, double alpha,
                                 const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C,
                                 int64_t ldc, void *stream);
+
+/* Diagnostics of the failure path: one m x n x k tensor-core GEMM on the context's stream in which
+ * the TMA producer withholds the loads of its first pipeline stage, so the MMA warp's bounded wait
+ * for them runs out by design after wait_cycles SM clock cycles (<= 0: the normal bound, ~2 s).
+ * Returns CCSD_GPU_ETIMEOUT when the kernel reported the time-out as designed; the context stays
+ * usable afterwards.  No counterpart in eT. */
+int ccsd_gpu_selftest_gemm_stall(void *ctx, int64_t m, int64_t n, int64_t k, int64_t wait_cycles);
 
 /* Algorithmic flop count of one Omega at this context's dimensions, summed over eT's own BLAS
  * call sites (2mnk per DGEMM, n(n+1)k per DSFRK). */

@@ -193,3 +193,33 @@ def test_multipliers_residual_h2o_he(h2o_he):
     r = gpu.jacobian_transpose_transformation(tbar) + gpu.construct_eta()
     assert np.linalg.norm(r) < 1e-8
     gpu.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_prepared_transformations_equal_fresh_ones(precision):
+    """ccsd_gpu_prepare_jacobian records the residual once; the transformations that follow reuse
+    it and must give exactly what a fresh recording gives.  New amplitudes drop the preparation."""
+    from et_b200 import CCSD
+    n_o, n_v, n_J = 4, 16, 40
+    s = make_system(n_o, n_v, n_J, seed=17)
+    rng = np.random.default_rng(8)
+    with CCSD(n_o, n_v, n_J, precision=precision, mixed_min_flops=1) as g:
+        g.set_system(s.L_mo, s.h_mo, s.eps)
+        amp = 0.05 * rng.standard_normal(g.n_amp)
+        g.set_amplitudes(amp)
+        C = rng.standard_normal((g.n_amp, 3))
+        fresh = (g.jacobian_transformation(C), g.jacobian_transpose_transformation(C))
+        g.prepare_for_jacobian(0)
+        for _ in range(2):
+            prepared = (g.jacobian_transformation(C), g.jacobian_transpose_transformation(C))
+            for a, b in zip(fresh, prepared):
+                assert np.array_equal(a, b)
+        assert np.array_equal(g.jacobian_transformation(C[:, 1]), fresh[0][:, 1])
+        g.set_amplitudes(2.0 * amp)
+        ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
+        ref.set_amplitudes(2.0 * amp)
+        rho, rho_ref = g.jacobian_transformation(C[:, 0]), ref.jacobian_transformation(C[:, 0])
+        tol = 1e-11 if precision == 0 else 1e-4
+        assert np.linalg.norm(rho - rho_ref) <= tol * np.linalg.norm(rho_ref)
+        g.prepare_for_jacobian(1)
+        g.prepare_for_jacobian(-1)
