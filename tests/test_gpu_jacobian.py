@@ -209,12 +209,13 @@ def test_prepared_transformations_equal_fresh_ones(precision):
         g.set_amplitudes(amp)
         C = rng.standard_normal((g.n_amp, 3))
         fresh = (g.jacobian_transformation(C), g.jacobian_transpose_transformation(C))
+        fresh1 = g.jacobian_transformation(C[:, 1])      # one vector: other GEMM shapes than the block
         g.prepare_for_jacobian(0)
         for _ in range(2):
             prepared = (g.jacobian_transformation(C), g.jacobian_transpose_transformation(C))
             for a, b in zip(fresh, prepared):
                 assert np.array_equal(a, b)
-        assert np.array_equal(g.jacobian_transformation(C[:, 1]), fresh[0][:, 1])
+        assert np.array_equal(g.jacobian_transformation(C[:, 1]), fresh1)
         g.set_amplitudes(2.0 * amp)
         ref = oc.CCSDSystem(s.L_mo, s.h_mo, s.eps, s.n_o)
         ref.set_amplitudes(2.0 * amp)
