@@ -231,6 +231,51 @@ __global__ void energy_partial_kernel(const double *__restrict__ t1, const doubl
     }
 }
 
+// E_corr partial sums from the packed doubles: the (ia, jb) matrix of g_iajb is symmetric
+// (g_iajb = g_jbia), so its o x o sub-block P_ab[i,j] = g_iajb also gives g_ibja = P_ab[j,i] and
+// serves both orders of the virtual pair:
+//   E_ab + E_ba = sum_ij T[ai,bj] (2 P[i,j] - P[j,i]) + T[bi,aj] (2 P[j,i] - P[i,j]),
+// T = t2 + t1 t1.  One pair a >= b at a time per block: P is staged in shared memory (read once,
+// coalesced along i), and every packed t2 element belongs to exactly one pair, so the kernel reads
+// half of g and all of t2 once.  Pairs run in packed order (b fastest), so blocks resident together
+// share the DRAM sectors of neighbouring t2 rows.
+__global__ void energy_pairs_kernel(const double *__restrict__ t1, const double *__restrict__ t2,
+                                    const double *__restrict__ g, int no, int64_t nv, int64_t npairs,
+                                    double *__restrict__ partial) {
+    extern __shared__ double P[];   // (no + 1) x no, padded against bank conflicts
+    const int ld = no + 1, nn = no * no;
+    double acc = 0.0;
+    for (int64_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+        int64_t a, b;
+        untri(p, a, b);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+            const int i = k % no, j = k / no;
+            P[i + ld * j] = g[i + no * (a + nv * (j + (int64_t)no * b))];
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+            const int i = k % no, j = k / no;
+            const double pij = P[i + ld * j], pji = P[j + ld * i];
+            const int64_t ai = a + nv * i, bj = b + nv * j;
+            acc += (t2[pk(ai, bj)] + t1[ai] * t1[bj]) * (2.0 * pij - pji);
+            if (a != b) {
+                const int64_t bi = b + nv * i, aj = a + nv * j;
+                acc += (t2[pk(bi, aj)] + t1[bi] * t1[aj]) * (2.0 * pji - pij);
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double r = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = r;
+    }
+}
+
 __global__ void sum_partial_kernel(const double *__restrict__ partial, int n, double add, double *__restrict__ out) {
     __shared__ double sh[32];
     double acc = 0.0;
@@ -451,7 +496,13 @@ void energy_reduce(Exec &ex, const double *t1, const double *t2, const double *g
                    double add, double *d_out) {
     const int nb = 592;
     DBuf part = dalloc(nb, ex.stream);
-    energy_partial_kernel<<<nb, 256, 0, ex.stream>>>(t1, t2, g_ovov, no, nv, part.d());
+    if (no <= 64) {
+        // staged sub-blocks of up to 64 x 65 doubles (33 KB of shared memory)
+        const size_t smem = sizeof(double) * (size_t)(no + 1) * (size_t)no;
+        energy_pairs_kernel<<<nb, 256, smem, ex.stream>>>(t1, t2, g_ovov, (int)no, nv, nv * (nv + 1) / 2, part.d());
+    } else {
+        energy_partial_kernel<<<nb, 256, 0, ex.stream>>>(t1, t2, g_ovov, no, nv, part.d());
+    }
     sum_partial_kernel<<<1, 256, 0, ex.stream>>>(part.d(), nb, add, d_out);
     ex.launches += 2;
     CU_CHECK(cudaGetLastError());

@@ -45,6 +45,36 @@ __global__ void permute_simple_kernel(PermArgs a, int64_t total, double alpha, c
     }
 }
 
+// Rows of the output-fastest dim (dim 0, at least 16 long): a warp takes one row, so the int64
+// div/mod chain that locates a row in the other dims runs once per row instead of once per element,
+// and both sides stream along dim 0 (this kernel serves permutations whose input-fastest dim is dim
+// 0 as well, or whose other dims are too short for the tiled transpose).
+__global__ void permute_rows_kernel(PermArgs a, int64_t nrows, double alpha, const double *__restrict__ in,
+                                    double beta, double *__restrict__ out) {
+    const int64_t n0 = a.n[0], si0 = a.si[0], so0 = a.so[0];
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.y + threadIdx.y; row < nrows;
+         row += (int64_t)gridDim.x * blockDim.y) {
+        int64_t r = row, oi = 0, oo = 0;
+#pragma unroll
+        for (int d = 1; d < MAXD; d++) {
+            if (d < a.nd) {
+                const int64_t q = r / a.n[d];
+                const int64_t i = r - q * a.n[d];
+                r = q;
+                oi += i * a.si[d];
+                oo += i * a.so[d];
+            }
+        }
+        const double *src = in + oi;
+        double *dst = out + oo;
+        if (beta == 0.0) {
+            for (int64_t i0 = threadIdx.x; i0 < n0; i0 += 32) dst[i0 * so0] = alpha * src[i0 * si0];
+        } else {
+            for (int64_t i0 = threadIdx.x; i0 < n0; i0 += 32) dst[i0 * so0] = alpha * src[i0 * si0] + beta * dst[i0 * so0];
+        }
+    }
+}
+
 // 32x32 tile over (p = input-fastest dim, q = output-fastest dim); the remaining dims
 // are flattened into the z loop.  Dims 2.. of `a` are the batch dims.
 __global__ void permute_tiled_kernel(PermArgs a, int64_t nbatch, double alpha, const double *__restrict__ in,
@@ -155,7 +185,13 @@ void permute_add(Exec &ex, double alpha, const TV &in, double beta, const TV &ou
             a.si[k] = in.s[dims[k]];
             a.so[k] = out.s[dims[k]];
         }
-        permute_simple_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(a, total, alpha, in.p, beta, out.p);
+        if (a.n[0] >= 16) {
+            const int64_t nrows = total / a.n[0];
+            const int blocks = (int)std::min<int64_t>((nrows + 7) / 8, 148 * 64);
+            permute_rows_kernel<<<blocks, dim3(32, 8), 0, ex.stream>>>(a, nrows, alpha, in.p, beta, out.p);
+        } else {
+            permute_simple_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(a, total, alpha, in.p, beta, out.p);
+        }
     }
     ex.launches++;
     CU_CHECK(cudaGetLastError());

@@ -1,6 +1,6 @@
-"""The benchmark's JSON contract on the CPU: the reference arm (the oracle timed on the host cores)
-prints one line with the benchmark's metric, its own cpu_baseline and an e2e record without device
-copies; the roofline traffic comes from the committed launch list."""
+"""The benchmark's JSON contract on the CPU: the reference arm (the CPU restatement of eT's algorithm
+timed on the host cores) prints one line with the benchmark's metric, its own cpu_baseline and an e2e
+record without device copies; the roofline traffic comes from the committed launch list."""
 
 import json
 import os
@@ -24,20 +24,23 @@ def test_roofline_traffic_comes_from_the_committed_launch_list():
 
 
 def test_reference_arm_prints_one_contract_line():
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0", "--cpu-seconds", "1", "--cpu-o", "4", "--cpu-v", "24", "--cpu-J", "60"],
+    """At a small shape (the default is the benchmark's o=32, v=320, N_J=1200): one line whose steps
+    are the iterations actually timed."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "20",
+                        "--warmup", "5", "--cpu-iterations", "2", "--n-o", "4", "--n-v", "24", "--n-J", "60"],
                        capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
-    assert d["impl"] == "reference" and d["unit"] == "TFLOP/s" and d["higher_is_better"] is True
+    assert d["impl"] == "reference" and d["unit"] == "s/iter" and d["higher_is_better"] is False
     assert d["metric"] == _bench().METRIC
     assert d["value"] > 0 and d["value"] == d["cpu_baseline"]["value"] == d["e2e"]["value"]
     cb = d["cpu_baseline"]
-    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"] and cb["cpu_model"]
+    assert d["steps"] == cb["iterations_timed"] == 2 and d["warmup"] == 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
-    assert "workload" in d["config"]
+    assert d["config"]["n_o"] == 4 and "workload" in d["config"]
 
 
 def test_synthetic_cholesky_vectors_in_et_layout():
