@@ -666,19 +666,26 @@ def run_gemm(args):
     launch (256^3) is a warm-up, so profilers skip one launch."""
     from et_b200 import CCSD
     m, n, k = args.gemm_m, args.gemm_n, args.gemm_k
+    digits = args.gemm_digits
+    mode = digits if digits else True
     rng = np.random.default_rng(0)
     A = np.asfortranarray(rng.standard_normal((m, k)))
     B = np.asfortranarray(rng.standard_normal((k, n)))
     with CCSD(2, 3, 4) as ctx:
-        ctx.selftest_gemm(A[:256, :256], B[:256, :256], mixed=True)
+        ctx.selftest_gemm(A[:256, :256], B[:256, :256], mixed=mode)
         ctx.set_profiling(True)
         for _ in range(args.gemm_reps):
-            ctx.selftest_gemm(A, B, mixed=True)
-        nl, ms, fl = ctx.gemm_profile()
+            ctx.selftest_gemm(A, B, mixed=mode)
+        nl, ms, fl = ctx.digit_gemm_profile() if digits else ctx.gemm_profile()
     per = ms / max(nl, 1)
-    print(json.dumps({"workload": "tensor-core GEMM", "m": m, "n": n, "k": k, "launches": nl,
-                      "ms_per_launch": round(per, 4), "issued_tflops": round(fl / nl / (per * 1e-3) / 1e12, 1),
-                      "fp64_equivalent_tflops": round(2.0 * m * n * k / (per * 1e-3) / 1e12, 1)}), flush=True)
+    out = {"workload": "tensor-core GEMM", "kernel": "ozaki_gemm_kernel (int8 digits)" if digits else
+           "split_bf16_gemm_kernel", "m": m, "n": n, "k": k, "launches": nl, "ms_per_launch": round(per, 4),
+           "fp64_equivalent_tflops": round(2.0 * m * n * k / (per * 1e-3) / 1e12, 1)}
+    if digits:
+        out.update({"digits": digits, "int8_tops_issued": round(fl / nl / (per * 1e-3) / 1e12, 1)})
+    else:
+        out["issued_tflops"] = round(fl / nl / (per * 1e-3) / 1e12, 1)
+    print(json.dumps(out), flush=True)
 
 
 def host_cpu():
@@ -760,6 +767,8 @@ def main():
     p.add_argument("--gemm-n", dest="gemm_n", type=int, default=10240)
     p.add_argument("--gemm-k", dest="gemm_k", type=int, default=10240)
     p.add_argument("--gemm-reps", dest="gemm_reps", type=int, default=3)
+    p.add_argument("--gemm-digits", dest="gemm_digits", type=int, default=0,
+                   help="gemm workload: 4..7 = the FP64-accurate int8 digit GEMM, 0 = the split-BF16 GEMM")
     p.add_argument("--roots", type=int, default=12)
     p.add_argument("--directions", type=int, default=256)
     p.add_argument("--systems", type=int, default=64)

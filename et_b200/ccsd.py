@@ -55,7 +55,7 @@ class SolverOptions(ctypes.Structure):
     _fields_ = [("max_iterations", ctypes.c_int32), ("diis_dimension", ctypes.c_int32),
                 ("omega_threshold", ctypes.c_double), ("energy_threshold", ctypes.c_double),
                 ("refine_threshold", ctypes.c_double), ("refine_target", ctypes.c_double),
-                ("reserved", ctypes.c_int32 * 6)]
+                ("refresh_digits", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 class BatchSystem(ctypes.Structure):
@@ -105,6 +105,8 @@ SIGNATURES = {
     "ccsd_gpu_stats": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP]),
     "ccsd_gpu_set_graphs": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_set_fp64_integrals": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "ccsd_gpu_set_fp64_digits": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_double]),
+    "ccsd_gpu_digit_gemm_profile": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _DP, _DP]),
     "ccsd_gpu_set_term_timing": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "ccsd_gpu_term_timing_report": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int64,
                                                    ctypes.POINTER(ctypes.c_int64)]),
@@ -367,15 +369,18 @@ class CCSD:
         return out, it.value
 
     def solve_ground_state(self, *, max_iterations=100, diis_dimension=8, omega_threshold=1e-5,
-                           energy_threshold=1e-5, refine_threshold=1e-4, refine_target=0.0,
+                           energy_threshold=1e-5, refine_threshold=1e-4, refine_target=0.0, refresh_digits=0,
                            raise_on_failure=True):
         """run_diis_cc_gs on the device; returns (energy, iterations, history[(E, |Omega|)], status).
 
         Mixed precision only: ``refine_threshold`` is |Omega| of the first FP64 refresh,
-        ``refine_target`` the true residual the refreshes aim at (0: ``omega_threshold``)."""
+        ``refine_target`` the true residual the refreshes aim at (0: ``omega_threshold``),
+        ``refresh_digits`` the arithmetic of the FP64 evaluations (4..7: int8 digit GEMM on the
+        tensor cores, -1: cuBLAS DGEMM, 0: the library default)."""
         opt = SolverOptions(max_iterations=max_iterations, diis_dimension=diis_dimension,
                             omega_threshold=omega_threshold, energy_threshold=energy_threshold,
-                            refine_threshold=refine_threshold, refine_target=refine_target)
+                            refine_threshold=refine_threshold, refine_target=refine_target,
+                            refresh_digits=refresh_digits)
         e = ctypes.c_double()
         it = ctypes.c_int32()
         hist = np.zeros(2 * max_iterations)
@@ -392,6 +397,20 @@ class CCSD:
         """FP64 residual from resident integrals of the untransformed vectors (default, when they
         fit) or from T1-transformed integrals formed in every call (eT's omega_ccsd_a2)."""
         self._check(self.lib.ccsd_gpu_set_fp64_integrals(self.ctx, 1 if resident else 0))
+
+    def set_fp64_digits(self, digits: int, min_flops: float = 0.0):
+        """FP64 products of at least ``min_flops`` (0: 1e10) on the int8 tensor cores with 4..7
+        digits per operand (0: cuBLAS DGEMM)."""
+        self._check(self.lib.ccsd_gpu_set_fp64_digits(self.ctx, int(digits), float(min_flops)))
+
+    def digit_gemm_profile(self):
+        """(launches, device ms, int8 ops) of the digit GEMM since profiling was enabled."""
+        n = ctypes.c_int64()
+        ms = ctypes.c_double()
+        ops = ctypes.c_double()
+        self._check(self.lib.ccsd_gpu_digit_gemm_profile(self.ctx, ctypes.byref(n), ctypes.byref(ms),
+                                                         ctypes.byref(ops)))
+        return n.value, ms.value, ops.value
 
     def set_term_timing(self, on: bool):
         """Per-term device times under eT's timing labels; on starts a fresh log."""

@@ -8,6 +8,7 @@
 #include "autotune.cuh"
 #include "ccsd.cuh"
 #include "mixed_gemm.cuh"
+#include "ozaki_gemm.cuh"
 #include "ccsd_kernels.cuh"
 #include "tensor_ops.cuh"
 
@@ -336,6 +337,31 @@ int ccsd_gpu_set_graphs(void *ctx, int32_t on) {
     });
 }
 
+int ccsd_gpu_set_fp64_digits(void *ctx, int32_t digits, double min_flops) {
+    return guarded(ctx, [&](Context &c) {
+        REQUIRE(digits == 0 || (digits >= 4 && digits <= 7), CCSD_GPU_EINVAL, "digits must be 0 or 4..7");
+        if (digits != c.ex.fp64_digits) c.drop_jacobian();
+        c.ex.fp64_digits = digits;
+        c.ex.fp64_digits_min_flops = min_flops > 0.0 ? min_flops : 1e10;
+    });
+}
+
+int ccsd_gpu_digit_gemm_profile(void *ctx, int64_t *launches, double *device_ms, double *int8_ops) {
+    return guarded(ctx, [&](Context &c) {
+        CU_CHECK(cudaStreamSynchronize(c.ex.stream));
+        double ms = 0.0, ops = 0.0;
+        for (size_t i = 0; i < c.prof.oz_events.size(); i++) {
+            float t = 0.f;
+            CU_CHECK(cudaEventElapsedTime(&t, c.prof.oz_events[i].first, c.prof.oz_events[i].second));
+            ms += t;
+            ops += c.prof.oz_ops[i];
+        }
+        if (launches) *launches = (int64_t)c.prof.oz_events.size();
+        if (device_ms) *device_ms = ms;
+        if (int8_ops) *int8_ops = ops;
+    });
+}
+
 int ccsd_gpu_set_fp64_integrals(void *ctx, int32_t resident) {
     return guarded(ctx, [&](Context &c) {
         CU_CHECK(cudaStreamSynchronize(c.ex.stream));
@@ -432,8 +458,11 @@ int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t tra
         h2d(c, dA.d(), A, na);
         h2d(c, dB.d(), B, nb);
         h2d(c, dC.d(), C, nc);
-        REQUIRE(mixed >= 0 && mixed <= 2, CCSD_GPU_EINVAL, "mixed must be 0, 1 or 2");
-        if (mixed) {
+        REQUIRE((mixed >= 0 && mixed <= 2) || (mixed >= 4 && mixed <= 7), CCSD_GPU_EINVAL,
+                "mixed must be 0, 1, 2 or 4..7 (int8 digits)");
+        if (mixed >= 4) {
+            ccsd::ozaki_gemm(c.ex, transA, transB, m, n, k, alpha, dA.d(), lda, dB.d(), ldb, beta, dC.d(), ldc, mixed);
+        } else if (mixed) {
             const int planes = c.ex.planes;
             c.ex.planes = mixed == 2 ? 3 : 2;
             try {

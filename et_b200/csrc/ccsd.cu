@@ -660,6 +660,12 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     const double ethr = o ? o->energy_threshold : 1e-5;
     const double refine = o && o->refine_threshold > 0 ? o->refine_threshold : 1e-4;
     const double rtarget = o && o->refine_target > 0 ? o->refine_target : othr;
+    const int rdig = o ? o->refresh_digits : 0;
+    REQUIRE(rdig == 0 || rdig == -1 || (rdig >= 4 && rdig <= 7), CCSD_GPU_EINVAL,
+            "refresh_digits must be 0 (default), -1 (DGEMM) or 4..7");
+    // arithmetic of the FP64 evaluations: the option, else the context's setting (ccsd_gpu_set_fp64_digits)
+    const int user_digits = ex.fp64_digits;
+    const int fp64_digits = rdig > 0 ? rdig : (rdig < 0 ? 0 : user_digits);
     cudaStream_t s = ex.stream;
     orbital_differences(ex, eps.d(), no, nv, epsdiff.d());
     DBuf omega_v = dalloc(namp, s);
@@ -677,12 +683,13 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     struct Restore {
         Exec &ex;
         Prec prec;
-        int planes;
+        int planes, digits;
         ~Restore() {
             ex.prec = prec;
             ex.planes = planes;
+            ex.fp64_digits = digits;
         }
-    } restore{ex, ex.prec, ex.planes};
+    } restore{ex, ex.prec, ex.planes, ex.fp64_digits};
     // Mixed precision with defect correction: Omega~(t) = Omega_mixed(t) + c, where
     // c = Omega_fp64(t_c) - Omega_mixed(t_c) is refreshed by one FP64 evaluation at a time.  The mixed
     // error d(t) = Omega_fp64(t) - Omega_mixed(t) is mostly frozen, but the truncating FP32
@@ -747,7 +754,9 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         last_check = it;
         CU_CHECK(cudaMemcpyAsync(moved_v.d(), omega_v.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
         ex.prec = Prec::FP64;
+        ex.fp64_digits = fp64_digits;
         omega(omega_v.d());
+        ex.fp64_digits = user_digits;
         ex.prec = user;
         CU_CHECK(cudaMemcpyAsync(corr.d(), omega_v.d(), sizeof(double) * namp, cudaMemcpyDeviceToDevice, s));
         axpby(ex, namp, -1.0, om_mixed.d(), 1.0, corr.d());
@@ -774,8 +783,12 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         bool exact = !mixed;
         if (!mixed || fp64_final) {
             exact = true;
-            if (fp64_final) ex.prec = Prec::FP64;
+            if (fp64_final) {
+                ex.prec = Prec::FP64;
+                ex.fp64_digits = fp64_digits;
+            }
             omega(omega_v.d());
+            ex.fp64_digits = user_digits;
             ex.prec = user;
             nrm = norm_of(omega_v.d());
         } else {

@@ -119,13 +119,19 @@ struct GemmProfile {
     bool on = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     std::vector<double> flops;    // tensor flops issued per launch (3 products x 2mnk)
+    // the int8 digit GEMM of FP64-accurate evaluations: its launches and int8 ops issued
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> oz_events;
+    std::vector<double> oz_ops;
     void clear() {
-        for (auto &e : events) {
-            cudaEventDestroy(e.first);
-            cudaEventDestroy(e.second);
-        }
+        for (auto *v : {&events, &oz_events})
+            for (auto &e : *v) {
+                cudaEventDestroy(e.first);
+                cudaEventDestroy(e.second);
+            }
         events.clear();
         flops.clear();
+        oz_events.clear();
+        oz_ops.clear();
     }
     ~GemmProfile() { clear(); }
 };
@@ -165,6 +171,10 @@ struct Exec {
     int *gemm_err = nullptr;     // device error word of this caller's tensor-core GEMMs (one per context)
     long long wait_cycles = 0;   // bound of the GEMM's barrier waits (<= 0: the default, ~2 s)
     int stall_test = 0;          // diagnostics only: the next GEMMs withhold one stage of loads
+    // FP64 products of at least 1e10 flops (and 256 in every dimension) run on the int8 tensor
+    // cores with this many 7-bit digits per operand (ozaki_gemm); 0 = cuBLAS DGEMM
+    int fp64_digits = 0;
+    double fp64_digits_min_flops = 1e10;
 };
 
 // Times the enclosing scope as one term of ex.terms (nothing happens unless the log is on, and

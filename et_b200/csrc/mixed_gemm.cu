@@ -24,8 +24,11 @@
 #include <mutex>
 
 #include "mixed_gemm.cuh"
+#include "tc_common.cuh"
 
 namespace ccsd {
+
+using namespace tc;
 
 namespace {
 
@@ -61,86 +64,6 @@ using ModeX3 = Mode<2, 256>;
 using ModeX6 = Mode<3, 128>;
 static_assert(ModeX3::STAGE_BYTES == 96 * 1024 && ModeX6::STAGE_BYTES == 96 * 1024, "stage size");
 static_assert(B_ROW_PAD % ModeX3::BN == 0 && B_ROW_PAD % ModeX6::BN == 0, "B padding");
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// the first bounded wait that runs out names the error; later ones keep it
-__device__ __forceinline__ void record_error(int *err, int code) { atomicCAS(err, 0, code); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// bounded wait for the completion of the phase with the given parity; false after `limit` cycles
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
-    uint32_t addr = smem_u32(bar);
-    const long long t0 = clock64();
-    while (true) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if (clock64() - t0 > limit) return false;
-    }
-}
-
-__device__ __forceinline__ void tma_load_3d(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1,
-                                            int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
-// K-major operand tile, 128-byte swizzle: 8-row x 128 B atoms stacked along M/N (SBO = 1024 B)
-__device__ __forceinline__ uint64_t smem_desc(const void *tile, uint32_t k_byte_offset) {
-    uint64_t addr = smem_u32(tile) + k_byte_offset;
-    uint64_t d = 0;
-    d |= (addr >> 4) & 0x3FFFull;              // start address
-    d |= (uint64_t)(16 >> 4) << 16;            // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;          // stride byte offset
-    d |= 1ull << 46;                           // descriptor version (sm_100)
-    d |= 2ull << 61;                           // SWIZZLE_128B
-    return d;
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-}
 
 }  // namespace
 
@@ -497,24 +420,6 @@ __global__ void sum_splits_kernel(const double *__restrict__ P, int splits, int6
         double *dst = C + r + ldc * c;
         *dst = beta != 0.0 ? beta * *dst + acc : acc;
     }
-}
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    REQUIRE(fn != nullptr, CCSD_GPU_ECUDA, "cuTensorMapEncodeTiled unavailable");
-    return fn;
 }
 
 // planes x rows x K tensor of bf16, box (BK, box_rows, 1); rows beyond `rows` read as zero

@@ -1,0 +1,462 @@
+// FP64-accurate GEMM on the int8 tensor cores of sm_100a (Ozaki's error-free slicing).
+//
+// Every row r of op(A) is scaled by 2^-ea_r (ea_r: the exponent of the power of two just above
+// max_k |A_rk|) and cut into S digits of 7 bits,
+//     A_rk = 2^ea_r sum_t DA_t[r,k] 2^(-7(t+1)),   DA_t integers in [-127, 127],
+// exactly up to the truncation of the last digit (relative 2^-7S); the columns of op(B) the same
+// with eb_c.  Then
+//     C_rc = 2^(ea_r + eb_c) sum_{t,u} 2^(-7(t+u+2)) sum_k DA_t[r,k] DB_u[k,c],
+// and every digit product sum_k is exact in int32: |d d'| <= 127^2, and an accumulator takes at
+// most 7 products (one diagonal d = t + u) over a K chunk of at most 16384, 7 * 16384 * 127^2 < 2^31.
+// Products with t + u <= S - 1 are kept; the dropped ones lie below the last digit of either
+// operand.  With S = 7 the 28 products reproduce an FP64 GEMM to ~1e-14 of the largest output.
+//
+// Kernel: persistent, warp specialised like the split-BF16 GEMM (warp 0 issues TMA loads, warp 1
+// issues tcgen05.mma.kind::i8 with int32 accumulation in TMEM, warps 2-5 drain), 128 x 128 output
+// tiles, K blocks of 64 int8 (64-byte swizzled rows).  A stage holds the digit tiles of both
+// operands for one K block (up to 7 + 7 tiles of 8 KB), two stages.  The diagonals of a tile are
+// accumulated in passes of at most four (4 x 128 TMEM columns = all 512): pass 0 takes d = 0..3
+// (digits 0..3 of both operands), pass 1 takes d = 4..S-1 (all digits).  The epilogue adds
+// 2^(-7(d+2)) acc_d in FP64, scales by alpha 2^(ea_r + eb_c) and accumulates into the FP64 output;
+// one CTA takes all units (K chunk, pass) of a tile in order, so the sum is deterministic.  Every
+// mbarrier wait is bounded and reports to the caller's error word, as in the split-BF16 GEMM.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "ozaki_gemm.cuh"
+#include "tc_common.cuh"
+
+namespace ccsd {
+
+using namespace tc;
+
+namespace {
+
+constexpr int OBM = 128, OBN = 128, OBK = 64;            // tile; K block = one 64-byte row of int8
+constexpr int SLOTS = 7;                                 // digit tiles per operand in a stage
+constexpr int OSTAGES = 2;
+constexpr int OTHREADS = 192, OEPI = 128;
+constexpr int A_TILE = OBM * OBK, B_TILE = OBN * OBK;    // bytes
+constexpr int OSTAGE_BYTES = SLOTS * (A_TILE + B_TILE);
+constexpr int OSMEM = OSTAGES * OSTAGE_BYTES + 1024 + 256;
+constexpr uint32_t OTMEM_COLS = 512;                     // four 128-column int32 accumulators
+constexpr int MAX_DIAG_PER_PASS = 4;
+constexpr int OK_CHUNK = 16384;                          // K elements per exact int32 accumulation
+constexpr long long OWAIT_CYCLES = 4000000000ll;
+// kind::i8 instruction descriptor: S8 x S8 -> S32, both K-major, M = 128, N = 128
+constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OBN >> 3) << 17) |
+                              ((uint32_t)(OBM >> 4) << 24);
+static_assert(OSMEM <= 232448, "shared memory of the Ozaki GEMM");
+static_assert(7 * OK_CHUNK * 127 * 127 < 2147483647ll, "int32 accumulation must stay exact");
+constexpr int ERR_PRODUCER = 1, ERR_MMA_FULL = 2, ERR_EPILOGUE = 3, ERR_MMA_ACC = 4, ERR_DONE = 5, ERR_DRAIN = 6;
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(IDESC_I8), "r"(accumulate));
+}
+
+struct OzMap {
+    int num_mt, num_nt, group_m;
+    int nk_all;          // K blocks of 64
+    int kc;              // K blocks per chunk
+    int nchunks;
+    int digits;          // S
+    int npass;           // 1 (S <= 4) or 2
+    int M, N;
+    long long ldc;
+    double alpha, beta;
+    double *C;
+    const int *ea, *eb;  // row exponents of op(A), column exponents of op(B)
+    int *err;
+    long long wait_cycles;
+    __device__ __forceinline__ void tile(int t, int &m0, int &n0) const {
+        const int per_group = group_m * num_nt;
+        const int grp = t / per_group, in = t - grp * per_group;
+        const int first_m = grp * group_m;
+        const int gsz = min(group_m, num_mt - first_m);
+        m0 = (first_m + in % gsz) * OBM;
+        n0 = (in / gsz) * OBN;
+    }
+    // diagonals [d0, d1) of pass p and the digits they need
+    __device__ __forceinline__ void pass(int p, int &d0, int &d1, int &nd) const {
+        d0 = p == 0 ? 0 : MAX_DIAG_PER_PASS;
+        d1 = p == 0 ? min(digits, MAX_DIAG_PER_PASS) : digits;
+        nd = min(d1, digits);   // digits 0..nd-1 of both operands (t, u <= d1 - 1)
+    }
+};
+
+__global__ void __launch_bounds__(OTHREADS, 1)
+ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzMap map,
+                  int num_tiles) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + OSTAGES * OSTAGE_BYTES);
+    uint64_t *empty = full + OSTAGES;
+    uint64_t *acc_full = empty + OSTAGES;
+    uint64_t *acc_empty = acc_full + 1;
+    uint64_t *done = acc_empty + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < OSTAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, OEPI);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(OTMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: for every (tile, chunk, pass) unit, the digit tiles of each K block
+            int g = 0;
+            int issued[OSTAGES] = {};
+            for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
+                int m0, n0;
+                map.tile(t, m0, n0);
+                for (int c = 0; c < map.nchunks && !*abort_flag; c++) {
+                    const int kb0 = c * map.kc, kb1 = min(map.nk_all, kb0 + map.kc);
+                    for (int p = 0; p < map.npass && !*abort_flag; p++) {
+                        int d0, d1, nd;
+                        map.pass(p, d0, d1, nd);
+                        for (int kb = kb0; kb < kb1; kb++, g++) {
+                            const int s = g % OSTAGES;
+                            if (!mbar_wait(&empty[s], ((g / OSTAGES) & 1) ^ 1, map.wait_cycles) || *abort_flag) {
+                                record_error(map.err, ERR_PRODUCER);
+                                *abort_flag = 1;
+                                break;
+                            }
+                            issued[s]++;
+                            uint8_t *st = smem + s * OSTAGE_BYTES;
+                            mbar_expect_tx(&full[s], (uint32_t)nd * (A_TILE + B_TILE));
+                            for (int q = 0; q < nd; q++) {
+                                tma_load_3d(&tmA, &full[s], st + q * A_TILE, kb * OBK, m0, q);
+                                tma_load_3d(&tmB, &full[s], st + SLOTS * A_TILE + q * B_TILE, kb * OBK, n0, q);
+                            }
+                        }
+                    }
+                }
+            }
+            for (int s = 0; s < OSTAGES; s++)
+                if (issued[s] && !mbar_wait(&full[s], (issued[s] - 1) & 1, map.wait_cycles))
+                    record_error(map.err, ERR_DRAIN);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer: one unit at a time into the (up to four) diagonal accumulators
+            int g = 0, uc = 0;
+            for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
+                for (int c = 0; c < map.nchunks && !*abort_flag; c++) {
+                    const int kb0 = c * map.kc, kb1 = min(map.nk_all, kb0 + map.kc);
+                    for (int p = 0; p < map.npass && !*abort_flag; p++, uc++) {
+                        int d0, d1, nd;
+                        map.pass(p, d0, d1, nd);
+                        if (!mbar_wait(acc_empty, (uc & 1) ^ 1, map.wait_cycles)) {
+                            record_error(map.err, ERR_MMA_ACC);
+                            *abort_flag = 1;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        for (int kb = kb0; kb < kb1; kb++, g++) {
+                            const int s = g % OSTAGES;
+                            if (!mbar_wait(&full[s], (g / OSTAGES) & 1, map.wait_cycles) || *abort_flag) {
+                                record_error(map.err, ERR_MMA_FULL);
+                                *abort_flag = 1;
+                                break;
+                            }
+                            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                            const uint8_t *st = smem + s * OSTAGE_BYTES;
+#pragma unroll
+                            for (int kk = 0; kk < OBK / 32; kk++) {
+                                const uint32_t ko = kk * 32;   // 32 int8 = 32 bytes per MMA
+                                for (int d = d0; d < d1; d++) {
+                                    const uint32_t acc = tmem + (uint32_t)((d - d0) * OBN);
+                                    const int tlo = max(0, d - (map.digits - 1)), thi = min(d, map.digits - 1);
+                                    for (int tq = tlo; tq <= thi; tq++) {
+                                        const int uq = d - tq;
+                                        const uint32_t accumulate = (kb > kb0 || kk > 0 || tq > tlo) ? 1u : 0u;
+                                        mma_i8(acc, smem_desc_k<64>(st + tq * A_TILE, ko),
+                                               smem_desc_k<64>(st + SLOTS * A_TILE + uq * B_TILE, ko), accumulate);
+                                    }
+                                }
+                            }
+                            mma_commit(&empty[s]);
+                        }
+                        mma_commit(acc_full);
+                    }
+                }
+            }
+            mma_commit(done);
+        }
+    } else {
+        // epilogue: warp w drains TMEM lanes 32 (w % 4) .. +31, one output row per thread
+        const int quarter = warp & 3;
+        int uc = 0;
+        bool aborted = false;
+        for (int t = blockIdx.x; t < num_tiles && !aborted; t += gridDim.x) {
+            int m0, n0;
+            map.tile(t, m0, n0);
+            const int row = m0 + quarter * 32 + lane;
+            const double row_scale = row < map.M ? map.alpha * exp2((double)map.ea[row]) : 0.0;
+            for (int c = 0; c < map.nchunks && !aborted; c++) {
+                for (int p = 0; p < map.npass; p++, uc++) {
+                    int d0, d1, nd;
+                    map.pass(p, d0, d1, nd);
+                    bool ok = !*abort_flag && mbar_wait(acc_full, uc & 1, map.wait_cycles);
+                    __syncwarp();
+                    if (!ok || *abort_flag) {
+                        record_error(map.err, ERR_EPILOGUE);
+                        *abort_flag = 1;
+                        aborted = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const bool first = (c == 0 && p == 0);
+                    const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll 1
+                    for (int cc = 0; cc < OBN; cc += 16) {
+                        double v[16];
+#pragma unroll
+                        for (int j = 0; j < 16; j++) v[j] = 0.0;
+                        for (int d = d0; d < d1; d++) {
+                            uint32_t r[16];
+                            tmem_ld16u(base + (uint32_t)((d - d0) * OBN + cc), r);
+                            const double w = exp2(-7.0 * (double)(d + 2));
+#pragma unroll
+                            for (int j = 0; j < 16; j++) v[j] += w * (double)(int)r[j];
+                        }
+                        if (row < map.M) {
+                            double *out = map.C + (long long)(n0 + cc) * map.ldc + row;
+                            double old[16];
+#pragma unroll
+                            for (int j = 0; j < 16; j++) {
+                                const bool in = n0 + cc + j < map.N;
+                                old[j] = (in && (!first || map.beta != 0.0)) ? __ldcg(out + (long long)j * map.ldc) : 0.0;
+                            }
+#pragma unroll
+                            for (int j = 0; j < 16; j++) {
+                                const int col = n0 + cc + j;
+                                if (col < map.N) {
+                                    const double x = row_scale * exp2((double)map.eb[col]) * v[j];
+                                    out[(long long)j * map.ldc] = first ? x + map.beta * old[j] : x + old[j];
+                                }
+                            }
+                        }
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(acc_empty)) : "memory");
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (!mbar_wait(done, 0, map.wait_cycles)) record_error(map.err, ERR_DONE);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(OTMEM_COLS));
+    }
+}
+
+// Row exponents of a strided FP64 view (element (r, k) at src[r sr + k sk]): e[r] = the exponent of
+// the power of two just above max_k |x_rk| (frexp), by atomicMax over K slices of 32 x 32 tiles
+// (e must start below any exponent: all-zero rows keep the start value).
+__global__ void oz_rowexp_kernel(const double *__restrict__ src, long long sr, long long sk, int R, int K,
+                                 int *__restrict__ e) {
+    __shared__ double tile[32][33];
+    __shared__ double red[8][33];
+    const int r0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
+    const bool k_fast = (sk == 1);
+    double m = 0.0;
+    for (int k0 = blockIdx.y * 32; k0 < K; k0 += gridDim.y * 32) {
+        for (int i = ty; i < 32; i += 8) {
+            int r, k;
+            if (k_fast) {
+                r = r0 + i;
+                k = k0 + tx;
+            } else {
+                r = r0 + tx;
+                k = k0 + i;
+            }
+            const double x = (r < R && k < K) ? src[(long long)r * sr + (long long)k * sk] : 0.0;
+            if (k_fast) tile[i][tx] = x;
+            else tile[tx][i] = x;
+        }
+        __syncthreads();
+        for (int i = ty; i < 32; i += 8) m = fmax(m, fabs(tile[tx][i]));
+        __syncthreads();
+    }
+    red[ty][tx] = m;
+    __syncthreads();
+    if (ty == 0 && r0 + tx < R) {
+        for (int j = 1; j < 8; j++) m = fmax(m, red[j][tx]);
+        if (m > 0.0) {
+            int ex;
+            frexp(m, &ex);
+            atomicMax(&e[r0 + tx], ex);
+        }
+    }
+}
+
+// Digits of the scaled rows: x 2^-e = sum_t d_t 2^(-7(t+1)), d_t = trunc of the remaining fraction
+// times 128 (exact in FP64), written as int8 planes [digit][Rp][Kp], K-major, zero padded.
+__global__ void oz_digits_kernel(const double *__restrict__ src, long long sr, long long sk, int R, int K, int Rp,
+                                 int Kp, int digits, const int *__restrict__ e, int8_t *__restrict__ out) {
+    __shared__ double tile[32][33];
+    const int r0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
+    const bool k_fast = (sk == 1);
+    const size_t plane = (size_t)Rp * Kp;
+    for (int k0 = blockIdx.y * 32; k0 < Kp; k0 += gridDim.y * 32) {
+        for (int i = ty; i < 32; i += 8) {
+            int r, k;
+            if (k_fast) {
+                r = r0 + i;
+                k = k0 + tx;
+            } else {
+                r = r0 + tx;
+                k = k0 + i;
+            }
+            const double x = (r < R && k < K) ? src[(long long)r * sr + (long long)k * sk] : 0.0;
+            if (k_fast) tile[i][tx] = x;
+            else tile[tx][i] = x;
+        }
+        __syncthreads();
+        for (int i = ty; i < 32; i += 8) {
+            const int r = r0 + i, k = k0 + tx;
+            if (r < Rp && k < Kp) {
+                const int er = (r < R) ? e[r] : 0;
+                double y = (r < R && er > -1100) ? ldexp(tile[i][tx], -er) : 0.0;   // |y| < 1
+                const size_t o = (size_t)r * Kp + k;
+                for (int t = 0; t < digits; t++) {
+                    y *= 128.0;
+                    const double d = trunc(y);
+                    y -= d;
+                    out[t * plane + o] = (int8_t)(int)d;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// digits x rows x Kp tensor of int8, box (64, 128, 1), 64-byte swizzle
+CUtensorMap make_i8_map(void *base, int64_t rows, int64_t Kp, int64_t plane_stride, int planes) {
+    CUtensorMap m;
+    REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, CCSD_GPU_EINVAL, "tensor map base must be 16-byte aligned");
+    REQUIRE(Kp % 64 == 0 && plane_stride % 16 == 0, CCSD_GPU_EINVAL, "int8 digit planes: bad padding");
+    cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)planes};
+    cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)plane_stride};
+    cuuint32_t box[3] = {OBK, 128, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    REQUIRE(r == CUDA_SUCCESS, CCSD_GPU_ECUDA, "cuTensorMapEncodeTiled (int8) failed: " + std::to_string((int)r));
+    return m;
+}
+
+int num_sms() {
+    int dev = 0, v = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    CU_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    return v;
+}
+
+// rows of a strided view -> exponents e[R] and digits [digits][Rp][Kp]
+void digits_of(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
+               int digits, int *e, int8_t *out) {
+    // start every exponent below any frexp exponent: 0x80 bytes = -2139062144
+    CU_CHECK(cudaMemsetAsync(e, 0x80, sizeof(int) * (size_t)Rp, ex.stream));
+    const int64_t rb = (R + 31) / 32;
+    // enough blocks over K to fill the GPU when there are few row blocks
+    const int64_t kb = std::max<int64_t>(1, std::min<int64_t>((K + 31) / 32, (4 * 148 + rb - 1) / rb));
+    oz_rowexp_kernel<<<dim3((unsigned)rb, (unsigned)std::min<int64_t>(kb, 65535)), dim3(32, 8), 0, ex.stream>>>(
+        src, sr, sk, (int)R, (int)K, e);
+    oz_digits_kernel<<<dim3((unsigned)(Rp / 32), (unsigned)std::min<int64_t>(Kp / 32, 65535)), dim3(32, 8), 0,
+                       ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, digits, e, out);
+    ex.launches += 2;
+    CU_CHECK(cudaGetLastError());
+}
+
+}  // namespace
+
+void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
+                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, int digits) {
+    REQUIRE(m > 0 && n > 0 && k > 0, CCSD_GPU_EINVAL, "ozaki_gemm: empty product");
+    REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "ozaki_gemm: size too large");
+    REQUIRE(digits >= 2 && digits <= SLOTS, CCSD_GPU_EINVAL, "ozaki_gemm: 2 to 7 digits");
+    REQUIRE(ex.gemm_err != nullptr, CCSD_GPU_EINVAL, "ozaki_gemm: no error word");
+    const int64_t Kp = round_up(k, OBK), Mp = round_up(m, OBM), Np = round_up(n, OBN);
+    DBuf da(sizeof(int8_t) * (size_t)digits * Mp * Kp, ex.stream), db(sizeof(int8_t) * (size_t)digits * Np * Kp, ex.stream);
+    DBuf ea(sizeof(int) * (size_t)Mp, ex.stream), eb(sizeof(int) * (size_t)Np, ex.stream);
+    // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T); op(B)(kk, c) rows c: B[kk + ldb c] (N) or B[c + ldb kk] (T)
+    if (!transA) digits_of(ex, A, 1, lda, m, k, Mp, Kp, digits, ea.as<int>(), da.as<int8_t>());
+    else digits_of(ex, A, lda, 1, m, k, Mp, Kp, digits, ea.as<int>(), da.as<int8_t>());
+    if (!transB) digits_of(ex, B, ldb, 1, n, k, Np, Kp, digits, eb.as<int>(), db.as<int8_t>());
+    else digits_of(ex, B, 1, ldb, n, k, Np, Kp, digits, eb.as<int>(), db.as<int8_t>());
+
+    CU_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OSMEM));
+    CUtensorMap ta = make_i8_map(da.as<void>(), Mp, Kp, Mp * Kp, digits);
+    CUtensorMap tb = make_i8_map(db.as<void>(), Np, Kp, Np * Kp, digits);
+    OzMap map{};
+    map.num_mt = (int)(Mp / OBM);
+    map.num_nt = (int)(Np / OBN);
+    map.group_m = std::min(map.num_mt, 16);
+    map.nk_all = (int)(Kp / OBK);
+    map.kc = OK_CHUNK / OBK;
+    map.nchunks = (map.nk_all + map.kc - 1) / map.kc;
+    map.digits = digits;
+    map.npass = digits > MAX_DIAG_PER_PASS ? 2 : 1;
+    map.M = (int)m;
+    map.N = (int)n;
+    map.ldc = ldc;
+    map.alpha = alpha;
+    map.beta = beta;
+    map.C = C;
+    map.ea = ea.as<int>();
+    map.eb = eb.as<int>();
+    map.err = ex.gemm_err;
+    map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : OWAIT_CYCLES;
+    const int num_tiles = map.num_mt * map.num_nt;
+    const int grid = std::min(num_tiles, num_sms());
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ex.prof && ex.prof->on) {
+        CU_CHECK(cudaEventCreate(&e0));
+        CU_CHECK(cudaEventCreate(&e1));
+        CU_CHECK(cudaEventRecord(e0, ex.stream));
+    }
+    ozaki_gemm_kernel<<<grid, OTHREADS, OSMEM, ex.stream>>>(ta, tb, map, num_tiles);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+    if (e0) {
+        CU_CHECK(cudaEventRecord(e1, ex.stream));
+        ex.prof->oz_events.emplace_back(e0, e1);
+        ex.prof->oz_ops.push_back(2.0 * (double)digits * (digits + 1) / 2.0 * (double)m * (double)n * (double)k);
+    }
+}
+
+int ozaki_products(int digits) { return digits * (digits + 1) / 2; }
+
+}  // namespace ccsd

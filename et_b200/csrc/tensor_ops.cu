@@ -8,6 +8,7 @@
 
 #include "autotune.cuh"
 #include "mixed_gemm.cuh"
+#include "ozaki_gemm.cuh"
 #include "tensor_ops.cuh"
 
 namespace ccsd {
@@ -244,6 +245,11 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
                      (long long)k, fl, route);
     if (mixed) {
         mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, route);
+        return;
+    }
+    if (ex.fp64_digits > 0 && fl >= ex.fp64_digits_min_flops &&
+        (ex.fp64_digits_min_flops <= 1 || (m >= 256 && n >= 256 && k >= 256))) {
+        ozaki_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, ex.fp64_digits);
         return;
     }
     BLAS_CHECK(cublasDgemm_64(ex.blas, transA ? CUBLAS_OP_T : CUBLAS_OP_N, transB ? CUBLAS_OP_T : CUBLAS_OP_N, m,

@@ -78,7 +78,12 @@ typedef struct ccsd_gpu_solver_options {
     double refine_target;        /* MIXED only: the true residual the refinement aims at; refreshes
                                     that remove drift happen only while the drift exceeds it
                                     (0 = omega_threshold) */
-    int32_t reserved[6];
+    int32_t refresh_digits;      /* MIXED only: arithmetic of the FP64 evaluations (refreshes and the
+                                    FP64 iterations after them): 4..7 = the FP64-accurate int8 digit GEMM
+                                    on the tensor cores with that many 7-bit digits per operand for
+                                    products of at least 1e10 flops, -1 = cuBLAS DGEMM for every
+                                    product, 0 = the default (cuBLAS DGEMM) */
+    int32_t reserved[5];
 } ccsd_gpu_solver_options;
 
 /* Creation / teardown.  Replaces the wavefunction set-up that allocates t, Omega and the
@@ -209,6 +214,15 @@ int ccsd_gpu_stats(void *ctx, int64_t *kernel_launches, double *gemm_flops);
  * captured graphs.  No counterpart in eT, which calls BLAS per contraction. */
 int ccsd_gpu_set_graphs(void *ctx, int32_t on);
 
+/* FP64 products of at least min_flops flops (<= 0: 1e10; then also 256 in every dimension; 1:
+ * every product) on the int8 tensor cores: digits = 4..7 cuts each operand row / column into that many 7-bit int8 digits after a power-of-two
+ * scaling (Ozaki's error-free splitting), sums the digit products of weight >= 2^(-7(digits+1))
+ * exactly in int32 (tcgen05 kind::i8) and in FP64 in the epilogue; 7 digits reproduce DGEMM to ~1e-14
+ * of the largest output.  0 (the default) keeps cuBLAS DGEMM.  Applies to FP64-precision work of the
+ * context (the residual, transformations, and the solver's FP64 evaluations unless
+ * ccsd_gpu_solver_options.refresh_digits says otherwise).  No counterpart in eT. */
+int ccsd_gpu_set_fp64_digits(void *ctx, int32_t digits, double min_flops);
+
 /* Integrals of the FP64 residual.  resident = 1 (the default unless the environment sets
  * CCSD_GPU_FP64_RESIDENT=0): the A2 ladder's +/- pair integrals and the ovvv block of the
  * untransformed Cholesky vectors are formed once per Cholesky set and kept on the device when they
@@ -235,12 +249,16 @@ int ccsd_gpu_graph_stats(void *ctx, int64_t *residual_replays, int64_t *tuned_ro
  * their summed device time (ms) and the tensor flops they issued (3 products x 2mnk). */
 int ccsd_gpu_set_profiling(void *ctx, int32_t on);
 int ccsd_gpu_gemm_profile(void *ctx, int64_t *launches, double *device_ms, double *tensor_flops);
+/* The same for the int8 digit GEMM of FP64-accurate products (ccsd_gpu_set_fp64_digits): launches,
+ * summed device time (ms) and int8 tensor ops issued (2mnk per digit product). */
+int ccsd_gpu_digit_gemm_profile(void *ctx, int64_t *launches, double *device_ms, double *int8_ops);
 
 /* Diagnostics: C (m x n, column-major, host) = alpha op(A) op(B) + beta C on the device, through
  * the FP64 DGEMM (mixed = 0) or the split-BF16 tcgen05 GEMM that the contractions use (mixed = 1,
  * two bf16 planes), or the three-plane variant of that GEMM (mixed = 2; 6 products, operand rounding
  * 2^-24; not used by the contractions because the FP32 accumulation in the tensor cores, not the
- * operand split, limits their accuracy at CCSD's long K). */
+ * operand split, limits their accuracy at CCSD's long K), or the FP64-accurate int8 digit GEMM with
+ * mixed = 4..7 digits of 7 bits per operand (tcgen05 kind::i8, exact int32 accumulation). */
 int ccsd_gpu_selftest_gemm(void *ctx, int32_t mixed, int32_t transA, int32_t transB, int64_t m, int64_t n,
                            int64_t k, double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
                            double beta, double *C, int64_t ldc);
