@@ -164,7 +164,12 @@ def gemm_traffic(n_o, n_v, n_J):
     return None
 
 
-def converged_solve(gpu, stream, refine, thr=1e-9, ethr=1e-11, L=None):
+# arithmetic of the mixed path's FP64 evaluations (refreshes): int8 digits per operand on the tensor
+# cores (ozaki_gemm), or -1 for cuBLAS DGEMM; set from --refresh-digits
+REFRESH_DIGITS = 7
+
+
+def converged_solve(gpu, stream, refine, thr=1e-9, ethr=1e-11, L=None, refresh_digits=None):
     """From the MP2 start to |Omega| < thr and |dE| < ethr between iterations (certified by an FP64
     evaluation in mixed precision): (seconds by CUDA events, iterations, energy, converged).  With L
     the Cholesky vectors are set again first (untimed), so every integral kept on the device for a
@@ -178,7 +183,8 @@ def converged_solve(gpu, stream, refine, thr=1e-9, ethr=1e-11, L=None):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     e, it, _, rc = gpu.solve_ground_state(max_iterations=60, omega_threshold=thr, energy_threshold=ethr,
-                                          refine_threshold=refine, raise_on_failure=False)
+                                          refine_threshold=refine, raise_on_failure=False,
+                                          refresh_digits=REFRESH_DIGITS if refresh_digits is None else refresh_digits)
     ev1.record(stream)
     torch.cuda.synchronize()
     return ev0.elapsed_time(ev1) / 1e3, it, e, rc == 0
@@ -205,6 +211,7 @@ def timed_solve(gpu, stream, iters, refine, world, clocks_dev=None):
     ev0.record(stream)
     e, it, hist, rc = gpu.solve_ground_state(max_iterations=iters, omega_threshold=1e-30, energy_threshold=-1.0,
                                              refine_threshold=refine, refine_target=REFINE_TARGET,
+                                             refresh_digits=REFRESH_DIGITS,
                                              raise_on_failure=False)
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -297,6 +304,8 @@ def run_gpu(args):
         "config": {"workload": f"CCSD ground-state iteration, synthetic Cholesky system o={n_o} v={n_v} N_J={n_J}",
                    "n_o": n_o, "n_v": n_v, "n_J": n_J, "precision": args.precision,
                    "refine_threshold": args.refine, "refine_target": REFINE_TARGET,
+                   "refresh_arithmetic": (f"int8 digit GEMM ({REFRESH_DIGITS} digits) for FP64 products of at "
+                                          f"least 1e10 flops" if REFRESH_DIGITS > 0 else "cuBLAS DGEMM"),
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "inputs larger than L2 (t2 419 MB, L 1.19 GB at full size)",
                    "flops_per_iter": flops_iter},
@@ -337,6 +346,8 @@ def run_gpu(args):
         gpu.set_precision(MIXED)
         tmb, itmb, emb, okmb = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8, L=L)
         tm, itm, em, okm = converged_solve(gpu, stream, args.refine, 1e-9, 1e-11, L=L)
+        # attribution: the same mixed solve with its FP64 evaluations on cuBLAS DGEMM
+        tmd, itmd, emd, okmd = converged_solve(gpu, stream, args.refine, 1e-6, 1e-8, L=L, refresh_digits=-1)
         result["fp64_path"] = {"algorithm": "T1-transformed ladder integrals formed in every call (eT)",
                                "s_per_iter": round(s64, 5), "energy": e_ref, "converged": ok64,
                                "to_1e-9": {"s": round(t64, 3), "iterations": n64},
@@ -349,10 +360,14 @@ def run_gpu(args):
                                         "to_1e-9": {"s": round(t64r, 3), "iterations": n64r},
                                         "to_target": {"s": round(t64rb, 3), "iterations": n64rb,
                                                       "converged": ok64rb, "dE": abs(e64rb - e_ref)}}
-        result["mixed_path"] = {"to_1e-9": {"s": round(tm, 3), "iterations": itm, "converged": okm,
+        result["mixed_path"] = {"refresh_arithmetic": (f"int8 digit GEMM, {REFRESH_DIGITS} digits" if REFRESH_DIGITS > 0
+                                                       else "cuBLAS DGEMM"),
+                                "to_1e-9": {"s": round(tm, 3), "iterations": itm, "converged": okm,
                                             "dE": abs(em - e_ref)},
                                 "to_target": {"s": round(tmb, 3), "iterations": itmb, "converged": okmb,
-                                              "dE": abs(emb - e_ref)}}
+                                              "dE": abs(emb - e_ref)},
+                                "to_target_dgemm_refreshes": {"s": round(tmd, 3), "iterations": itmd,
+                                                              "converged": okmd, "dE": abs(emd - e_ref)}}
         result["target"] = "|dE| <= 1e-8 Eh vs converged FP64: thresholds |Omega| < 1e-6, |dE| < 1e-8"
         result["speedup_per_iter_vs_fp64"] = round(s64 / (ms_step / 1e3), 3)
         result["speedup_to_target_vs_fp64"] = round(t64b / tmb, 3)
@@ -452,6 +467,18 @@ def per_call_times(gpu, stream):
     f0 = gpu.stats()[1]
     omega()
     out["omega_fp64_resident_flops"] = gpu.stats()[1] - f0
+    if REFRESH_DIGITS > 0:
+        # the same FP64 evaluation with its large products on the int8 digit GEMM (the refreshes)
+        gpu.set_fp64_digits(REFRESH_DIGITS)
+        out["omega_fp64_resident_digits_s"] = med(omega, 3)
+        gpu.set_profiling(True)
+        omega()
+        n_oz, ms_oz, ops_oz = gpu.digit_gemm_profile()
+        gpu.set_profiling(False)
+        gpu.set_fp64_digits(0)
+        out["digit_gemm_in_one_evaluation"] = {"launches": n_oz, "device_ms": round(ms_oz, 2),
+                                               "int8_tops_issued": round(ops_oz / (ms_oz * 1e-3) / 1e12, 1)
+                                               if ms_oz else None}
     out["jacobian_fp64_resident_s"] = med(jac, 1)
     gpu.set_fp64_integrals(False)
     out["omega_fp64_s"] = med(omega, 3)
@@ -783,9 +810,13 @@ def main():
     p.add_argument("--cpu-iterations", dest="cpu_iterations", type=int, default=1,
                    help="ground-state iterations the CPU baseline times at the benchmark shape")
     p.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    p.add_argument("--refresh-digits", dest="refresh_digits", type=int, default=7,
+                   help="mixed path: int8 digits of the FP64 evaluations (4..7), -1 = cuBLAS DGEMM")
     p.add_argument("--no-extras", dest="extras", action="store_false",
                    help="skip the EOM, adjoint and uneven-batch workloads in the default line")
     args = p.parse_args()
+    global REFRESH_DIGITS
+    REFRESH_DIGITS = args.refresh_digits
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "eom":
