@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -729,6 +730,10 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     std::vector<double> norms;
     // CCSD_GPU_TRACE=1: one line per iteration on stderr with the refinement decisions
     const bool trace = std::getenv("CCSD_GPU_TRACE") && std::getenv("CCSD_GPU_TRACE")[0] == '1';
+    const auto trace_t0 = std::chrono::steady_clock::now();
+    auto trace_ms = [&]() {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - trace_t0).count();
+    };
     double trace_moved = 0.0;
     const char *trace_why = "";
     // shift every stored DIIS error vector by v and rebuild their Gram matrix
@@ -809,8 +814,9 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
             }
         }
         if (trace) {
-            std::fprintf(stderr, "ccsd_gpu gs %3d  E %.12f  |Omega| %.3e  %s  %-6s moved %.3e r_c %.3e%s\n", it, e, nrm,
-                         exact ? "fp64 " : "mixed", trace_why, trace_moved, r_c, fp64_final ? "  fp64 from here" : "");
+            std::fprintf(stderr, "ccsd_gpu gs %3d  E %.12f  |Omega| %.3e  %s  %-6s moved %.3e r_c %.3e  t %.1f ms%s\n", it,
+                         e, nrm, exact ? "fp64 " : "mixed", trace_why, trace_moved, r_c, trace_ms(),
+                         fp64_final ? "  fp64 from here" : "");
         }
         if (!std::isfinite(nrm) || !std::isfinite(e)) {
             ex.prec = user;

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "ozaki_gemm.cuh"
 #include "tc_common.cuh"
@@ -384,9 +385,8 @@ int num_sms() {
     return v;
 }
 
-// rows of a strided view -> exponents e[R] and digits [digits][Rp][Kp]
-void digits_of(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
-               int digits, int *e, int8_t *out) {
+// exponents e[R] of the rows of a strided view over the whole K
+void row_exponents(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int *e) {
     // start every exponent below any frexp exponent: 0x80 bytes = -2139062144
     CU_CHECK(cudaMemsetAsync(e, 0x80, sizeof(int) * (size_t)Rp, ex.stream));
     const int64_t rb = (R + 31) / 32;
@@ -394,9 +394,16 @@ void digits_of(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, i
     const int64_t kb = std::max<int64_t>(1, std::min<int64_t>((K + 31) / 32, (4 * 148 + rb - 1) / rb));
     oz_rowexp_kernel<<<dim3((unsigned)rb, (unsigned)std::min<int64_t>(kb, 65535)), dim3(32, 8), 0, ex.stream>>>(
         src, sr, sk, (int)R, (int)K, e);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
+}
+
+// digits [digits][Rp][Kp] of the K slab of a strided view (the exponents are those of whole rows)
+void slab_digits(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
+                 int digits, const int *e, int8_t *out) {
     oz_digits_kernel<<<dim3((unsigned)(Rp / 32), (unsigned)std::min<int64_t>(Kp / 32, 65535)), dim3(32, 8), 0,
                        ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, digits, e, out);
-    ex.launches += 2;
+    ex.launches++;
     CU_CHECK(cudaGetLastError());
 }
 
@@ -408,52 +415,66 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "ozaki_gemm: size too large");
     REQUIRE(digits >= 2 && digits <= SLOTS, CCSD_GPU_EINVAL, "ozaki_gemm: 2 to 7 digits");
     REQUIRE(ex.gemm_err != nullptr, CCSD_GPU_EINVAL, "ozaki_gemm: no error word");
-    const int64_t Kp = round_up(k, OBK), Mp = round_up(m, OBM), Np = round_up(n, OBN);
-    DBuf da(sizeof(int8_t) * (size_t)digits * Mp * Kp, ex.stream), db(sizeof(int8_t) * (size_t)digits * Np * Kp, ex.stream);
-    DBuf ea(sizeof(int) * (size_t)Mp, ex.stream), eb(sizeof(int) * (size_t)Np, ex.stream);
+    const int64_t Mp = round_up(m, OBM), Np = round_up(n, OBN);
     // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T); op(B)(kk, c) rows c: B[kk + ldb c] (N) or B[c + ldb kk] (T)
-    if (!transA) digits_of(ex, A, 1, lda, m, k, Mp, Kp, digits, ea.as<int>(), da.as<int8_t>());
-    else digits_of(ex, A, lda, 1, m, k, Mp, Kp, digits, ea.as<int>(), da.as<int8_t>());
-    if (!transB) digits_of(ex, B, ldb, 1, n, k, Np, Kp, digits, eb.as<int>(), db.as<int8_t>());
-    else digits_of(ex, B, 1, ldb, n, k, Np, Kp, digits, eb.as<int>(), db.as<int8_t>());
-
+    const int64_t a_sr = transA ? lda : 1, a_sk = transA ? 1 : lda;
+    const int64_t b_sr = transB ? 1 : ldb, b_sk = transB ? ldb : 1;
+    DBuf ea(sizeof(int) * (size_t)Mp, ex.stream), eb(sizeof(int) * (size_t)Np, ex.stream);
+    row_exponents(ex, A, a_sr, a_sk, m, k, Mp, ea.as<int>());
+    row_exponents(ex, B, b_sr, b_sk, n, k, Np, eb.as<int>());
+    // the digit planes of K slabs of whole 16384-wide chunks, at most ~4 GB of them at a time (a
+    // 21 GB operand would otherwise need 18 GB of planes at once); each slab's launch adds its chunks
+    // to C in the order one launch over all K would, so the result does not depend on the slabs
+    const int64_t per_chunk = (int64_t)digits * (Mp + Np) * OK_CHUNK;
+    int64_t budget = 4ll << 30;
+    if (const char *mb = std::getenv("CCSD_GPU_DIGIT_SLAB_MB")) budget = std::max<int64_t>(1, std::atoll(mb)) << 20;
+    const int64_t chunks_per_slab = std::max<int64_t>(1, budget / per_chunk);
+    const int64_t kslab = std::min<int64_t>(round_up(k, OBK), chunks_per_slab * OK_CHUNK);
+    DBuf da(sizeof(int8_t) * (size_t)digits * Mp * kslab, ex.stream), db(sizeof(int8_t) * (size_t)digits * Np * kslab,
+                                                                          ex.stream);
     CU_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OSMEM));
-    CUtensorMap ta = make_i8_map(da.as<void>(), Mp, Kp, Mp * Kp, digits);
-    CUtensorMap tb = make_i8_map(db.as<void>(), Np, Kp, Np * Kp, digits);
-    OzMap map{};
-    map.num_mt = (int)(Mp / OBM);
-    map.num_nt = (int)(Np / OBN);
-    map.group_m = std::min(map.num_mt, 16);
-    map.nk_all = (int)(Kp / OBK);
-    map.kc = OK_CHUNK / OBK;
-    map.nchunks = (map.nk_all + map.kc - 1) / map.kc;
-    map.digits = digits;
-    map.npass = digits > MAX_DIAG_PER_PASS ? 2 : 1;
-    map.M = (int)m;
-    map.N = (int)n;
-    map.ldc = ldc;
-    map.alpha = alpha;
-    map.beta = beta;
-    map.C = C;
-    map.ea = ea.as<int>();
-    map.eb = eb.as<int>();
-    map.err = ex.gemm_err;
-    map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : OWAIT_CYCLES;
-    const int num_tiles = map.num_mt * map.num_nt;
-    const int grid = std::min(num_tiles, num_sms());
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (ex.prof && ex.prof->on) {
-        CU_CHECK(cudaEventCreate(&e0));
-        CU_CHECK(cudaEventCreate(&e1));
-        CU_CHECK(cudaEventRecord(e0, ex.stream));
-    }
-    ozaki_gemm_kernel<<<grid, OTHREADS, OSMEM, ex.stream>>>(ta, tb, map, num_tiles);
-    ex.launches++;
-    CU_CHECK(cudaGetLastError());
-    if (e0) {
-        CU_CHECK(cudaEventRecord(e1, ex.stream));
-        ex.prof->oz_events.emplace_back(e0, e1);
-        ex.prof->oz_ops.push_back(2.0 * (double)digits * (digits + 1) / 2.0 * (double)m * (double)n * (double)k);
+    const int nsm = num_sms();
+    for (int64_t k0 = 0; k0 < k; k0 += kslab) {
+        const int64_t kk = std::min(kslab, k - k0), Kp = round_up(kk, OBK);
+        slab_digits(ex, A + k0 * a_sk, a_sr, a_sk, m, kk, Mp, Kp, digits, ea.as<int>(), da.as<int8_t>());
+        slab_digits(ex, B + k0 * b_sk, b_sr, b_sk, n, kk, Np, Kp, digits, eb.as<int>(), db.as<int8_t>());
+        CUtensorMap ta = make_i8_map(da.as<void>(), Mp, Kp, Mp * Kp, digits);
+        CUtensorMap tb = make_i8_map(db.as<void>(), Np, Kp, Np * Kp, digits);
+        OzMap map{};
+        map.num_mt = (int)(Mp / OBM);
+        map.num_nt = (int)(Np / OBN);
+        map.group_m = std::min(map.num_mt, 16);
+        map.nk_all = (int)(Kp / OBK);
+        map.kc = OK_CHUNK / OBK;
+        map.nchunks = (map.nk_all + map.kc - 1) / map.kc;
+        map.digits = digits;
+        map.npass = digits > MAX_DIAG_PER_PASS ? 2 : 1;
+        map.M = (int)m;
+        map.N = (int)n;
+        map.ldc = ldc;
+        map.alpha = alpha;
+        map.beta = k0 == 0 ? beta : 1.0;
+        map.C = C;
+        map.ea = ea.as<int>();
+        map.eb = eb.as<int>();
+        map.err = ex.gemm_err;
+        map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : OWAIT_CYCLES;
+        const int num_tiles = map.num_mt * map.num_nt;
+        const int grid = std::min(num_tiles, nsm);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (ex.prof && ex.prof->on) {
+            CU_CHECK(cudaEventCreate(&e0));
+            CU_CHECK(cudaEventCreate(&e1));
+            CU_CHECK(cudaEventRecord(e0, ex.stream));
+        }
+        ozaki_gemm_kernel<<<grid, OTHREADS, OSMEM, ex.stream>>>(ta, tb, map, num_tiles);
+        ex.launches++;
+        CU_CHECK(cudaGetLastError());
+        if (e0) {
+            CU_CHECK(cudaEventRecord(e1, ex.stream));
+            ex.prof->oz_events.emplace_back(e0, e1);
+            ex.prof->oz_ops.push_back(2.0 * (double)digits * (digits + 1) / 2.0 * (double)m * (double)n * (double)kk);
+        }
     }
 }
 

@@ -35,6 +35,19 @@ def test_digit_gemm_equals_emulation_bitwise(ctx, m, n, k, digits):
     assert np.array_equal(out, oz.ozaki_gemm(A, B, digits))
 
 
+def test_digit_gemm_in_k_slabs_equals_one_launch(ctx, monkeypatch):
+    """Operands whose digit planes exceed the slab budget are converted and multiplied in K slabs of
+    whole chunks; the result is bit for bit that of one launch over all K."""
+    rng = np.random.default_rng(12)
+    A = rng.standard_normal((300, 40000))
+    B = rng.standard_normal((40000, 200))
+    whole = ctx.selftest_gemm(A, B, mixed=7)
+    monkeypatch.setenv("CCSD_GPU_DIGIT_SLAB_MB", "1")          # one 16384-wide chunk per slab
+    sliced = ctx.selftest_gemm(A, B, mixed=7)
+    assert np.array_equal(whole, sliced)
+    assert np.array_equal(whole, oz.ozaki_gemm(A, B, 7))
+
+
 @pytest.mark.parametrize("m,n,k", [(129, 257, 65), (300, 1000, 777), (640, 520, 20000)])
 @pytest.mark.parametrize("tA,tB", [(False, False), (True, False), (False, True), (True, True)])
 def test_digit_gemm_matches_fp64(ctx, m, n, k, tA, tB):
