@@ -91,6 +91,37 @@ struct OzMap {
     }
 };
 
+// The MMAs of one K block for the diagonals [D0, D1) of S-digit operands, fully unrolled: the
+// descriptors of digit q sit a constant offset from those of digit 0 (a 16-byte unit in the start
+// field per 16 bytes, tiles of A_TILE / B_TILE bytes), so issuing an MMA costs a few integer adds.  An
+// int8 MMA of 128 x 128 x 32 lasts ~64 tensor cycles; rebuilding descriptors per MMA had the single
+// issuing thread, not the tensor pipe, set the pace.
+template <int S, int D0, int D1>
+__device__ __forceinline__ void issue_kblock(uint32_t tmem, uint64_t a0, uint64_t b0, bool first_kb) {
+#pragma unroll
+    for (int kk = 0; kk < OBK / 32; kk++) {
+#pragma unroll
+        for (int d = D0; d < D1; d++) {
+#pragma unroll
+            for (int t = (d - S + 1 > 0 ? d - S + 1 : 0); t <= (d < S - 1 ? d : S - 1); t++) {
+                const int u = d - t;
+                const bool first = kk == 0 && t == (d - S + 1 > 0 ? d - S + 1 : 0);
+                mma_i8(tmem + (uint32_t)((d - D0) * OBN),
+                       a0 + (uint64_t)(t * (A_TILE >> 4) + kk * 2),
+                       b0 + (uint64_t)(u * (B_TILE >> 4) + kk * 2), (first_kb && first) ? 0u : 1u);
+            }
+        }
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void issue_pass(int p, uint32_t tmem, const uint8_t *st, bool first_kb) {
+    const uint64_t a0 = smem_desc_k<64>(st, 0), b0 = smem_desc_k<64>(st + SLOTS * A_TILE, 0);
+    if (p == 0) issue_kblock<S, 0, (S < MAX_DIAG_PER_PASS ? S : MAX_DIAG_PER_PASS)>(tmem, a0, b0, first_kb);
+    else if constexpr (S > MAX_DIAG_PER_PASS) issue_kblock<S, MAX_DIAG_PER_PASS, S>(tmem, a0, b0, first_kb);
+}
+
+template <int S>
 __global__ void __launch_bounds__(OTHREADS, 1)
 ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzMap map,
                   int num_tiles) {
@@ -186,21 +217,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                                 break;
                             }
                             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                            const uint8_t *st = smem + s * OSTAGE_BYTES;
-#pragma unroll
-                            for (int kk = 0; kk < OBK / 32; kk++) {
-                                const uint32_t ko = kk * 32;   // 32 int8 = 32 bytes per MMA
-                                for (int d = d0; d < d1; d++) {
-                                    const uint32_t acc = tmem + (uint32_t)((d - d0) * OBN);
-                                    const int tlo = max(0, d - (map.digits - 1)), thi = min(d, map.digits - 1);
-                                    for (int tq = tlo; tq <= thi; tq++) {
-                                        const int uq = d - tq;
-                                        const uint32_t accumulate = (kb > kb0 || kk > 0 || tq > tlo) ? 1u : 0u;
-                                        mma_i8(acc, smem_desc_k<64>(st + tq * A_TILE, ko),
-                                               smem_desc_k<64>(st + SLOTS * A_TILE + uq * B_TILE, ko), accumulate);
-                                    }
-                                }
-                            }
+                            issue_pass<S>(p, tmem, smem + s * OSTAGE_BYTES, kb == kb0);
                             mma_commit(&empty[s]);
                         }
                         mma_commit(acc_full);
@@ -432,7 +449,10 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     const int64_t kslab = std::min<int64_t>(round_up(k, OBK), chunks_per_slab * OK_CHUNK);
     DBuf da(sizeof(int8_t) * (size_t)digits * Mp * kslab, ex.stream), db(sizeof(int8_t) * (size_t)digits * Np * kslab,
                                                                           ex.stream);
-    CU_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OSMEM));
+    auto kernel = digits == 7 ? ozaki_gemm_kernel<7> : digits == 6 ? ozaki_gemm_kernel<6>
+                : digits == 5 ? ozaki_gemm_kernel<5> : digits == 4 ? ozaki_gemm_kernel<4>
+                : digits == 3 ? ozaki_gemm_kernel<3> : ozaki_gemm_kernel<2>;
+    CU_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OSMEM));
     const int nsm = num_sms();
     for (int64_t k0 = 0; k0 < k; k0 += kslab) {
         const int64_t kk = std::min(kslab, k - k0), Kp = round_up(kk, OBK);
@@ -467,7 +487,7 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
             CU_CHECK(cudaEventCreate(&e1));
             CU_CHECK(cudaEventRecord(e0, ex.stream));
         }
-        ozaki_gemm_kernel<<<grid, OTHREADS, OSMEM, ex.stream>>>(ta, tb, map, num_tiles);
+        kernel<<<grid, OTHREADS, OSMEM, ex.stream>>>(ta, tb, map, num_tiles);
         ex.launches++;
         CU_CHECK(cudaGetLastError());
         if (e0) {
