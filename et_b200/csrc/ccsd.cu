@@ -62,6 +62,7 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     gemm_err = DBuf(sizeof(int), own_stream);
     CU_CHECK(cudaMemsetAsync(gemm_err.as<void>(), 0, sizeof(int), own_stream));
     ex.gemm_err = gemm_err.as<int>();
+    ex.digit_arena = &digit_arena;
     set_precision(opt ? opt->precision : CCSD_GPU_FP64);
     if (opt && opt->mixed_min_flops > 0) ex.mixed_min_flops = (double)opt->mixed_min_flops;
     if (opt && opt->mixed_k_chunk != 0) ex.k_chunk = opt->mixed_k_chunk;
@@ -100,7 +101,7 @@ Context::~Context() {
     if (graphs_captured) cudaDeviceGraphMemTrim(device);   // the physical memory the residual graphs held
     for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
                     &mbuf, &ybuf, &om_stage, &f64_gp, &f64_gm, &f64_ovvv, &hb_oo, &hb_ov, &hb_vo, &hb_vv,
-                    &gemm_err})
+                    &gemm_err, &digit_arena})
         b->release();
     if (blas) cublasDestroy(blas);
     blas = nullptr;

@@ -80,6 +80,7 @@ struct Context {
     int64_t cache_epoch = 0;
     DBuf blas_ws;                   // cuBLAS workspace (no allocation inside stream capture)
     DBuf gemm_err;                  // error word of this context's tensor-core GEMMs (ex.gemm_err)
+    DBuf digit_arena;               // scratch of the int8 digit GEMM (ex.digit_arena), grow-only
     // ccsd_gpu_prepare_jacobian: the recorded residual shared by the transformations, and the id
     // under which the ladder integrals a prepared transformation forms stay in mbuf for the next one
     std::unique_ptr<PreparedJacobian> prep;

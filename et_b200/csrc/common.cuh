@@ -175,6 +175,9 @@ struct Exec {
     // cores with this many 7-bit digits per operand (ozaki_gemm); 0 = cuBLAS DGEMM
     int fp64_digits = 0;
     double fp64_digits_min_flops = 1e10;
+    // grow-only scratch of the digit GEMM (digit planes and exponents), owned by the context: the
+    // multi-GB planes are neither allocated nor freed per product
+    DBuf *digit_arena = nullptr;
 };
 
 // Times the enclosing scope as one term of ex.terms (nothing happens unless the log is on, and

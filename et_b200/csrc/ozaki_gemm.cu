@@ -378,6 +378,7 @@ __global__ void oz_digits_kernel(const double *__restrict__ src, long long sr, l
 }
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
 // digits x rows x Kp tensor of int8, box (64, 128, 1), 64-byte swizzle
 CUtensorMap make_i8_map(void *base, int64_t rows, int64_t Kp, int64_t plane_stride, int planes) {
@@ -436,9 +437,8 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T); op(B)(kk, c) rows c: B[kk + ldb c] (N) or B[c + ldb kk] (T)
     const int64_t a_sr = transA ? lda : 1, a_sk = transA ? 1 : lda;
     const int64_t b_sr = transB ? 1 : ldb, b_sk = transB ? ldb : 1;
-    DBuf ea(sizeof(int) * (size_t)Mp, ex.stream), eb(sizeof(int) * (size_t)Np, ex.stream);
-    row_exponents(ex, A, a_sr, a_sk, m, k, Mp, ea.as<int>());
-    row_exponents(ex, B, b_sr, b_sk, n, k, Np, eb.as<int>());
+    // scratch: exponents of both operands and the digit planes of one K slab
+    const size_t exp_bytes = round_up(sizeof(int) * (size_t)(Mp + Np), 256);
     // the digit planes of K slabs of whole 16384-wide chunks, at most ~4 GB of them at a time (a
     // 21 GB operand would otherwise need 18 GB of planes at once); each slab's launch adds its chunks
     // to C in the order one launch over all K would, so the result does not depend on the slabs
@@ -447,8 +447,19 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     if (const char *mb = std::getenv("CCSD_GPU_DIGIT_SLAB_MB")) budget = std::max<int64_t>(1, std::atoll(mb)) << 20;
     const int64_t chunks_per_slab = std::max<int64_t>(1, budget / per_chunk);
     const int64_t kslab = std::min<int64_t>(round_up(k, OBK), chunks_per_slab * OK_CHUNK);
-    DBuf da(sizeof(int8_t) * (size_t)digits * Mp * kslab, ex.stream), db(sizeof(int8_t) * (size_t)digits * Np * kslab,
-                                                                          ex.stream);
+    const size_t a_bytes = round_up((size_t)digits * Mp * kslab, 1024), b_bytes = (size_t)digits * Np * kslab;
+    const size_t need = exp_bytes + a_bytes + b_bytes;
+    DBuf local;
+    DBuf *arena = ex.digit_arena ? ex.digit_arena : &local;
+    if (arena->bytes() < need) {
+        arena->release();
+        arena->alloc(need, ex.stream);
+    }
+    uint8_t *base = arena->as<uint8_t>();
+    int *ea = reinterpret_cast<int *>(base), *eb = ea + Mp;
+    int8_t *da = reinterpret_cast<int8_t *>(base + exp_bytes), *db = da + a_bytes;
+    row_exponents(ex, A, a_sr, a_sk, m, k, Mp, ea);
+    row_exponents(ex, B, b_sr, b_sk, n, k, Np, eb);
     auto kernel = digits == 7 ? ozaki_gemm_kernel<7> : digits == 6 ? ozaki_gemm_kernel<6>
                 : digits == 5 ? ozaki_gemm_kernel<5> : digits == 4 ? ozaki_gemm_kernel<4>
                 : digits == 3 ? ozaki_gemm_kernel<3> : ozaki_gemm_kernel<2>;
@@ -456,10 +467,10 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     const int nsm = num_sms();
     for (int64_t k0 = 0; k0 < k; k0 += kslab) {
         const int64_t kk = std::min(kslab, k - k0), Kp = round_up(kk, OBK);
-        slab_digits(ex, A + k0 * a_sk, a_sr, a_sk, m, kk, Mp, Kp, digits, ea.as<int>(), da.as<int8_t>());
-        slab_digits(ex, B + k0 * b_sk, b_sr, b_sk, n, kk, Np, Kp, digits, eb.as<int>(), db.as<int8_t>());
-        CUtensorMap ta = make_i8_map(da.as<void>(), Mp, Kp, Mp * Kp, digits);
-        CUtensorMap tb = make_i8_map(db.as<void>(), Np, Kp, Np * Kp, digits);
+        slab_digits(ex, A + k0 * a_sk, a_sr, a_sk, m, kk, Mp, Kp, digits, ea, da);
+        slab_digits(ex, B + k0 * b_sk, b_sr, b_sk, n, kk, Np, Kp, digits, eb, db);
+        CUtensorMap ta = make_i8_map(da, Mp, Kp, Mp * Kp, digits);
+        CUtensorMap tb = make_i8_map(db, Np, Kp, Np * Kp, digits);
         OzMap map{};
         map.num_mt = (int)(Mp / OBM);
         map.num_nt = (int)(Np / OBN);
@@ -475,8 +486,8 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
         map.alpha = alpha;
         map.beta = k0 == 0 ? beta : 1.0;
         map.C = C;
-        map.ea = ea.as<int>();
-        map.eb = eb.as<int>();
+        map.ea = ea;
+        map.eb = eb;
         map.err = ex.gemm_err;
         map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : OWAIT_CYCLES;
         const int num_tiles = map.num_mt * map.num_nt;
