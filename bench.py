@@ -626,8 +626,8 @@ def adjoint_summary(args):
 
 def run_batch(args):
     """64 independent systems o ~ U{6..24}, v = 8o, N_J = 3(o+v), each from its MP2 start to the
-    benchmark's target (|Omega| < 1e-6 and |dE| < 1e-8 between iterations, which puts every energy
-    within 1e-8 Eh of the converged one): systems/s of the concurrent mixed batch
+    benchmark's target, |dE| <= 1e-8 Eh from the converged FP64 energy (stopping at |Omega| < 5e-7 and
+    |dE| < 5e-9 between iterations, the same for every run): systems/s of the concurrent mixed batch
     (ccsd_gpu_solve_gs_batch, --workers contexts in flight) against 64 sequential plain FP64 solves,
     with the two other combinations for attribution, and |dE| against FP64 energies converged to
     |Omega| < 1e-9 (untimed).  The synthetic inputs are generated before the timed region; each
@@ -659,10 +659,14 @@ def batch_summary(args, rank=0, local=0, world=1):
         systems.append((s.L_mo, s.h_mo, s.eps, s.n_o, s.e_hf))
     e_ref, _, st_ref, _ = solve_ground_states(systems, precision=FP64, device=local, workers=args.workers,
                                               max_iterations=80, omega_threshold=1e-9, energy_threshold=1e-11)
+    # the stopping thresholds of the timed solves (all four runs alike): |Omega| < 1e-6 and |dE| < 1e-8
+    # between iterations put energies at ~4e-9 from the converged one, too close to the 1e-8 target when
+    # a solve path shifts; half of each keeps every system inside it
+    thr, ethr = 5e-7, 5e-9
     # untimed warm-up of the mixed path: the GEMM routes of every shape are timed once per process
     t0 = time.perf_counter()
     solve_ground_states(systems, precision=MIXED, device=local, workers=1, max_iterations=80,
-                        omega_threshold=1e-6, energy_threshold=1e-8)
+                        omega_threshold=thr, energy_threshold=ethr)
     tune_s = time.perf_counter() - t0
     runs = {}
     for name, prec, workers in (("mixed_batched", MIXED, args.workers), ("fp64_sequential", FP64, 1),
@@ -671,7 +675,7 @@ def batch_summary(args, rank=0, local=0, world=1):
         barrier(world)
         t0 = time.perf_counter()
         e, it, st, _ = solve_ground_states(systems, precision=prec, device=local, workers=workers,
-                                           max_iterations=80, omega_threshold=1e-6, energy_threshold=1e-8)
+                                           max_iterations=80, omega_threshold=thr, energy_threshold=ethr)
         torch.cuda.synchronize()
         dt = max_over_ranks(time.perf_counter() - t0, world)
         runs[name] = (dt, e, st)
@@ -682,6 +686,7 @@ def batch_summary(args, rank=0, local=0, world=1):
             "n_gpus": world, "workers": args.workers, "systems_per_s": sps,
             "untimed_warmup_s": round(tune_s, 3),
             "speedup_vs_sequential_fp64": round(runs["fp64_sequential"][0] / runs["mixed_batched"][0], 3),
+            "thresholds": {"omega": thr, "energy": ethr}, "target": "|dE| <= 1e-8 Eh vs FP64 converged to 1e-9",
             "max_abs_dE_mixed": de, "max_abs_dE_fp64": de64, "target_met": bool(de <= 1e-8),
             "all_converged": all(bool((r[2] == 0).all()) for r in runs.values()) and bool((st_ref == 0).all())}
 

@@ -42,7 +42,7 @@ class CCSDGPUError(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("ladder_batch", ctypes.c_int64),
                 ("mixed_min_flops", ctypes.c_int64), ("mixed_k_chunk", ctypes.c_int64),
-                ("autotune", ctypes.c_int64), ("reserved", ctypes.c_int64 * 3)]
+                ("autotune", ctypes.c_int64), ("ladder_pair_budget", ctypes.c_int64), ("reserved", ctypes.c_int64 * 2)]
 
 
 class DavidsonOptions(ctypes.Structure):
@@ -159,7 +159,7 @@ class CCSD:
     """One Cholesky-factored closed-shell CCSD system resident on one GPU."""
 
     def __init__(self, n_o, n_v, n_J, *, precision=FP64, device=0, ladder_batch=0, mixed_min_flops=0,
-                 mixed_k_chunk=0, autotune=0):
+                 mixed_k_chunk=0, autotune=0, ladder_pair_budget=0):
         self.lib = load_library()
         self.n_o, self.n_v, self.n_J = int(n_o), int(n_v), int(n_J)
         self.n_mo = self.n_o + self.n_v
@@ -167,7 +167,8 @@ class CCSD:
         self.n_t2 = self.n_t1 * (self.n_t1 + 1) // 2
         self.n_amp = self.n_t1 + self.n_t2
         opt = Options(device=device, precision=precision, ladder_batch=ladder_batch,
-                      mixed_min_flops=mixed_min_flops, mixed_k_chunk=mixed_k_chunk, autotune=autotune)
+                      mixed_min_flops=mixed_min_flops, mixed_k_chunk=mixed_k_chunk, autotune=autotune,
+                      ladder_pair_budget=ladder_pair_budget)
         ctx = _VP()
         rc = self.lib.ccsd_gpu_create(self.n_o, self.n_v, self.n_J, ctypes.byref(opt), ctypes.byref(ctx))
         if rc != 0:

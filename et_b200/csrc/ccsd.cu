@@ -72,6 +72,7 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
         ex.autotune = at > 0 || (at == 0 && !(opt && opt->mixed_min_flops > 0) && !(env && env[0] == '0'));
     }
     ladder_batch = opt ? opt->ladder_batch : 0;
+    ladder_pair_budget = opt ? opt->ladder_pair_budget : 0;
     cudaStream_t s = ex.stream;
     for (auto *b : {&L_oo, &Lt_oo}) *b = dalloc(nJ * no * no, s);
     for (auto *b : {&L_ov, &Lt_ov}) *b = dalloc(nJ * no * nv, s);
@@ -352,6 +353,42 @@ void Context::set_precision(int32_t precision) {
 // (untransformed = true) stay valid until the Cholesky vectors change, so the mixed residual forms
 // them once per Cholesky set; any other L_vv (T1-transformed, or transposed for the adjoint) is
 // formed once per call and shared by all vectors of that call.
+// split L_vv rows r = c + nv a (K = J) as bf16 planes [np][pad(nv^2)][pad(J)]
+DBuf Context::split_lvv_rows(const double *Lvv) {
+    const int np = ex.planes;
+    cudaStream_t s = ex.stream;
+    const int64_t nv2 = nv * nv, Jp = tc_pad_k(nJ), l_rows = tc_pad_rows_a(nv2);
+    DBuf LS(sizeof(__nv_bfloat16) * np * l_rows * Jp, s);
+    // r = c + nv a  ->  offset nJ*(a + nv*c): not a single stride, so split from the (J, c, a) copy
+    DBuf LT = dalloc(nJ * nv2, s);
+    TV src = tv(Lvv, {nJ, nv, nv});   // [J, a, c]
+    TV dst;
+    dst.p = LT.d();
+    dst.nd = 3;
+    dst.n[0] = nJ;
+    dst.n[1] = nv;
+    dst.n[2] = nv;
+    dst.s[0] = 1;
+    dst.s[1] = nJ * nv;   // a
+    dst.s[2] = nJ;        // c
+    permute_add(ex, 1.0, src, 0.0, dst);
+    split_rows(ex, LT.d(), nJ, 1, nv2, nJ, l_rows, Jp, LS.as<__nv_bfloat16>());
+    return LS;
+}
+
+// Whether the split-bf16 pair integrals of all v(v+1)/2 pairs stay resident: they must fit the
+// budget (ccsd_gpu_options.ladder_pair_budget, else half of the free device memory).  Otherwise the
+// ladder forms them block by block in every call (ladder_tc_streamed), as eT's omega_ccsd_a2 does.
+bool Context::ladder_pairs_resident() {
+    const int64_t nab = nv * (nv + 1) / 2;
+    const double need = 2.0 * ex.planes * (double)tc_pad_rows_a(nab) * (double)tc_pad_k(nv * nv);
+    if (ladder_pair_budget > 0) return need <= (double)ladder_pair_budget;
+    if (mbuf_bytes >= need) return true;
+    size_t free_b = 0, total_b = 0;
+    CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    return need <= 0.5 * (double)free_b;
+}
+
 void Context::ladder_pairs(const double *Lvv, bool untransformed) {
     const int np = ex.planes;
     if (untransformed && mbuf_kind == 1 && mbuf_version == l_version && mbuf_planes == np) return;
@@ -363,25 +400,8 @@ void Context::ladder_pairs(const double *Lvv, bool untransformed) {
     cudaStream_t s = ex.stream;
     const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2;
     const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
-    // split L_vv rows r = c + nv a (K = J): source element (r, J) = L[J, a, c] at J + nJ (a + nv c)
     const int64_t l_rows = tc_pad_rows_a(nv2);
-    DBuf LS(sizeof(__nv_bfloat16) * np * l_rows * Jp, s);
-    {
-        // r = c + nv a  ->  offset nJ*(a + nv*c): not a single stride, so split from the (J, c, a) copy
-        DBuf LT = dalloc(nJ * nv2, s);
-        TV src = tv(Lvv, {nJ, nv, nv});   // [J, a, c]
-        TV dst;
-        dst.p = LT.d();
-        dst.nd = 3;
-        dst.n[0] = nJ;
-        dst.n[1] = nv;
-        dst.n[2] = nv;
-        dst.s[0] = 1;
-        dst.s[1] = nJ * nv;   // a
-        dst.s[2] = nJ;        // c
-        permute_add(ex, 1.0, src, 0.0, dst);
-        split_rows(ex, LT.d(), nJ, 1, nv2, nJ, l_rows, Jp, LS.as<__nv_bfloat16>());
-    }
+    DBuf LS = split_lvv_rows(Lvv);
     // all pair integrals, resident: [np][mrows][Kq] (padding rows / K positions are never written, so
     // they stay zero when the plane count changes)
     const int64_t mrows = tc_pad_rows_a(nab);
@@ -420,8 +440,63 @@ void Context::ladder_tc_apply(const double *t2, double *om2, int64_t nvec) {
 }
 
 void Context::ladder_tc(const double *Lvv, const double *t2, double *om2, int64_t nvec, bool untransformed) {
+    if (!ladder_pairs_resident()) {
+        if (mbuf) {
+            mbuf.release();
+            mbuf_bytes = 0;
+            mbuf_kind = 0;
+            cache_epoch++;
+        }
+        ladder_tc_streamed(Lvv, t2, om2, nvec);
+        return;
+    }
     ladder_pairs(Lvv, untransformed);
     ladder_tc_apply(t2, om2, nvec);
+}
+
+// The same ladder with bounded memory: the pair rows of a block of consecutive a (at most
+// ladder_block_rows() rows) are formed into one buffer by the pair-integral GEMM and contracted with
+// [T+; T-] right away (omega_ccsd_a2's (a, b) batching on the tensor cores, omega_ccsd.F90:236-458).
+// Every output element is the dot product it is in the resident form (one K split, the same K
+// chunks), so the result equals the resident ladder's bit for bit.
+void Context::ladder_tc_streamed(const double *Lvv, const double *t2, double *om2, int64_t nvec) {
+    cudaStream_t s = ex.stream;
+    const int np = ex.planes;
+    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
+    const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2), l_rows = tc_pad_rows_a(nv2);
+    DBuf LS = split_lvv_rows(Lvv);
+    const int64_t rows_T = tc_pad_rows_b(nvec * nrow);
+    DBuf TS(sizeof(__nv_bfloat16) * np * rows_T * Kq, s);
+    build_T(ex, t2, nvec, no, nv, rows_T, Kq, np, TS.as<__nv_bfloat16>());
+    DBuf W = dalloc(nab * nvec * nrow, s);
+    // rows of one block: the budget (or half of the free memory) over the bytes of one pair row, and
+    // at least the rows of the largest a
+    int64_t budget = ladder_pair_budget;
+    if (budget <= 0) {
+        size_t free_b = 0, total_b = 0;
+        CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
+        budget = (int64_t)(0.25 * (double)free_b);
+    }
+    const int64_t row_bytes = 2 * np * Kq;
+    const int64_t max_rows = std::max<int64_t>(nv, budget / row_bytes - 128);
+    const int64_t Rp_max = tc_pad_rows_a(max_rows);
+    DBuf P(sizeof(__nv_bfloat16) * np * Rp_max * Kq, s);
+    // K positions beyond nv^2 are never written and must read as zero
+    CU_CHECK(cudaMemsetAsync(P.as<void>(), 0, P.bytes(), s));
+    const int64_t nA = ladder_batch > 0 ? ladder_batch : 16;
+    for (int64_t a0 = 0; a0 < nv;) {
+        int64_t a1 = a0 + 1;
+        while (a1 < nv && (a1 + 1) * (a1 + 2) / 2 - a0 * (a0 + 1) / 2 <= max_rows) a1++;
+        const int64_t row0 = a0 * (a0 + 1) / 2, R = a1 * (a1 + 1) / 2 - row0;
+        for (int64_t b0 = a0; b0 < a1; b0 += nA)
+            tc_gemm_pairs(ex, LS.as<__nv_bfloat16>(), l_rows, Jp, nv, b0, std::min(a1, b0 + nA), P.as<__nv_bfloat16>(),
+                          Rp_max, Kq, nJ, row0);
+        tc_gemm_f64(ex, P.as<__nv_bfloat16>(), Rp_max, TS.as<__nv_bfloat16>(), rows_T, Kq, R, nvec * nrow, nv2, 1.0,
+                    0.0, W.d() + row0, nab, 1);
+        a0 = a1;
+    }
+    for (int64_t v = 0; v < nvec; v++) add_omega_T(ex, om2 + v * nt2, W.d() + v * nrow * nab, nab, no, nv);
+    ex.flops += double(nv2) * double(nv2 + 1) * double(nJ) + 2.0 * double(nab) * double(nvec * nrow) * double(nv2);
 }
 
 // Mixed precision keeps the ovvv integrals of the untransformed Cholesky vectors resident as split

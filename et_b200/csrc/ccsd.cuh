@@ -36,6 +36,7 @@ struct Context {
     GemmProfile prof;
     TermLog terms;                  // per-term device times under eT's labels (ccsd_gpu_set_term_timing)
     int64_t ladder_batch = 0;
+    int64_t ladder_pair_budget = 0;  // bytes the resident split-bf16 pair integrals may take (0 = automatic)
     double e_hf = 0.0;
     bool have_L = false, have_h = false, have_t = false;
     std::string err;
@@ -156,6 +157,9 @@ struct Context {
     // n_t2); the integrals are formed once per call
     void ladder(const double *Lvv, const double *t2, double *om2, int64_t nvec = 1);
     void ladder_tc(const double *Lvv, const double *t2, double *om2, int64_t nvec, bool untransformed);
+    DBuf split_lvv_rows(const double *Lvv);
+    bool ladder_pairs_resident();
+    void ladder_tc_streamed(const double *Lvv, const double *t2, double *om2, int64_t nvec);
     void ladder_pairs(const double *Lvv, bool untransformed);
     void ladder_tc_apply(const double *t2, double *om2, int64_t nvec);
     // the residual's ladder in mixed precision from untransformed integrals plus t1 corrections

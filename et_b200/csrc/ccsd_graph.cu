@@ -337,7 +337,7 @@ void Context::omega_eager(double *om_out) {
 void Context::prepare_residual_caches() {
     g_ovov_const();
     if (ex.prec == Prec::MIXED) {
-        ladder_pairs(L_vv.d(), true);
+        if (ladder_pairs_resident()) ladder_pairs(L_vv.d(), true);
         if (ovvv_resident()) ovvv_pairs();
     } else if (f64_resident()) {
         f64_integrals();

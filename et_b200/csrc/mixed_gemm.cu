@@ -119,6 +119,7 @@ struct EpiPairs {
     __nv_bfloat16 *out;
     size_t plane;
     long long ldk;
+    long long row0;   // pair row of out's first row (a buffer holding a block of pair rows)
     int nv, a0, M, N, np;
     int a, c;
     __device__ __forceinline__ void tile_setup(int) {}
@@ -135,7 +136,7 @@ struct EpiPairs {
         if (row >= M || col >= N) return;
         const int b = col / nv, d = col - b * nv;
         if (b > a) return;
-        const size_t idx = (size_t)((long long)a * (a + 1) / 2 + b) * ldk + c + (long long)nv * d;
+        const size_t idx = (size_t)((long long)a * (a + 1) / 2 + b - row0) * ldk + c + (long long)nv * d;
         store_split_planes(out, plane, idx, v, np);
     }
 };
@@ -652,9 +653,12 @@ void tc_gemm_ovvv(Exec &ex, const __nv_bfloat16 *Lov, int64_t ov_rows, const __n
 }
 
 void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,
-                   __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld, int64_t k_true) {
+                   __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld, int64_t k_true, int64_t row0) {
+    REQUIRE(row0 <= a0 * (a0 + 1) / 2 && a1 * (a1 + 1) / 2 - row0 <= out_rows_pad, CCSD_GPU_EINVAL,
+            "tc_gemm_pairs: pair rows outside the buffer");
     EpiPairs epi{};
     epi.out = out;
+    epi.row0 = row0;
     epi.plane = (size_t)out_rows_pad * (size_t)out_ld;
     epi.ldk = out_ld;
     epi.nv = (int)nv;

@@ -377,6 +377,60 @@ __global__ void oz_digits_kernel(const double *__restrict__ src, long long sr, l
     }
 }
 
+// The same two steps for operands whose K index is contiguous (element (r, k) at src[r sr + k]):
+// no transpose is needed, so the rows stream through with 16-byte loads.  One warp per (row, K
+// slice) for the exponents; for the digits each thread takes 8 consecutive k of a row and writes one
+// 8-byte word per digit plane.
+__global__ void oz_rowexp_kfast_kernel(const double *__restrict__ src, long long sr, int R, int K, int kslices,
+                                       int *__restrict__ e) {
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int per = (K + kslices - 1) / kslices;
+    for (long long w = wid; w < (long long)R * kslices; w += nwarps) {
+        const int r = (int)(w / kslices), sl = (int)(w - (long long)r * kslices);
+        const int k0 = sl * per, k1 = min(K, k0 + per);
+        const double *row = src + (long long)r * sr;
+        double m = 0.0;
+        for (int k = k0 + lane; k < k1; k += 32) m = fmax(m, fabs(__ldg(row + k)));
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0 && m > 0.0) {
+            int ex;
+            frexp(m, &ex);
+            atomicMax(&e[r], ex);
+        }
+    }
+}
+
+__global__ void oz_digits_kfast_kernel(const double *__restrict__ src, long long sr, int R, int K, int Rp, int Kp,
+                                       int digits, const int *__restrict__ e, int8_t *__restrict__ out) {
+    const size_t plane = (size_t)Rp * Kp;
+    const int per_row = Kp / 8;
+    const long long total = (long long)Rp * per_row;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / per_row), k0 = (int)(idx - (long long)r * per_row) * 8;
+        double y[8];
+        const int er = r < R ? e[r] : 0;
+        const bool live = r < R && er > -1100;
+        const double *row = src + (long long)r * sr;
+#pragma unroll
+        for (int j = 0; j < 8; j++) y[j] = (live && k0 + j < K) ? ldexp(__ldg(row + k0 + j), -er) : 0.0;   // |y| < 1
+        int8_t *o = out + (size_t)r * Kp + k0;
+        for (int t = 0; t < digits; t++) {
+            uint64_t word = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                y[j] *= 128.0;
+                const double d = trunc(y[j]);
+                y[j] -= d;
+                word |= (uint64_t)(uint8_t)(int8_t)(int)d << (8 * j);
+            }
+            *reinterpret_cast<uint64_t *>(o + t * plane) = word;
+        }
+    }
+}
+
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
@@ -407,6 +461,16 @@ int num_sms() {
 void row_exponents(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int *e) {
     // start every exponent below any frexp exponent: 0x80 bytes = -2139062144
     CU_CHECK(cudaMemsetAsync(e, 0x80, sizeof(int) * (size_t)Rp, ex.stream));
+    if (sk == 1) {
+        // K slices so that every row has a few warps when rows are few
+        const int kslices = (int)std::max<int64_t>(1, std::min<int64_t>((K + 1023) / 1024, (148 * 64 + R - 1) / R));
+        const int64_t warps = R * kslices;
+        const int blocks = (int)std::min<int64_t>((warps + 7) / 8, 148 * 16);
+        oz_rowexp_kfast_kernel<<<blocks, 256, 0, ex.stream>>>(src, sr, (int)R, (int)K, kslices, e);
+        ex.launches++;
+        CU_CHECK(cudaGetLastError());
+        return;
+    }
     const int64_t rb = (R + 31) / 32;
     // enough blocks over K to fill the GPU when there are few row blocks
     const int64_t kb = std::max<int64_t>(1, std::min<int64_t>((K + 31) / 32, (4 * 148 + rb - 1) / rb));
@@ -419,6 +483,14 @@ void row_exponents(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t 
 // digits [digits][Rp][Kp] of the K slab of a strided view (the exponents are those of whole rows)
 void slab_digits(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
                  int digits, const int *e, int8_t *out) {
+    if (sk == 1) {
+        const int64_t total = Rp * (Kp / 8);
+        const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+        oz_digits_kfast_kernel<<<blocks, 256, 0, ex.stream>>>(src, sr, (int)R, (int)K, (int)Rp, (int)Kp, digits, e, out);
+        ex.launches++;
+        CU_CHECK(cudaGetLastError());
+        return;
+    }
     oz_digits_kernel<<<dim3((unsigned)(Rp / 32), (unsigned)std::min<int64_t>(Kp / 32, 65535)), dim3(32, 8), 0,
                        ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, digits, e, out);
     ex.launches++;

@@ -66,7 +66,11 @@ typedef struct ccsd_gpu_options {
                                     K-split count) timed once per process: 1 on, -1 off (fixed flop
                                     threshold and split rule), 0 = on unless mixed_min_flops is given
                                     or the environment sets CCSD_GPU_AUTOTUNE=0 */
-    int64_t reserved[3];
+    int64_t ladder_pair_budget;  /* MIXED only: bytes the split-bf16 A2 pair integrals of all v(v+1)/2 pairs
+                                    may take when kept on the device (0 = half of the free memory);
+                                    beyond it they are formed block by block in every call into a buffer
+                                    of at most this size (eT's (a, b) batching of omega_ccsd_a2) */
+    int64_t reserved[2];
 } ccsd_gpu_options;
 
 typedef struct ccsd_gpu_solver_options {

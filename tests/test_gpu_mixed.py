@@ -213,3 +213,27 @@ def test_mixed_singles_jacobian_with_t1_matches_fp64(dims):
             assert err <= 1e-4 * np.linalg.norm(r64)
             if which == 0:
                 assert err <= 1e-3 * ladder_t1, (err, ladder_t1)
+
+
+@pytest.mark.parametrize("dims", [(5, 19, 33), (6, 40, 90)])
+def test_streamed_ladder_equals_resident(dims):
+    """A pair-integral budget below the resident size forms the split-bf16 ladder integrals block by
+    block in every call (eT's (a, b) batching).  With one K split (the fixed GEMM rule) every output
+    element is the same dot product, so Omega, A c and A^T b equal the resident form's bit for bit,
+    for one a per block (budget 1 byte) and for blocks of several a."""
+    from et_b200 import CCSD, MIXED
+    n_o, n_v, n_J = dims
+    s = make_system(n_o, n_v, n_J, seed=23)
+    rng = np.random.default_rng(4)
+    row_bytes = 2 * 2 * ((n_v * n_v + 63) // 64 * 64)
+    res = {}
+    for budget in (0, 1, (3 * n_v + 128) * row_bytes):
+        with CCSD(n_o, n_v, n_J, precision=MIXED, mixed_min_flops=1, ladder_pair_budget=budget) as g:
+            g.set_system(s.L_mo, s.h_mo, s.eps)
+            amp = 0.05 * np.random.default_rng(4).standard_normal(g.n_amp)
+            g.set_amplitudes(amp)
+            C = np.random.default_rng(5).standard_normal((g.n_amp, 2))
+            res[budget] = (g.construct_omega(), g.jacobian_transformation(C), g.jacobian_transpose_transformation(C))
+    for budget in list(res)[1:]:
+        for x, y in zip(res[0], res[budget]):
+            assert np.array_equal(x, y), budget
