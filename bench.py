@@ -147,18 +147,17 @@ def load_peaks():
         return 1590.0, 1400.0, 6650.0, "fallback"
 
 
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "launch_list_gs_iteration_o32_v320_J1200_mixed.md")
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "tc_gemm_bf16x3_c2d2_10240cubed_full.md")
 
 
-def gemm_traffic(n_o, n_v, n_J):
-    """DRAM bytes per tensor-core GEMM launch (read + write) from the committed ncu launch list of
-    this workload (o=32 v=320 N_J=1200), or None for other sizes."""
-    if (n_o, n_v, n_J) != (32, 320, 1200):
-        return None
+def gemm_traffic(issued_flops_per_launch):
+    """DRAM bytes (read + write) of an average tensor-core GEMM launch: the committed single-kernel
+    ncu capture's bytes per issued FLOP (10240^3, profiles/) times the launch's issued FLOPs, or None
+    when the capture summary is missing."""
     try:
         for line in open(TRAFFIC_PROFILE):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":")[1])
+            if line.startswith("dram_bytes_per_issued_pflop:"):
+                return float(line.split(":")[1]) * issued_flops_per_launch / 1e15
     except OSError:
         pass
     return None
@@ -285,8 +284,10 @@ def run_gpu(args):
         roof = {"kernel": "split_bf16_gemm_kernel (tcgen05 split-BF16 GEMM)", "bound": "tensor",
                 "achieved": round(achieved, 2), "peak": peak_sust, "unit": "TFLOP/s",
                 "frac": round(achieved / peak_sust, 4), "peak_kind": f"{peak_kind} bf16 sustained (timed inside a long step)",
-                "traffic": gemm_traffic(n_o, n_v, n_J), "traffic_source": "ncu launch list (profiles/), "
-                "DRAM read + write bytes per GEMM launch", "launches": n_gemm, "avg_launch_ms": round(gemm_ms / n_gemm, 4),
+                "traffic": gemm_traffic(gemm_flops / n_gemm),
+                "traffic_source": "DRAM read + write bytes per issued FLOP of the single-launch ncu capture "
+                                  "(profiles/tc_gemm_bf16x3_c2d2_10240cubed_full.md) times the window's average "
+                                  "issued FLOPs per launch", "launches": n_gemm, "avg_launch_ms": round(gemm_ms / n_gemm, 4),
                 "share_of_step": round(gemm_ms / ms, 4),
                 "flops_counted": "issued tensor flops: 3 bf16 products x 2mnk per launch"}
 

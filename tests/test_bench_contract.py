@@ -16,11 +16,12 @@ def _bench():
     return bench
 
 
-def test_roofline_traffic_comes_from_the_committed_launch_list():
+def test_roofline_traffic_comes_from_the_committed_capture():
+    """bytes per issued FLOP of the committed 10240^3 capture, scaled to a launch's issued FLOPs"""
     bench = _bench()
-    traffic = bench.gemm_traffic(32, 320, 1200)
-    assert traffic is not None and 1e9 < traffic < 1e11
-    assert bench.gemm_traffic(8, 40, 100) is None
+    per_10240 = bench.gemm_traffic(6.0 * 10240 ** 3)
+    assert per_10240 is not None and 5e9 < per_10240 < 1e10
+    assert abs(bench.gemm_traffic(3.0 * 10240 ** 3) - 0.5 * per_10240) < 1.0
 
 
 def test_reference_arm_prints_one_contract_line():
