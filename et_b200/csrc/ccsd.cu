@@ -55,6 +55,12 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
         use_graphs = g && g[0] == '1';
         const char *r = std::getenv("CCSD_GPU_FP64_RESIDENT");
         f64_resident_on = !(r && r[0] == '0');
+        // digits of the first-order FP64 terms of the mixed residual: CCSD_GPU_MIXED_FP64_DIGITS=0 keeps
+        // them on cuBLAS DGEMM
+        if (const char *d = std::getenv("CCSD_GPU_MIXED_FP64_DIGITS")) {
+            const int v = std::atoi(d);
+            ex.mixed_fp64_digits = (v >= 4 && v <= 7) ? v : 0;
+        }
     }
     ex.blas = blas;
     ex.prof = &prof;
@@ -85,6 +91,10 @@ Context::Context(int64_t no_, int64_t nv_, int64_t nJ_, const ccsd_gpu_options *
     hb_vv = dalloc(nv * nv, s);
     eps = dalloc(nmo, s);
     F = dalloc(nmo * nmo, s);
+    fb_oo = dalloc(no * no, s);
+    fb_ov = dalloc(no * nv, s);
+    fb_vo = dalloc(nv * no, s);
+    fb_vv = dalloc(nv * nv, s);
     t = dalloc(namp, s);
     epsdiff = dalloc(namp, s);
     scal = dalloc(64, s);
@@ -102,7 +112,7 @@ Context::~Context() {
     if (graphs_captured) cudaDeviceGraphMemTrim(device);   // the physical memory the residual graphs held
     for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
                     &mbuf, &ybuf, &om_stage, &f64_gp, &f64_gm, &f64_ovvv, &hb_oo, &hb_ov, &hb_vo, &hb_vv,
-                    &gemm_err, &digit_arena})
+                    &gemm_err, &digit_arena, &fb_oo, &fb_ov, &fb_vo, &fb_vv})
         b->release();
     if (blas) cublasDestroy(blas);
     blas = nullptr;
@@ -217,8 +227,17 @@ void Context::refresh() {
     {
         TermTimer tt(ex, "Fock matrix construction (T1 basis)");
         construct_fock();
+        auto blk = [&](DBuf &dst, int64_t r0, int64_t c0, int64_t nr, int64_t nc) {
+            CU_CHECK(cudaMemcpy2DAsync(dst.d(), sizeof(double) * nr, F.d() + r0 + nmo * c0, sizeof(double) * nmo,
+                                       sizeof(double) * nr, nc, cudaMemcpyDeviceToDevice, ex.stream));
+        };
+        blk(fb_oo, 0, 0, no, no);
+        blk(fb_ov, 0, no, no, nv);
+        blk(fb_vo, no, 0, nv, no);
+        blk(fb_vv, no, no, nv, nv);
     }
     ex.prec = keep;
+    t1_current = true;
 }
 
 // g_ovov[i,a,j,b] = sum_J L_ia L_jb  (eri_t1%get('ovov'))
@@ -910,6 +929,7 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         }
         // quasi-Newton step (quasi_newton_updater_class.F90, amplitude_updater_class.F90)
         qn_update(ex, omega_v.d(), epsdiff.d(), t.d(), namp, nt1);
+        t1_current = false;   // the next iteration's refresh() transforms with the new t1
         // diis%update(e = scaled preconditioned residual, x = updated amplitudes)
         if (reset_diis) {
             order.clear();

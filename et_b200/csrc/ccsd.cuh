@@ -47,6 +47,10 @@ struct Context {
     DBuf L_oo, L_ov, L_vo, L_vv;
     DBuf Lt_oo, Lt_ov, Lt_vo, Lt_vv;
     DBuf h, eps, F;          // h_mo, orbital energies, T1 Fock (n_mo x n_mo)
+    DBuf fb_oo, fb_ov, fb_vo, fb_vv;   // the T1 Fock matrix in o/v blocks (contiguous)
+    // Lt_* and F hold the T1 transformation of the current t1 (set by refresh(), cleared when the
+    // solver moves t): the plain residual then takes them as inputs instead of recording them
+    bool t1_current = false;
     DBuf hb_oo, hb_ov, hb_vo, hb_vv;   // MO h in o/v blocks
     DBuf t;                  // [t1 | packed t2]
     DBuf epsdiff;            // orbital differences (n_amp)
@@ -130,7 +134,9 @@ struct Context {
     void prepare_residual_caches();          // builds what a captured residual only reads
     void capture_residual(ResidualGraph &G, double *d_omega);
     // const_ovov: take g_iajb from the cache (no derivative flows into L_ov through it)
-    OmegaNodes record_omega(Graph &g, bool const_ovov = true);
+    // const_t1: take the T1-transformed blocks and the Fock matrix from the context (only when no
+    // derivative will be taken and t1_current holds)
+    OmegaNodes record_omega(Graph &g, bool const_ovov = true, bool const_t1 = false);
     void record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv_in, int tf);
     void ladder_y(const double *Lvv, const double *tfull, double *Y);
     // mixed precision: whether the resident ovvv planes fit, their construction, and

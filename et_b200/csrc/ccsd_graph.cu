@@ -66,7 +66,7 @@ __global__ void join_amp_kernel(const double *__restrict__ x1, const double *__r
 // ---------------------------------------------------------------------------
 // Omega on the graph
 // ---------------------------------------------------------------------------
-OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
+OmegaNodes Context::record_omega(Graph &g, bool const_ovov, bool const_t1) {
     OmegaNodes n{};
     g.nov = nov;
     const std::vector<int64_t> V4 = {nv, no, nv, no};
@@ -82,49 +82,65 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov) {
     n.h_vv = g.input("h_vv", {nv, nv}, hb_vv.d());
     const int t1 = n.t1;
 
-    // construct_t1_cholesky (src/wavefunctions/ccs/t1_ccs.F90:208-499); the ov block is unchanged
-    auto t1_timer = std::make_unique<TermTimer>(ex, "T1 transform cholesky");
-    const int Lt_ov = g.alias(n.L_ov);
-    const int Lt_oo = g.zeros("Lt_oo", {nJ, no, no});
-    g.permute(Lt_oo, "Jij->Jij", 1.0, n.L_oo);
-    g.contract(Lt_oo, "Jia,aj->Jij", 1.0, n.L_ov, t1, true);
-    const int Lt_vo = g.zeros("Lt_vo", {nJ, nv, no});
-    g.permute(Lt_vo, "Jai->Jai", 1.0, n.L_vo);
-    g.contract(Lt_vo, "Jab,bi->Jai", 1.0, n.L_vv, t1, true);
-    g.contract(Lt_vo, "aj,Jji->Jai", -1.0, t1, Lt_oo, true);
-    const int Lt_vv = g.zeros("Lt_vv", {nJ, nv, nv});
-    g.permute(Lt_vv, "Jab->Jab", 1.0, n.L_vv);
-    g.contract(Lt_vv, "aj,Jjb->Jab", -1.0, t1, n.L_ov, true);
-    n.Lt_vv = Lt_vv;
-    t1_timer.reset();
+    int Lt_ov, Lt_oo, Lt_vo, Lt_vv, F_oo, F_ov, F_vo, F_vv;
+    if (const_t1) {
+        // the context transformed the blocks and built the Fock matrix at this t1 (refresh())
+        Lt_oo = g.input("Lt_oo", {nJ, no, no}, this->Lt_oo.d());
+        Lt_ov = g.input("Lt_ov", {nJ, no, nv}, this->Lt_ov.d());
+        Lt_vo = g.input("Lt_vo", {nJ, nv, no}, this->Lt_vo.d());
+        Lt_vv = g.input("Lt_vv", {nJ, nv, nv}, this->Lt_vv.d());
+        F_oo = g.input("F_oo", {no, no}, fb_oo.d());
+        F_ov = g.input("F_ov", {no, nv}, fb_ov.d());
+        F_vo = g.input("F_vo", {nv, no}, fb_vo.d());
+        F_vv = g.input("F_vv", {nv, nv}, fb_vv.d());
+        n.Lt_vv = Lt_vv;
+    } else {
+        // construct_t1_cholesky (src/wavefunctions/ccs/t1_ccs.F90:208-499); the ov block is unchanged
+        auto t1_timer = std::make_unique<TermTimer>(ex, "T1 transform cholesky");
+        Lt_ov = g.alias(n.L_ov);
+        Lt_oo = g.zeros("Lt_oo", {nJ, no, no});
+        g.permute(Lt_oo, "Jij->Jij", 1.0, n.L_oo);
+        g.contract(Lt_oo, "Jia,aj->Jij", 1.0, n.L_ov, t1, true);
+        Lt_vo = g.zeros("Lt_vo", {nJ, nv, no});
+        g.permute(Lt_vo, "Jai->Jai", 1.0, n.L_vo);
+        g.contract(Lt_vo, "Jab,bi->Jai", 1.0, n.L_vv, t1, true);
+        g.contract(Lt_vo, "aj,Jji->Jai", -1.0, t1, Lt_oo, true);
+        Lt_vv = g.zeros("Lt_vv", {nJ, nv, nv});
+        g.permute(Lt_vv, "Jab->Jab", 1.0, n.L_vv);
+        g.contract(Lt_vv, "aj,Jjb->Jab", -1.0, t1, n.L_ov, true);
+        n.Lt_vv = Lt_vv;
+        t1_timer.reset();
 
-    // T1 Fock matrix in blocks (fock_ccs.F90:242-1107): h~ = (1 - t1) h (1 + t1) then
-    // F_pq = h~_pq + 2 sum_J L~_pq X_J - sum_Jk L~_pk L~_kq, X_J = sum_k L~_kk
-    auto fock_timer = std::make_unique<TermTimer>(ex, "Fock matrix construction (T1 basis)");
-    const int F_oo = g.zeros("F_oo", {no, no}), F_ov = g.zeros("F_ov", {no, nv});
-    const int F_vo = g.zeros("F_vo", {nv, no}), F_vv = g.zeros("F_vv", {nv, nv});
-    g.permute(F_oo, "ij->ij", 1.0, n.h_oo);
-    g.contract(F_oo, "ia,aj->ij", 1.0, n.h_ov, t1, true);          // h~_oo = h_oo + h_ov t1
-    g.permute(F_ov, "ia->ia", 1.0, n.h_ov);                          // h~_ov = h_ov
-    g.permute(F_vv, "ab->ab", 1.0, n.h_vv);
-    g.contract(F_vv, "ai,ib->ab", -1.0, t1, n.h_ov, true);          // h~_vv = h_vv - t1 h_ov
-    const int Woo = g.zeros("W_oo", {no, no});
-    g.permute(Woo, "ij->ij", 1.0, n.h_oo);
-    g.contract(Woo, "ia,aj->ij", 1.0, n.h_ov, t1, true);
-    g.permute(F_vo, "ai->ai", 1.0, n.h_vo);
-    g.contract(F_vo, "ab,bi->ai", 1.0, n.h_vv, t1, true);
-    g.contract(F_vo, "aj,ji->ai", -1.0, t1, Woo, true);             // h~_vo = h_vo + h_vv t1 - t1 W_oo
-    const int X = g.zeros("X_J", {nJ});
-    g.trace(X, Lt_oo);
-    g.contract(F_oo, "Jpq,J->pq", 2.0, Lt_oo, X, true);
-    g.contract(F_ov, "Jpq,J->pq", 2.0, Lt_ov, X, true);
-    g.contract(F_vo, "Jpq,J->pq", 2.0, Lt_vo, X, true);
-    g.contract(F_vv, "Jpq,J->pq", 2.0, Lt_vv, X, true);
-    g.contract(F_oo, "Jpk,Jkq->pq", -1.0, Lt_oo, Lt_oo, true);
-    g.contract(F_ov, "Jpk,Jkq->pq", -1.0, Lt_oo, Lt_ov, true);
-    g.contract(F_vo, "Jpk,Jkq->pq", -1.0, Lt_vo, Lt_oo, true);
-    g.contract(F_vv, "Jpk,Jkq->pq", -1.0, Lt_vo, Lt_ov, true);
-    fock_timer.reset();
+        // T1 Fock matrix in blocks (fock_ccs.F90:242-1107): h~ = (1 - t1) h (1 + t1) then
+        // F_pq = h~_pq + 2 sum_J L~_pq X_J - sum_Jk L~_pk L~_kq, X_J = sum_k L~_kk
+        auto fock_timer = std::make_unique<TermTimer>(ex, "Fock matrix construction (T1 basis)");
+        F_oo = g.zeros("F_oo", {no, no});
+        F_ov = g.zeros("F_ov", {no, nv});
+        F_vo = g.zeros("F_vo", {nv, no});
+        F_vv = g.zeros("F_vv", {nv, nv});
+        g.permute(F_oo, "ij->ij", 1.0, n.h_oo);
+        g.contract(F_oo, "ia,aj->ij", 1.0, n.h_ov, t1, true);          // h~_oo = h_oo + h_ov t1
+        g.permute(F_ov, "ia->ia", 1.0, n.h_ov);                          // h~_ov = h_ov
+        g.permute(F_vv, "ab->ab", 1.0, n.h_vv);
+        g.contract(F_vv, "ai,ib->ab", -1.0, t1, n.h_ov, true);          // h~_vv = h_vv - t1 h_ov
+        const int Woo = g.zeros("W_oo", {no, no});
+        g.permute(Woo, "ij->ij", 1.0, n.h_oo);
+        g.contract(Woo, "ia,aj->ij", 1.0, n.h_ov, t1, true);
+        g.permute(F_vo, "ai->ai", 1.0, n.h_vo);
+        g.contract(F_vo, "ab,bi->ai", 1.0, n.h_vv, t1, true);
+        g.contract(F_vo, "aj,ji->ai", -1.0, t1, Woo, true);             // h~_vo = h_vo + h_vv t1 - t1 W_oo
+        const int X = g.zeros("X_J", {nJ});
+        g.trace(X, Lt_oo);
+        g.contract(F_oo, "Jpq,J->pq", 2.0, Lt_oo, X, true);
+        g.contract(F_ov, "Jpq,J->pq", 2.0, Lt_ov, X, true);
+        g.contract(F_vo, "Jpq,J->pq", 2.0, Lt_vo, X, true);
+        g.contract(F_vv, "Jpq,J->pq", 2.0, Lt_vv, X, true);
+        g.contract(F_oo, "Jpk,Jkq->pq", -1.0, Lt_oo, Lt_oo, true);
+        g.contract(F_ov, "Jpk,Jkq->pq", -1.0, Lt_oo, Lt_ov, true);
+        g.contract(F_vo, "Jpk,Jkq->pq", -1.0, Lt_vo, Lt_oo, true);
+        g.contract(F_vv, "Jpk,Jkq->pq", -1.0, Lt_vo, Lt_ov, true);
+        fock_timer.reset();
+    }
 
     // construct_omega_ccsd (src/wavefunctions/ccsd/omega_ccsd.F90:39-110)
     const int om1 = g.zeros("omega1", {nv, no});
@@ -329,7 +345,7 @@ void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv
 
 void Context::omega_eager(double *om_out) {
     Graph g(ex);
-    OmegaNodes n = record_omega(g);
+    OmegaNodes n = record_omega(g, true, t1_current);
     CU_CHECK(cudaMemcpyAsync(om_out, g.value(n.om1), sizeof(double) * nt1, cudaMemcpyDeviceToDevice, ex.stream));
     CU_CHECK(cudaMemcpyAsync(om_out + nt1, g.value(n.om2), sizeof(double) * nt2, cudaMemcpyDeviceToDevice, ex.stream));
 }
@@ -384,6 +400,7 @@ void Context::capture_residual(ResidualGraph &G, double *om_out) {
 
 void Context::omega(double *om_out) {
     REQUIRE(have_t, CCSD_GPU_ESTATE, "amplitudes not set");
+    if (!t1_current) refresh();   // the residual reads the context's T1-transformed blocks
     TermTimer tt(ex, "Construct CCSD Omega");
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CU_CHECK(cudaStreamIsCapturing(ex.stream, &cap));

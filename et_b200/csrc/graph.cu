@@ -109,6 +109,26 @@ __global__ void trace_batch_kernel(const double *__restrict__ a, double *__restr
 
 std::string with_batch(const std::string &labels) { return labels + BATCH; }
 
+// An op recorded as FP64 (the first-order terms of the mixed residual) runs in FP64 arithmetic; in a
+// mixed-precision evaluation its large products go to the int8 digit GEMM (ex.mixed_fp64_digits
+// digits, FP64-accurate) rather than DGEMM, unless the caller already chose the FP64 arithmetic.
+struct Fp64Scope {
+    Exec &ex;
+    Prec prec;
+    int digits;
+    Fp64Scope(Exec &e, bool on) : ex(e), prec(e.prec), digits(e.fp64_digits) {
+        if (!on) return;
+        if (prec == Prec::MIXED && ex.fp64_digits == 0) ex.fp64_digits = ex.mixed_fp64_digits;
+        ex.prec = Prec::FP64;
+    }
+    ~Fp64Scope() {
+        ex.prec = prec;
+        ex.fp64_digits = digits;
+    }
+    Fp64Scope(const Fp64Scope &) = delete;
+    Fp64Scope &operator=(const Fp64Scope &) = delete;
+};
+
 }  // namespace
 
 int Graph::input(const std::string &name, std::vector<int64_t> dims, const double *p) {
@@ -177,8 +197,7 @@ double *Graph::adjoint(int i, int nvec) {
 }
 
 void Graph::run_forward(const GOp &op) {
-    Prec keep = ex_.prec;
-    if (op.fp64) ex_.prec = Prec::FP64;
+    Fp64Scope fp64(ex_, op.fp64);
     switch (op.kind) {
     case OpKind::Contract:
         ccsd::contract(ex_, op.spec.c_str(), op.alpha, view(op.a), view(op.b), 1.0, view(op.out));
@@ -226,7 +245,6 @@ void Graph::run_forward(const GOp &op) {
         break;
     }
     CU_CHECK(cudaGetLastError());
-    ex_.prec = keep;
 }
 
 void Graph::contract(int out, const char *spec, double alpha, int a, int b, bool fp64) {
@@ -340,8 +358,7 @@ void Graph::jvp(const std::vector<int> &inputs, const std::vector<const double *
     }
     for (const GOp &op : ops_) {
         if (!nodes_[op.out].active) continue;
-        Prec keep = ex_.prec;
-        if (op.fp64) ex_.prec = Prec::FP64;
+        Fp64Scope fp64(ex_, op.fp64);
         switch (op.kind) {
         case OpKind::Contract: {
             std::string s = op.spec;
@@ -404,7 +421,6 @@ void Graph::jvp(const std::vector<int> &inputs, const std::vector<const double *
             break;
         }
         CU_CHECK(cudaGetLastError());
-        ex_.prec = keep;
     }
     for (size_t k = 0; k < outputs.size(); k++) {
         const GNode &n = nodes_[outputs[k]];
@@ -427,8 +443,7 @@ void Graph::vjp(const std::vector<int> &outputs, const std::vector<const double 
     for (int oi = (int)ops_.size() - 1; oi >= 0; --oi) {
         const GOp &op = ops_[oi];
         if (!nodes_[op.out].active || !nodes_[op.out].adj) continue;
-        Prec keep = ex_.prec;
-        if (op.fp64) ex_.prec = Prec::FP64;
+        Fp64Scope fp64(ex_, op.fp64);
         switch (op.kind) {
         case OpKind::Contract: {
             std::string s = op.spec;
@@ -494,7 +509,6 @@ void Graph::vjp(const std::vector<int> &outputs, const std::vector<const double 
             break;
         }
         CU_CHECK(cudaGetLastError());
-        ex_.prec = keep;
     }
     for (size_t k = 0; k < inputs.size(); k++) {
         const GNode &n = nodes_[inputs[k]];

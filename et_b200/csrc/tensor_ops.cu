@@ -248,7 +248,7 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
         return;
     }
     if (ex.fp64_digits > 0 && fl >= ex.fp64_digits_min_flops &&
-        (ex.fp64_digits_min_flops <= 1 || (m >= 256 && n >= 256 && k >= 256))) {
+        (ex.fp64_digits_min_flops <= 1 || (m >= 256 && n >= 256 && k >= 512))) {
         ozaki_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, ex.fp64_digits);
         return;
     }
