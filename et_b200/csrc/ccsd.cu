@@ -829,6 +829,17 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     auto trace_ms = [&]() {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - trace_t0).count();
     };
+    // the stream-ordered pool's reserved and used memory (GB), printed with each traced iteration
+    auto trace_pool = [&](double &reserved, double &used) {
+        reserved = used = 0.0;
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return;
+        uint64_t r = 0, u = 0;
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u);
+        reserved = 1e-9 * (double)r;
+        used = 1e-9 * (double)u;
+    };
     double trace_moved = 0.0;
     const char *trace_why = "";
     // shift every stored DIIS error vector by v and rebuild their Gram matrix
@@ -909,8 +920,11 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
             }
         }
         if (trace) {
-            std::fprintf(stderr, "ccsd_gpu gs %3d  E %.12f  |Omega| %.3e  %s  %-6s moved %.3e r_c %.3e  t %.1f ms%s\n", it,
-                         e, nrm, exact ? "fp64 " : "mixed", trace_why, trace_moved, r_c, trace_ms(),
+            double pool_r, pool_u;
+            trace_pool(pool_r, pool_u);
+            std::fprintf(stderr,
+                         "ccsd_gpu gs %3d  E %.12f  |Omega| %.3e  %s  %-6s moved %.3e r_c %.3e  t %.1f ms  pool %.1f/%.1f GB%s\n",
+                         it, e, nrm, exact ? "fp64 " : "mixed", trace_why, trace_moved, r_c, trace_ms(), pool_u, pool_r,
                          fp64_final ? "  fp64 from here" : "");
         }
         if (!std::isfinite(nrm) || !std::isfinite(e)) {

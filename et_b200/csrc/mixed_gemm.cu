@@ -33,8 +33,7 @@ using namespace tc;
 namespace {
 
 constexpr int BM = 128;
-constexpr int BK = 64;                     // one 128-byte swizzle row of bf16
-constexpr int STAGES = 2;
+constexpr int BK = 64;                     // K padding of the planes: one 128-byte swizzle row of bf16
 constexpr int B_ROW_PAD = 256;             // B operand rows are padded to 256 in both modes
 constexpr int THREADS = 192;              // producer warp, MMA warp, four epilogue warps
 constexpr int EPI_THREADS = 128;
@@ -42,14 +41,19 @@ constexpr long long WAIT_CYCLES = 4000000000ll;   // ~2 s at 2 GHz: far above an
 // error codes written to the caller's error word when a bounded wait runs out
 constexpr int ERR_PRODUCER = 1, ERR_MMA_FULL = 2, ERR_EPILOGUE = 3, ERR_MMA_ACC = 4, ERR_DONE = 5, ERR_DRAIN = 6;
 
-// plane count and N tile of one mode
-template <int NP_, int BN_>
+// plane count, N tile, K block of one pipeline stage (64 bf16 in 128-byte swizzled rows, or 32 in
+// 64-byte rows) and stage count of one mode.  Four 48 KB stages of 32-wide blocks measured 5 %
+// slower than two 96 KB stages of 64-wide blocks at 10240^3 and equal at 4096 x 4096 x 1200.
+template <int NP_, int BN_, int KB_ = 64, int STAGES_ = 2>
 struct Mode {
     static constexpr int NP = NP_;
     static constexpr int BN = BN_;
+    static constexpr int KB = KB_;
+    static constexpr int STAGES = STAGES_;
+    static constexpr int ROW_BYTES = 2 * KB;
     static constexpr int NPROD = NP == 2 ? 3 : 6;
-    static constexpr int A_TILE = BM * BK * 2;       // bytes per plane
-    static constexpr int B_TILE = BN * BK * 2;
+    static constexpr int A_TILE = BM * KB * 2;       // bytes per plane
+    static constexpr int B_TILE = BN * KB * 2;
     static constexpr int STAGE_BYTES = NP * (A_TILE + B_TILE);
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
     static constexpr uint32_t TMEM_COLS = 2 * BN;    // two FP32 accumulators of 128 lanes x BN columns
@@ -207,7 +211,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TileMap map,
                    int num_tiles, Epi epi) {
     constexpr int NP = MD::NP, BN = MD::BN, A_TILE = MD::A_TILE, B_TILE = MD::B_TILE;
-    constexpr int STAGE_BYTES = MD::STAGE_BYTES;
+    constexpr int STAGE_BYTES = MD::STAGE_BYTES, STAGES = MD::STAGES, KB = MD::KB;
     constexpr uint32_t TMEM_COLS = MD::TMEM_COLS;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -264,7 +268,7 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
                     issued[s]++;
                     uint8_t *st = smem + s * STAGE_BYTES;
                     mbar_expect_tx(&full[s], STAGE_BYTES);
-                    const int k0 = (kt0 + i) * BK;
+                    const int k0 = (kt0 + i) * KB;
 #pragma unroll
                     for (int p = 0; p < NP; p++) {
                         tma_load_3d(&tmA, &full[s], st + p * A_TILE, k0, m0, p);
@@ -308,13 +312,13 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint8_t *st = smem + s * STAGE_BYTES;
 #pragma unroll
-                    for (int kk = 0; kk < BK / 16; kk++) {
+                    for (int kk = 0; kk < KB / 16; kk++) {
                         const uint32_t ko = kk * 32;   // 16 bf16 = 32 bytes inside the swizzled row
 #pragma unroll
                         for (int p = 0; p < MD::NPROD; p++) {
                             const uint8_t *ta = st + MD::pa(p) * A_TILE;
                             const uint8_t *tb = st + NP * A_TILE + MD::pb(p) * B_TILE;
-                            mma_bf16(d, smem_desc(ta, ko), smem_desc(tb, ko), MD::IDESC,
+                            mma_bf16(d, smem_desc_k<MD::ROW_BYTES>(ta, ko), smem_desc_k<MD::ROW_BYTES>(tb, ko), MD::IDESC,
                                      (i > c0 || kk > 0 || p > 0) ? 1u : 0u);
                         }
                     }
@@ -423,16 +427,19 @@ __global__ void sum_splits_kernel(const double *__restrict__ P, int splits, int6
     }
 }
 
-// planes x rows x K tensor of bf16, box (BK, box_rows, 1); rows beyond `rows` read as zero
-CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t plane_stride, int planes) {
+// planes x rows x K tensor of bf16, box (kb, box_rows, 1) with the swizzle of kb-wide rows; rows
+// beyond `rows` read as zero
+CUtensorMap make_map(void *base, int64_t rows, int64_t Kp, int box_rows, int64_t plane_stride, int planes,
+                     int kb = BK) {
     CUtensorMap m;
     REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, CCSD_GPU_EINVAL, "tensor map base must be 16-byte aligned");
     cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)planes};
     cuuint64_t strides[2] = {(cuuint64_t)Kp * 2, (cuuint64_t)plane_stride * 2};
-    cuuint32_t box[3] = {BK, (cuuint32_t)box_rows, 1};
+    cuuint32_t box[3] = {(cuuint32_t)kb, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     REQUIRE(r == CUDA_SUCCESS, CCSD_GPU_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     return m;
@@ -463,16 +470,16 @@ void launch_mode(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_pla
     REQUIRE(Kp % BK == 0 && Kp > 0 && Mp > 0 && Np > 0, CCSD_GPU_EINVAL, "tc gemm: bad padding");
     CU_CHECK(cudaFuncSetAttribute(split_bf16_gemm_kernel<MD, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   MD::SMEM_BYTES));
-    CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane, MD::NP);
-    CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, MD::BN, b_plane, MD::NP);
+    CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane, MD::NP, MD::KB);
+    CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, MD::BN, b_plane, MD::NP, MD::KB);
     TileMap map;
     map.num_mt = (int)(Mp / BM);
     map.num_nt = (int)(Np / MD::BN);
-    map.nk_all = (int)(Kp / BK);
+    map.nk_all = (int)(Kp / MD::KB);
     map.nks = (map.nk_all + splits - 1) / splits;
     map.bn = MD::BN;
     map.group_m = std::min(map.num_mt, 16);
-    map.kc = (Epi::kChunked && ex.k_chunk > 0) ? (int)std::max<int64_t>(1, ex.k_chunk / BK) : map.nks;
+    map.kc = (Epi::kChunked && ex.k_chunk > 0) ? (int)std::max<int64_t>(1, ex.k_chunk / MD::KB) : map.nks;
     REQUIRE(ex.gemm_err != nullptr, CCSD_GPU_EINVAL, "tc gemm: no error word");
     map.err = ex.gemm_err;
     map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : WAIT_CYCLES;
