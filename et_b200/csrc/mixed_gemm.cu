@@ -372,42 +372,76 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
     }
 }
-// FP64 (strided view of op(X): element (r, k) at src[r*sr + k*sk]) -> np bf16 planes, K-major
-// [plane][R_pad][K_pad], zero padded: plane p holds the bf16 rounding of x minus the planes before
-// it.  32x32 smem tile so both sides stay coalesced; blockIdx.x runs over row blocks (up to
-// 2^31), blockIdx.y strides over K blocks.
-__global__ void split_bf16_kernel(const double *__restrict__ src, long long sr, long long sk, int R, int K, int Rp,
-                                  int Kp, int np, __nv_bfloat16 *__restrict__ out) {
-    __shared__ double tile[32][33];
-    const int r0 = blockIdx.x * 32;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const bool k_fast = (sk == 1);
+// FP64 operand (a strided gather: element (r, k) at p[roff(r) + koff(k)], the row and K indices
+// each spread over up to four tensor dimensions) -> np bf16 planes, K-major [plane][Rp][Kp], zero
+// padded: plane q holds the bf16 rounding of x minus the planes before it.  One pass reads the FP64
+// tensor in whatever order its dimensions lie and writes the planes, so an operand whose indices are
+// not in GEMM order needs no FP64 reordering copy first.  32 x 64 tiles staged in shared memory:
+// the reads run along the tensor's unit-stride index (rows or K), the writes along K as bf16 pairs.
+constexpr int GS_R = 32, GS_K = 64, GS_LD = GS_K + 2;   // row pitch: 16-byte aligned double pairs
+
+__global__ void __launch_bounds__(256) gather_split_kernel(SplitView v, int R, int K, int Rp, int Kp, int np,
+                                                            __nv_bfloat16 *__restrict__ out) {
+    __shared__ __align__(16) double tile[GS_R * GS_LD];
+    __shared__ long long roff[GS_R], koff[GS_K];
+    const int tid = threadIdx.x;
+    const int tiles_k = (Kp + GS_K - 1) / GS_K;
+    const long long ntiles = (long long)(Rp / GS_R) * tiles_k;
+    const bool row_fast = v.rs[0] == 1 && v.ks[0] != 1;
     const size_t plane = (size_t)Rp * Kp;
-    for (int k0 = blockIdx.y * 32; k0 < Kp; k0 += gridDim.y * 32) {
-        for (int i = ty; i < 32; i += 8) {
-            int r, k;
-            if (k_fast) {
-                r = r0 + i;
-                k = k0 + tx;
-            } else {
-                r = r0 + tx;
-                k = k0 + i;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int r0 = (int)(t / tiles_k) * GS_R, k0 = (int)(t % tiles_k) * GS_K;
+        if (tid < GS_R) {
+            long long x = r0 + tid, off = -1;
+            if (x < R) {
+                off = 0;
+                for (int d = 0; d < v.nr; d++) {
+                    const long long q = x / v.rn[d];
+                    off += (x - q * v.rn[d]) * v.rs[d];
+                    x = q;
+                }
             }
-            double x = (r < R && k < K) ? src[(long long)r * sr + (long long)k * sk] : 0.0;
-            if (k_fast) tile[i][tx] = x;
-            else tile[tx][i] = x;
+            roff[tid] = off;
+        } else if (tid < GS_R + GS_K) {
+            long long x = k0 + tid - GS_R, off = -1;
+            if (x < K) {
+                off = 0;
+                for (int d = 0; d < v.nk; d++) {
+                    const long long q = x / v.kn[d];
+                    off += (x - q * v.kn[d]) * v.ks[d];
+                    x = q;
+                }
+            }
+            koff[tid - GS_R] = off;
         }
         __syncthreads();
-        for (int i = ty; i < 32; i += 8) {
-            const int r = r0 + i, k = k0 + tx;
-            if (r < Rp && k < Kp) {
-                double x = tile[i][tx];
-                const size_t o = (size_t)r * Kp + k;
-                for (int p = 0; p < np; p++) {
-                    __nv_bfloat16 q = __double2bfloat16(x);
-                    out[p * plane + o] = q;
-                    x -= (double)__bfloat162float(q);
-                }
+        double x[GS_R * GS_K / 256];
+#pragma unroll
+        for (int it = 0; it < GS_R * GS_K / 256; it++) {
+            const int e = tid + 256 * it;
+            const int i = row_fast ? e % GS_R : e / GS_K, j = row_fast ? e / GS_R : e % GS_K;
+            const long long ro = roff[i], ko = koff[j];
+            x[it] = (ro >= 0 && ko >= 0) ? __ldg(v.p + ro + ko) : 0.0;
+        }
+#pragma unroll
+        for (int it = 0; it < GS_R * GS_K / 256; it++) {
+            const int e = tid + 256 * it;
+            const int i = row_fast ? e % GS_R : e / GS_K, j = row_fast ? e / GS_R : e % GS_K;
+            tile[i * GS_LD + j] = x[it];
+        }
+        __syncthreads();
+        // warp w writes rows w, w + 8, ...; lane l the K pair (2l, 2l + 1) of every plane
+        const int warp = tid >> 5, lane = tid & 31, k = k0 + 2 * lane;
+        for (int i = warp; i < GS_R; i += 8) {
+            const int r = r0 + i;
+            if (r >= Rp || k >= Kp) continue;
+            double2 y = *reinterpret_cast<const double2 *>(&tile[i * GS_LD + 2 * lane]);
+            const size_t o = (size_t)r * Kp + k;
+            for (int q = 0; q < np; q++) {
+                const __nv_bfloat16 a = __double2bfloat16(y.x), b = __double2bfloat16(y.y);
+                *reinterpret_cast<__nv_bfloat162 *>(out + q * plane + o) = __halves2bfloat162(a, b);
+                y.x -= (double)__bfloat162float(a);
+                y.y -= (double)__bfloat162float(b);
             }
         }
         __syncthreads();
@@ -514,13 +548,21 @@ void launch_tc(Exec &ex, int planes, const __nv_bfloat16 *A, int64_t a_rows, int
 
 int n_tile(int planes) { return planes == 3 ? ModeX6::BN : ModeX3::BN; }
 
-void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
-           int planes, __nv_bfloat16 *out) {
-    dim3 grid((unsigned)(Rp / 32), (unsigned)std::min<int64_t>(Kp / 32, 65535));
-    split_bf16_kernel<<<grid, dim3(32, 8), 0, ex.stream>>>(src, sr, sk, (int)R, (int)K, (int)Rp, (int)Kp, planes,
-                                                           out);
+void split_view(Exec &ex, const SplitView &v, int64_t R, int64_t K, int64_t Rp, int64_t Kp, int planes,
+                __nv_bfloat16 *out) {
+    REQUIRE(Rp % GS_R == 0 && Kp % 2 == 0 && R <= Rp && K <= Kp && Kp < (1ll << 31) && Rp < (1ll << 31),
+            CCSD_GPU_EINVAL, "operand split: bad padding");
+    REQUIRE(v.nr >= 1 && v.nr <= 4 && v.nk >= 1 && v.nk <= 4, CCSD_GPU_EINVAL, "operand split: 1 to 4 dims per group");
+    const int64_t tiles = (Rp / GS_R) * ((Kp + GS_K - 1) / GS_K);
+    const int blocks = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * 8);
+    gather_split_kernel<<<blocks, 256, 0, ex.stream>>>(v, (int)R, (int)K, (int)Rp, (int)Kp, planes, out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
+}
+
+void split(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R, int64_t K, int64_t Rp, int64_t Kp,
+           int planes, __nv_bfloat16 *out) {
+    split_view(ex, matrix_view(src, R, sr, K, sk), R, K, Rp, Kp, planes, out);
 }
 
 int check_planes(int planes) {
@@ -579,18 +621,14 @@ std::vector<int> tc_split_candidates(int64_t m, int64_t n, int64_t k, int planes
     return out;
 }
 
-void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
-                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, int splits) {
+void mixed_gemm_views(Exec &ex, const SplitView &A, const SplitView &B, int64_t m, int64_t n, int64_t k, double alpha,
+                      double beta, double *C, int64_t ldc, int splits) {
     REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "mixed_gemm: size too large");
     const int np = check_planes(ex.planes);
     const int64_t Kp = round_up(k, BK), Mp = round_up(m, BM), Np = round_up(n, B_ROW_PAD);
     DBuf a(sizeof(__nv_bfloat16) * np * Mp * Kp, ex.stream), b(sizeof(__nv_bfloat16) * np * Np * Kp, ex.stream);
-    // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T)
-    if (!transA) split(ex, A, 1, lda, m, k, Mp, Kp, np, a.as<__nv_bfloat16>());
-    else split(ex, A, lda, 1, m, k, Mp, Kp, np, a.as<__nv_bfloat16>());
-    // B operand rows are output columns: op(B)(kk, c) = B[kk + ldb c] (N) or B[c + ldb kk] (T)
-    if (!transB) split(ex, B, ldb, 1, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
-    else split(ex, B, 1, ldb, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
+    split_view(ex, A, m, k, Mp, Kp, np, a.as<__nv_bfloat16>());
+    split_view(ex, B, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
     if (splits <= 0) splits = tc_default_splits(m, n, k, np);
     splits = std::max(1, std::min<int>(splits, (int)(Kp / BK)));
     const double mnk = double(m) * double(n) * double(k);
@@ -607,6 +645,26 @@ void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
         part.d(), splits, m, n, beta, C, ldc);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
+}
+
+SplitView matrix_view(const double *p, int64_t rows, int64_t sr, int64_t K, int64_t sk) {
+    SplitView v{};
+    v.p = p;
+    v.nr = v.nk = 1;
+    v.rn[0] = std::max<int64_t>(rows, 1);
+    v.rs[0] = sr;
+    v.kn[0] = std::max<int64_t>(K, 1);
+    v.ks[0] = sk;
+    return v;
+}
+
+void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
+                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, int splits) {
+    // op(A)(r, kk): A[r + lda kk] (N) or A[kk + lda r] (T); B operand rows are output columns:
+    // op(B)(kk, c) = B[kk + ldb c] (N) or B[c + ldb kk] (T)
+    const SplitView a = transA ? matrix_view(A, m, lda, k, 1) : matrix_view(A, m, 1, k, lda);
+    const SplitView b = transB ? matrix_view(B, n, 1, k, ldb) : matrix_view(B, n, ldb, k, 1);
+    mixed_gemm_views(ex, a, b, m, n, k, alpha, beta, C, ldc, splits);
 }
 
 int64_t tc_pad_rows_a(int64_t m) { return round_up(m, BM); }

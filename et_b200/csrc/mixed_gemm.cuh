@@ -16,6 +16,22 @@ void mixed_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
                 const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc,
                 int splits = -1);
 
+// FP64 operand of the tensor-core GEMM as a strided gather: element (r, k) at p[roff(r) + koff(k)],
+// roff(r) = sum_d digit_d(r) * rs[d] with the digits of r over the extents rn[0..nr) (first
+// fastest), koff(k) likewise over kn/ks.  A tensor whose row or K indices span several dimensions
+// (a 4-index amplitude or integral block in any index order) is split straight into bf16 planes.
+struct SplitView {
+    const double *p;
+    int nr, nk;
+    long long rn[4], rs[4], kn[4], ks[4];
+};
+SplitView matrix_view(const double *p, int64_t rows, int64_t sr, int64_t K, int64_t sk);
+
+// C (m x n, col-major, ldc) = alpha A B^T + beta C for operands given as views: A's rows are the m
+// output rows, B's rows the n output columns, both with the same k contraction indices.
+void mixed_gemm_views(Exec &ex, const SplitView &A, const SplitView &B, int64_t m, int64_t n, int64_t k, double alpha,
+                      double beta, double *C, int64_t ldc, int splits = -1);
+
 // K-split count of the fixed rule: split only when the output tiles cannot fill the SMs.
 int tc_default_splits(int64_t m, int64_t n, int64_t k, int planes);
 // K-split counts worth timing for an m x n x k product: 1, the fixed rule's count, and counts whose

@@ -1,6 +1,7 @@
 // Tensor primitives: strided permutations (smem-tiled when the fastest index changes),
 // GEMM-backed contractions, packed-doubles conversions and deterministic reductions.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -128,10 +129,18 @@ int trace_level() {
     }();
     return level;
 }
+// CCSD_GPU_TRACE=3 adds the host time spent inside each contraction call: a call that blocks (an
+// allocation that grows the pool, a synchronising library call) shows up as a long one
 struct PermTag {
     const char *prev;
-    explicit PermTag(const char *t) : prev(g_perm_tag) { g_perm_tag = t; }
-    ~PermTag() { g_perm_tag = prev; }
+    std::chrono::steady_clock::time_point t0;
+    explicit PermTag(const char *t) : prev(g_perm_tag), t0(std::chrono::steady_clock::now()) { g_perm_tag = t; }
+    ~PermTag() {
+        if (trace_level() >= 3)
+            std::fprintf(stderr, "ccsd_gpu   [%s] host %.3f ms\n", g_perm_tag,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+        g_perm_tag = prev;
+    }
 };
 }  // namespace
 
@@ -202,43 +211,71 @@ void permute_add(Exec &ex, double alpha, const TV &in, double beta, const TV &ou
 // GEMM dispatch
 // ---------------------------------------------------------------------------
 
+namespace {
+
+// Route of an m x n x k product: tensor cores (mixed, with `splits` K splits; -1 = the fixed rule's
+// count) or the FP64 engines.  known = false: the product is to be timed first (autotune on, a shape
+// not seen before); `key` then names it.
+struct Route {
+    bool known = true, mixed = false;
+    int splits = -1;
+    std::string key;
+};
+
+Route lookup_route(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double fl, bool allow_mixed) {
+    Route r;
+    const bool tc_ok = allow_mixed && ex.prec == Prec::MIXED && k >= 16;
+    if (tc_ok && ex.autotune) {
+        // measured route (0 = DGEMM, s >= 1 = tensor cores with s K-splits) for products big enough
+        // to be worth timing
+        if (fl < 5e7 || m < 16 || n < 16) {
+            r.splits = 0;
+            return r;
+        }
+        r.key = tune_key('g', m, n, k, transA, transB, ex);
+        const int route = tune_lookup(r.key);
+        if (route < 0) {
+            r.known = false;
+            return r;
+        }
+        r.mixed = route > 0;
+        r.splits = route;
+        return r;
+    }
+    // fixed rule: the tensor-core tile is 128 x 256 x 64, so skinny products stay on the FP64 pipe
+    r.mixed = tc_ok && fl >= ex.mixed_min_flops && (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64));
+    return r;
+}
+
+}  // namespace
+
 void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
           int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, bool allow_mixed) {
     if (m == 0 || n == 0) return;
     double fl = 2.0 * double(m) * double(n) * double(k);
     ex.flops += fl;
-    const bool tc_ok = allow_mixed && ex.prec == Prec::MIXED && k >= 16;
-    // measured route (0 = DGEMM, s >= 1 = tensor cores with s K-splits) for products big enough to
-    // be worth timing; -1 = the fixed rule below
-    int route = -1;
-    if (tc_ok && ex.autotune) {
-        if (fl < 5e7 || m < 16 || n < 16) {
-            route = 0;
-        } else {
-            const std::string key = tune_key('g', m, n, k, transA, transB, ex);
-            route = tune_lookup(key);
-            if (route < 0) {
-                std::vector<int> routes;
-                if (fl <= 4e11) routes.push_back(0);   // larger products never favour FP64
-                for (int sp : tc_split_candidates(m, n, k, ex.planes)) routes.push_back(sp);
-                DBuf scratch = dalloc(m * n, ex.stream);
-                route = tune_measure(ex, key, routes, [&](int r) {
-                    if (r == 0) {
-                        const double zero = 0.0;
-                        BLAS_CHECK(cublasDgemm_64(ex.blas, transA ? CUBLAS_OP_T : CUBLAS_OP_N,
-                                                  transB ? CUBLAS_OP_T : CUBLAS_OP_N, m, n, k, &alpha, A, lda, B, ldb,
-                                                  &zero, scratch.d(), m));
-                    } else {
-                        mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, 0.0, scratch.d(), m, r);
-                    }
-                });
+    Route rt = lookup_route(ex, transA, transB, m, n, k, fl, allow_mixed);
+    if (!rt.known) {
+        std::vector<int> routes;
+        if (fl <= 4e11) routes.push_back(0);   // larger products never favour FP64
+        for (int sp : tc_split_candidates(m, n, k, ex.planes)) routes.push_back(sp);
+        DBuf scratch = dalloc(m * n, ex.stream);
+        const int route = tune_measure(ex, rt.key, routes, [&](int r) {
+            if (r == 0) {
+                const double zero = 0.0;
+                BLAS_CHECK(cublasDgemm_64(ex.blas, transA ? CUBLAS_OP_T : CUBLAS_OP_N,
+                                          transB ? CUBLAS_OP_T : CUBLAS_OP_N, m, n, k, &alpha, A, lda, B, ldb,
+                                          &zero, scratch.d(), m));
+            } else {
+                mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, 0.0, scratch.d(), m, r);
             }
-        }
+        });
+        rt.known = true;
+        rt.mixed = route > 0;
+        rt.splits = route;
     }
-    // fixed rule: the tensor-core tile is 128 x 256 x 64, so skinny products stay on the FP64 pipe
-    const bool mixed = route >= 0 ? route > 0
-                                  : tc_ok && fl >= ex.mixed_min_flops &&
-                                        (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64));
+    const bool mixed = rt.mixed;
+    const int route = rt.splits;
     if (trace_level() >= 2)
         std::fprintf(stderr, "ccsd_gpu gemm [%s] %s m %lld n %lld k %lld  %.3g flop  splits %d\n",
                      g_perm_tag ? g_perm_tag : "direct", mixed ? "bf16x3" : "fp64", (long long)m, (long long)n,
@@ -339,6 +376,29 @@ TV make_contiguous(Exec &ex, const TV &v, const std::vector<int> &g1, const std:
     return dst;
 }
 
+// v as a GEMM operand gather: rows over the dims `rows`, K over the dims `ks` (each in the order
+// given, first fastest; unit dims dropped).  False when a group spans more than four dims.
+bool gather_view(const TV &v, const std::vector<int> &rows, const std::vector<int> &ks, SplitView *out) {
+    SplitView g{};
+    g.p = v.p;
+    for (int d : rows) {
+        if (v.n[d] == 1) continue;
+        if (g.nr == 4) return false;
+        g.rn[g.nr] = v.n[d];
+        g.rs[g.nr++] = v.s[d];
+    }
+    for (int d : ks) {
+        if (v.n[d] == 1) continue;
+        if (g.nk == 4) return false;
+        g.kn[g.nk] = v.n[d];
+        g.ks[g.nk++] = v.s[d];
+    }
+    if (g.nr == 0) g.rn[g.nr++] = 1;   // a single row (stride unused)
+    if (g.nk == 0) g.kn[g.nk++] = 1;
+    *out = g;
+    return true;
+}
+
 }  // namespace
 
 void contract(Exec &ex, const char *spec, double alpha, const TV &A, const TV &B, double beta, const TV &C) {
@@ -393,34 +453,29 @@ void contract(Exec &ex, const char *spec, double alpha, const TV &A, const TV &B
     TV Au = A, Bu = B;
     bool tA, tB;
     int64_t lda, ldb, ldc;
-    {
-        auto dK = dims_of(oK, info, 0), dM = dims_of(oM, info, 0);
-        if (groupable(A, dM, dK, &lda)) tA = false;
-        else if (groupable(A, dK, dM, &lda)) tA = true;
-        else {
-            Au = make_contiguous(ex, A, dK, dM, bufA);
-            tA = true;
-            lda = std::max<int64_t>(mK, 1);
-        }
+    // an operand whose indices are not two contiguous groups is reordered into a copy, unless the
+    // product goes to the tensor cores, whose operand split gathers it from its own layout
+    bool packA = false, packB = false;
+    const auto aK = dims_of(oK, info, 0), aM = dims_of(oM, info, 0);
+    const auto bK = dims_of(oK, info, 1), bN = dims_of(oN, info, 1);
+    if (groupable(A, aM, aK, &lda)) tA = false;
+    else if (groupable(A, aK, aM, &lda)) tA = true;
+    else {
+        packA = true;
+        tA = true;
+        lda = std::max<int64_t>(mK, 1);
     }
-    {
-        auto dK = dims_of(oK, info, 1), dN = dims_of(oN, info, 1);
-        if (groupable(B, dK, dN, &ldb)) tB = false;
-        else if (groupable(B, dN, dK, &ldb)) tB = true;
-        else {
-            Bu = make_contiguous(ex, B, dK, dN, bufB);
-            tB = false;
-            ldb = std::max<int64_t>(mK, 1);
-        }
+    if (groupable(B, bK, bN, &ldb)) tB = false;
+    else if (groupable(B, bN, bK, &ldb)) tB = true;
+    else {
+        packB = true;
+        tB = false;
+        ldb = std::max<int64_t>(mK, 1);
     }
     auto cM = dims_of(oM, info, 2), cN = dims_of(oN, info, 2);
-    if (groupable(C, cM, cN, &ldc)) {
-        gemm(ex, tA, tB, mM, mN, mK, alpha, Au.p, lda, Bu.p, ldb, beta, C.p, ldc);
-    } else if (groupable(C, cN, cM, &ldc)) {
-        gemm(ex, !tB, !tA, mN, mM, mK, alpha, Bu.p, ldb, Au.p, lda, beta, C.p, ldc);
-    } else {
-        bufC = dalloc(mM * mN, ex.stream);
-        gemm(ex, tA, tB, mM, mN, mK, alpha, Au.p, lda, Bu.p, ldb, 0.0, bufC.d(), mM);
+    const int cmode = groupable(C, cM, cN, &ldc) ? 0 : groupable(C, cN, cM, &ldc) ? 1 : 2;
+    // C = beta C + the column-major mM x mN product in bufC
+    auto scatter_C = [&]() {
         TV t;
         t.p = bufC.d();
         t.nd = C.nd;
@@ -435,6 +490,42 @@ void contract(Exec &ex, const char *spec, double alpha, const TV &A, const TV &B
             st *= C.n[d];
         }
         permute_add(ex, 1.0, t, beta, C);
+    };
+    if (packA || packB) {
+        SplitView va, vb;
+        if (gather_view(A, aM, aK, &va) && gather_view(B, bN, bK, &vb)) {
+            // the route of the product as the reordered copies would present it
+            const double fl = 2.0 * double(mM) * double(mN) * double(mK);
+            const Route rt = cmode == 1 ? lookup_route(ex, !tB, !tA, mN, mM, mK, fl, true)
+                                        : lookup_route(ex, tA, tB, mM, mN, mK, fl, true);
+            if (rt.known && rt.mixed) {
+                ex.flops += fl;
+                if (trace_level() >= 2)
+                    std::fprintf(stderr, "ccsd_gpu gemm [%s] bf16x3 gather m %lld n %lld k %lld  %.3g flop  splits %d\n",
+                                 spec, (long long)mM, (long long)mN, (long long)mK, fl, rt.splits);
+                if (cmode == 0) {
+                    mixed_gemm_views(ex, va, vb, mM, mN, mK, alpha, beta, C.p, ldc, rt.splits);
+                } else if (cmode == 1) {
+                    mixed_gemm_views(ex, vb, va, mN, mM, mK, alpha, beta, C.p, ldc, rt.splits);
+                } else {
+                    bufC = dalloc(mM * mN, ex.stream);
+                    mixed_gemm_views(ex, va, vb, mM, mN, mK, alpha, 0.0, bufC.d(), mM, rt.splits);
+                    scatter_C();
+                }
+                return;
+            }
+        }
+        if (packA) Au = make_contiguous(ex, A, aK, aM, bufA);
+        if (packB) Bu = make_contiguous(ex, B, bK, bN, bufB);
+    }
+    if (cmode == 0) {
+        gemm(ex, tA, tB, mM, mN, mK, alpha, Au.p, lda, Bu.p, ldb, beta, C.p, ldc);
+    } else if (cmode == 1) {
+        gemm(ex, !tB, !tA, mN, mM, mK, alpha, Bu.p, ldb, Au.p, lda, beta, C.p, ldc);
+    } else {
+        bufC = dalloc(mM * mN, ex.stream);
+        gemm(ex, tA, tB, mM, mN, mK, alpha, Au.p, lda, Bu.p, ldb, 0.0, bufC.d(), mM);
+        scatter_C();
     }
 }
 

@@ -237,3 +237,29 @@ def test_streamed_ladder_equals_resident(dims):
     for budget in list(res)[1:]:
         for x, y in zip(res[0], res[budget]):
             assert np.array_equal(x, y), budget
+
+
+def test_gathered_operands_equal_reordered_copies():
+    """An operand whose indices are not two contiguous groups (a 4-index block contracted over a
+    scattered pair of its indices) is split into bf16 planes straight from its own layout once its
+    product's route is known to be the tensor cores; before that (the first call of a shape, timed by
+    the autotuner) it goes through a reordered FP64 copy.  Both give the same planes, so the second
+    residual equals the first bit for bit, and every later call launches the same kernels."""
+    from et_b200 import CCSD, MIXED
+    n_o, n_v, n_J = 7, 45, 110                     # shapes no other test tunes
+    s = make_system(n_o, n_v, n_J, seed=31)
+    with CCSD(n_o, n_v, n_J, precision=MIXED, mixed_min_flops=1, autotune=1) as g:
+        g.set_system(s.L_mo, s.h_mo, s.eps)
+        g.set_amplitudes(0.05 * np.random.default_rng(6).standard_normal(g.n_amp))
+        first = g.construct_omega()
+        n0, _ = g.stats()
+        g.set_profiling(True)
+        second = g.construct_omega()
+        n1, _ = g.stats()
+        third = g.construct_omega()
+        n2, _ = g.stats()
+        tc_launches, _, _ = g.gemm_profile()
+        g.set_profiling(False)
+    assert tc_launches > 0
+    assert np.array_equal(first, second) and np.array_equal(second, third)
+    assert n2 - n1 == n1 - n0
