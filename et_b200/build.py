@@ -54,7 +54,7 @@ def build(verbose: bool = False, extra_flags=None) -> str:
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as pool:
         list(pool.map(run, jobs))
     if jobs or _stale(OUT, objs):
-        link = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcublas", "-lcusolver"]
+        link = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcublas", "-lcusolver", "-Xlinker", "--no-undefined"]
         run(link)
     return OUT
 

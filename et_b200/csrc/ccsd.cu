@@ -361,46 +361,71 @@ void Context::set_precision(int32_t precision) {
     ex.prec = p;
 }
 
-// Tensor-core form of the same ladder.  With M_ab[c,d] = g_acbd the +/- sums of
-// omega_ccsd_a2 over packed c >= d equal sums over all (c, d):
-//   omega+_ij,ab = sum_cd 1/2 (1 - d_ij/2)(t_cidj + t_cjdi) M_ab[c,d]
-//   omega-_ij,ab = sum_cd 1/2 (t_cidj - t_cjdi) M_ab[c,d]
-// so the split-bf16 integrals M_ab (written by the G GEMM epilogue, all pairs b <= a resident
-// in HBM) meet [T+; T-] of all vectors in one GEMM of N = nvec n_o^2 and K = n_v^2.
+// Tensor-core form of the same +/- ladder: the FP64 path's g+- (over packed c >= d, c > d) and t+-
+// meet in two GEMMs on split-bf16 planes, W+ = 1/2 t+ g+^T (K = n_v(n_v+1)/2) and W- = 1/2 t- g-^T
+// (K = n_v(n_v-1)/2): half the work of contracting M_ab[c,d] = g_acbd over all (c, d).  The g+- of
+// the pairs of a block of a come from the tensor-core GEMM G = L_block^T L (one K split, so each
+// element is the same dot product whatever the block) and one pass that forms the sums and
+// differences and writes them as planes (form_pm_planes).
 //
-// ladder_pairs fills mbuf with M_ab from the given L_vv.  The integrals of the untransformed L_vv
+// ladder_pairs fills mbuf with the planes of all pairs, P+ then P-.  Those of the untransformed L_vv
 // (untransformed = true) stay valid until the Cholesky vectors change, so the mixed residual forms
 // them once per Cholesky set; any other L_vv (T1-transformed, or transposed for the adjoint) is
 // formed once per call and shared by all vectors of that call.
-// split L_vv rows r = c + nv a (K = J) as bf16 planes [np][pad(nv^2)][pad(J)]
-DBuf Context::split_lvv_rows(const double *Lvv) {
-    const int np = ex.planes;
-    cudaStream_t s = ex.stream;
-    const int64_t nv2 = nv * nv, Jp = tc_pad_k(nJ), l_rows = tc_pad_rows_a(nv2);
-    DBuf LS(sizeof(__nv_bfloat16) * np * l_rows * Jp, s);
-    // r = c + nv a  ->  offset nJ*(a + nv*c): not a single stride, so split from the (J, c, a) copy
-    DBuf LT = dalloc(nJ * nv2, s);
+namespace {
+
+struct PairShape {
+    int64_t nvp, nvm;     // pairs c >= d, c > d (the K of the + and - GEMMs, and the pairs a >= b, a > b)
+    int64_t kp, km;       // K padded
+    int64_t rows_p, rows_m;   // rows of all pairs padded for the B operand
+    size_t plane_p() const { return (size_t)rows_p * kp; }
+    size_t plane_m() const { return (size_t)rows_m * km; }
+};
+
+PairShape pair_shape(int64_t nv) {
+    PairShape p;
+    p.nvp = nv * (nv + 1) / 2;
+    p.nvm = nv * (nv - 1) / 2;
+    p.kp = tc_pad_k(p.nvp);
+    p.km = tc_pad_k(std::max<int64_t>(p.nvm, 1));
+    p.rows_p = tc_pad_rows_b(p.nvp);
+    p.rows_m = tc_pad_rows_b(std::max<int64_t>(p.nvm, 1));
+    return p;
+}
+
+}  // namespace
+
+// L_vv as (J, c, a): the columns (c, a) of one block of a are contiguous
+DBuf Context::lvv_jca(const double *Lvv) {
+    DBuf LT = dalloc(nJ * nv * nv, ex.stream);
     TV src = tv(Lvv, {nJ, nv, nv});   // [J, a, c]
-    TV dst;
-    dst.p = LT.d();
-    dst.nd = 3;
-    dst.n[0] = nJ;
-    dst.n[1] = nv;
-    dst.n[2] = nv;
-    dst.s[0] = 1;
+    TV dst = tv(LT.d(), {nJ, nv, nv});
     dst.s[1] = nJ * nv;   // a
     dst.s[2] = nJ;        // c
     permute_add(ex, 1.0, src, 0.0, dst);
-    split_rows(ex, LT.d(), nJ, 1, nv2, nJ, l_rows, Jp, LS.as<__nv_bfloat16>());
-    return LS;
+    return LT;
 }
 
-// Whether the split-bf16 pair integrals of all v(v+1)/2 pairs stay resident: they must fit the
-// budget (ccsd_gpu_options.ladder_pair_budget, else half of the free device memory).  Otherwise the
-// ladder forms them block by block in every call (ladder_tc_streamed), as eT's omega_ccsd_a2 does.
+// g+- planes of the pairs a in [a0, a1) from LT = lvv_jca(L_vv): P+ rows a(a+1)/2 + b - rowp0 of a
+// buffer of rows_p padded rows per plane, P- rows a(a-1)/2 + b - rowm0 (rows_m per plane); G holds at
+// least n_v (a1 - a0) x n_v a1 doubles
+void Context::form_pair_planes(const double *LT, int64_t a0, int64_t a1, double *G, __nv_bfloat16 *Pp,
+                               int64_t rows_p, int64_t rowp0, __nv_bfloat16 *Pm, int64_t rows_m, int64_t rowm0) {
+    const PairShape ps = pair_shape(nv);
+    const int64_t M = nv * (a1 - a0), N = nv * a1;
+    // G[(c, a), (d, b)] = sum_J L_ac L_bd
+    mixed_gemm(ex, true, false, M, N, nJ, 1.0, LT + nJ * nv * a0, nJ, LT, nJ, 0.0, G, M, 1);
+    form_pm_planes(ex, G, M, nv, a0, a1, ex.planes, Pp, ps.kp, (size_t)rows_p * ps.kp, rowp0, Pm, ps.km,
+                   (size_t)rows_m * ps.km, rowm0);
+    ex.flops += 2.0 * double(M) * double(N) * double(nJ);
+}
+
+// Whether the split-bf16 pair integrals of all pairs stay resident: they must fit the budget
+// (ccsd_gpu_options.ladder_pair_budget, else half of the free device memory).  Otherwise the ladder
+// forms them block by block in every call (ladder_tc_streamed), as eT's omega_ccsd_a2 does.
 bool Context::ladder_pairs_resident() {
-    const int64_t nab = nv * (nv + 1) / 2;
-    const double need = 2.0 * ex.planes * (double)tc_pad_rows_a(nab) * (double)tc_pad_k(nv * nv);
+    const PairShape ps = pair_shape(nv);
+    const double need = 2.0 * ex.planes * (double)(ps.plane_p() + ps.plane_m());
     if (ladder_pair_budget > 0) return need <= (double)ladder_pair_budget;
     if (mbuf_bytes >= need) return true;
     size_t free_b = 0, total_b = 0;
@@ -417,24 +442,25 @@ void Context::ladder_pairs(const double *Lvv, bool untransformed) {
         mbuf_src == Lvv && mbuf_version == l_version && mbuf_planes == np)
         return;
     cudaStream_t s = ex.stream;
-    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2;
-    const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2);
-    const int64_t l_rows = tc_pad_rows_a(nv2);
-    DBuf LS = split_lvv_rows(Lvv);
-    // all pair integrals, resident: [np][mrows][Kq] (padding rows / K positions are never written, so
-    // they stay zero when the plane count changes)
-    const int64_t mrows = tc_pad_rows_a(nab);
-    if (mbuf_bytes < sizeof(__nv_bfloat16) * np * (size_t)mrows * Kq) {
-        mbuf = DBuf(sizeof(__nv_bfloat16) * np * (size_t)mrows * Kq, s);
+    const PairShape ps = pair_shape(nv);
+    const size_t bytes = sizeof(__nv_bfloat16) * np * (ps.plane_p() + ps.plane_m());
+    // padding rows and K positions are never written and must read as zero; P- moves when the plane
+    // count changes, so the buffer is cleared then too
+    if (mbuf_bytes < bytes) {
+        mbuf = DBuf(bytes, s);
         mbuf_bytes = mbuf.bytes();
         CU_CHECK(cudaMemsetAsync(mbuf.as<void>(), 0, mbuf_bytes, s));
+    } else if (mbuf_planes != np) {
+        CU_CHECK(cudaMemsetAsync(mbuf.as<void>(), 0, mbuf_bytes, s));
     }
-    int64_t nA = ladder_batch > 0 ? ladder_batch : 16;
-    for (int64_t a0 = 0; a0 < nv; a0 += nA) {
-        int64_t a1 = std::min(nv, a0 + nA);
-        tc_gemm_pairs(ex, LS.as<__nv_bfloat16>(), l_rows, Jp, nv, a0, a1, mbuf.as<__nv_bfloat16>(), mrows, Kq, nJ);
-    }
-    ex.flops += double(nv2) * double(nv2 + 1) * double(nJ);
+    __nv_bfloat16 *Pp = mbuf.as<__nv_bfloat16>(), *Pm = Pp + np * ps.plane_p();
+    DBuf LT = lvv_jca(Lvv);
+    // blocks of a whose G fits in about 2 GB
+    const int64_t nA = ladder_batch > 0 ? ladder_batch
+                                        : std::max<int64_t>(1, std::min<int64_t>(nv, (int64_t)(2.0e9 / (8.0 * nv * nv * nv))));
+    DBuf G = dalloc(nv * std::min(nA, nv) * nv * nv, s);
+    for (int64_t a0 = 0; a0 < nv; a0 += nA)
+        form_pair_planes(LT.d(), a0, std::min(nv, a0 + nA), G.d(), Pp, ps.rows_p, 0, Pm, ps.rows_m, 0);
     mbuf_kind = untransformed ? 1 : 2;
     mbuf_version = l_version;
     mbuf_planes = np;
@@ -443,19 +469,37 @@ void Context::ladder_pairs(const double *Lvv, bool untransformed) {
     cache_epoch++;
 }
 
-// om2[v] += ladder(pair integrals in mbuf, t2[v]) for nvec packed vectors
-void Context::ladder_tc_apply(const double *t2, double *om2, int64_t nvec) {
-    cudaStream_t s = ex.stream;
-    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
-    const int64_t Kq = tc_pad_k(nv2), mrows = tc_pad_rows_a(nab);
-    const int64_t rows_T = tc_pad_rows_b(nvec * nrow);
-    DBuf TS(sizeof(__nv_bfloat16) * ex.planes * rows_T * Kq, s);
-    build_T(ex, t2, nvec, no, nv, rows_T, Kq, ex.planes, TS.as<__nv_bfloat16>());
-    DBuf W = dalloc(nab * nvec * nrow, s);
-    tc_gemm_f64_tuned(ex, mbuf.as<__nv_bfloat16>(), mrows, TS.as<__nv_bfloat16>(), rows_T, Kq, nab, nvec * nrow, nv2,
-                      1.0, 0.0, W.d(), nab, 1);
-    for (int64_t v = 0; v < nvec; v++) add_omega_T(ex, om2 + v * nt2, W.d() + v * nrow * nab, nab, no, nv);
-    ex.flops += 2.0 * double(nab) * double(nvec * nrow) * double(nv2);
+// t+ and t- planes of nvec packed vectors (the A operands of the +/- GEMMs)
+Context::TPlanes Context::t_planes(const double *t2, int64_t nvec) {
+    const PairShape ps = pair_shape(nv);
+    const int np = ex.planes;
+    const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
+    TPlanes T;
+    T.rows_p = tc_pad_rows_a(nvec * nop);
+    T.rows_m = tc_pad_rows_a(std::max<int64_t>(nvec * nom, 1));
+    T.p = DBuf(sizeof(__nv_bfloat16) * np * T.rows_p * ps.kp, ex.stream);
+    T.m = DBuf(sizeof(__nv_bfloat16) * np * T.rows_m * ps.km, ex.stream);
+    build_tpm_planes(ex, t2, nvec, no, nv, true, T.rows_p, ps.kp, np, T.p.as<__nv_bfloat16>());
+    build_tpm_planes(ex, t2, nvec, no, nv, false, T.rows_m, ps.km, np, T.m.as<__nv_bfloat16>());
+    return T;
+}
+
+// om2[v] += the ladder of the pairs a in [a0, a1), whose g+- planes are Pp / Pm (row 0 = the
+// block's first pair, prow / mrow padded rows per plane)
+void Context::ladder_pm_block(const TPlanes &T, int64_t nvec, const __nv_bfloat16 *Pp, int64_t prow,
+                              const __nv_bfloat16 *Pm, int64_t mrow, int64_t a0, int64_t a1, double *om2) {
+    const PairShape ps = pair_shape(nv);
+    const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
+    const int64_t nabp = a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2, nabm = a1 * (a1 - 1) / 2 - a0 * (a0 - 1) / 2;
+    const int64_t ldp = nvec * nop, ldm = std::max<int64_t>(nvec * nom, 1);
+    DBuf wp = dalloc(ldp * nabp, ex.stream), wm = dalloc(ldm * std::max<int64_t>(nabm, 1), ex.stream);
+    tc_gemm_f64(ex, T.p.as<__nv_bfloat16>(), T.rows_p, Pp, prow, ps.kp, ldp, nabp, ps.nvp, 0.5, 0.0, wp.d(), ldp, 1);
+    if (nom > 0 && nabm > 0)
+        tc_gemm_f64(ex, T.m.as<__nv_bfloat16>(), T.rows_m, Pm, mrow, ps.km, nvec * nom, nabm, ps.nvm, 0.5, 0.0, wm.d(),
+                    ldm, 1);
+    for (int64_t v = 0; v < nvec; v++)
+        add_omega_pm(ex, om2 + v * nt2, wp.d() + v * nop, wm.d() + v * nom, no, nv, a0, a1, ldp, ldm);
+    ex.flops += 2.0 * double(ldp) * double(nabp) * double(ps.nvp) + 2.0 * double(nvec * nom) * double(nabm) * double(ps.nvm);
 }
 
 void Context::ladder_tc(const double *Lvv, const double *t2, double *om2, int64_t nvec, bool untransformed) {
@@ -470,52 +514,60 @@ void Context::ladder_tc(const double *Lvv, const double *t2, double *om2, int64_
         return;
     }
     ladder_pairs(Lvv, untransformed);
-    ladder_tc_apply(t2, om2, nvec);
+    const PairShape ps = pair_shape(nv);
+    const TPlanes T = t_planes(t2, nvec);
+    const __nv_bfloat16 *Pp = mbuf.as<__nv_bfloat16>(), *Pm = Pp + ex.planes * ps.plane_p();
+    ladder_pm_block(T, nvec, Pp, ps.rows_p, Pm, ps.rows_m, 0, nv, om2);
 }
 
-// The same ladder with bounded memory: the pair rows of a block of consecutive a (at most
-// ladder_block_rows() rows) are formed into one buffer by the pair-integral GEMM and contracted with
-// [T+; T-] right away (omega_ccsd_a2's (a, b) batching on the tensor cores, omega_ccsd.F90:236-458).
-// Every output element is the dot product it is in the resident form (one K split, the same K
-// chunks), so the result equals the resident ladder's bit for bit.
+// The same ladder with bounded memory: the g+- planes of a block of consecutive a are formed into
+// one buffer and contracted right away (omega_ccsd_a2's (a, b) batching on the tensor cores,
+// omega_ccsd.F90:236-458).  Every output element is the dot product it is in the resident form (the
+// same planes, one K split, the same K chunks), so the result equals the resident ladder's bit for bit.
 void Context::ladder_tc_streamed(const double *Lvv, const double *t2, double *om2, int64_t nvec) {
     cudaStream_t s = ex.stream;
     const int np = ex.planes;
-    const int64_t nv2 = nv * nv, nab = nv * (nv + 1) / 2, nrow = no * no;
-    const int64_t Jp = tc_pad_k(nJ), Kq = tc_pad_k(nv2), l_rows = tc_pad_rows_a(nv2);
-    DBuf LS = split_lvv_rows(Lvv);
-    const int64_t rows_T = tc_pad_rows_b(nvec * nrow);
-    DBuf TS(sizeof(__nv_bfloat16) * np * rows_T * Kq, s);
-    build_T(ex, t2, nvec, no, nv, rows_T, Kq, np, TS.as<__nv_bfloat16>());
-    DBuf W = dalloc(nab * nvec * nrow, s);
-    // rows of one block: the budget (or half of the free memory) over the bytes of one pair row, and
-    // at least the rows of the largest a
+    const PairShape ps = pair_shape(nv);
+    const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
+    const int64_t ldp = nvec * nop, ldm = std::max<int64_t>(nvec * nom, 1);
+    DBuf LT = lvv_jca(Lvv);
+    const TPlanes T = t_planes(t2, nvec);
+    // blocks: consecutive a whose G, planes and W fit the budget (or a quarter of the free memory),
+    // at least one a each
     int64_t budget = ladder_pair_budget;
     if (budget <= 0) {
         size_t free_b = 0, total_b = 0;
         CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
         budget = (int64_t)(0.25 * (double)free_b);
     }
-    const int64_t row_bytes = 2 * np * Kq;
-    const int64_t max_rows = std::max<int64_t>(nv, budget / row_bytes - 128);
-    const int64_t Rp_max = tc_pad_rows_a(max_rows);
-    DBuf P(sizeof(__nv_bfloat16) * np * Rp_max * Kq, s);
-    // K positions beyond nv^2 are never written and must read as zero
-    CU_CHECK(cudaMemsetAsync(P.as<void>(), 0, P.bytes(), s));
-    const int64_t nA = ladder_batch > 0 ? ladder_batch : 16;
+    auto block_bytes = [&](int64_t a0, int64_t a1) {
+        const int64_t nabp = a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2, nabm = a1 * (a1 - 1) / 2 - a0 * (a0 - 1) / 2;
+        return 8.0 * double(nv * (a1 - a0)) * double(nv * a1) +
+               2.0 * np * (double(tc_pad_rows_b(nabp)) * ps.kp + double(tc_pad_rows_b(std::max<int64_t>(nabm, 1))) * ps.km) +
+               8.0 * (double(ldp) * nabp + double(ldm) * nabm);
+    };
+    std::vector<std::pair<int64_t, int64_t>> blocks;
+    int64_t g_max = 0, prow_max = 0, mrow_max = 0;
     for (int64_t a0 = 0; a0 < nv;) {
         int64_t a1 = a0 + 1;
-        while (a1 < nv && (a1 + 1) * (a1 + 2) / 2 - a0 * (a0 + 1) / 2 <= max_rows) a1++;
-        const int64_t row0 = a0 * (a0 + 1) / 2, R = a1 * (a1 + 1) / 2 - row0;
-        for (int64_t b0 = a0; b0 < a1; b0 += nA)
-            tc_gemm_pairs(ex, LS.as<__nv_bfloat16>(), l_rows, Jp, nv, b0, std::min(a1, b0 + nA), P.as<__nv_bfloat16>(),
-                          Rp_max, Kq, nJ, row0);
-        tc_gemm_f64(ex, P.as<__nv_bfloat16>(), Rp_max, TS.as<__nv_bfloat16>(), rows_T, Kq, R, nvec * nrow, nv2, 1.0,
-                    0.0, W.d() + row0, nab, 1);
+        while (a1 < nv && block_bytes(a0, a1 + 1) <= (double)budget) a1++;
+        blocks.emplace_back(a0, a1);
+        g_max = std::max(g_max, nv * (a1 - a0) * nv * a1);
+        prow_max = std::max(prow_max, tc_pad_rows_b(a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2));
+        mrow_max = std::max(mrow_max, tc_pad_rows_b(std::max<int64_t>(a1 * (a1 - 1) / 2 - a0 * (a0 - 1) / 2, 1)));
         a0 = a1;
     }
-    for (int64_t v = 0; v < nvec; v++) add_omega_T(ex, om2 + v * nt2, W.d() + v * nrow * nab, nab, no, nv);
-    ex.flops += double(nv2) * double(nv2 + 1) * double(nJ) + 2.0 * double(nab) * double(nvec * nrow) * double(nv2);
+    DBuf G = dalloc(g_max, s);
+    DBuf P(sizeof(__nv_bfloat16) * np * (size_t(prow_max) * ps.kp + size_t(mrow_max) * ps.km), s);
+    // K positions beyond the pair count are never written and must read as zero
+    CU_CHECK(cudaMemsetAsync(P.as<void>(), 0, P.bytes(), s));
+    __nv_bfloat16 *Pp = P.as<__nv_bfloat16>(), *Pm = Pp + np * size_t(prow_max) * ps.kp;
+    for (const auto &blk : blocks) {
+        const int64_t a0 = blk.first, a1 = blk.second;
+        form_pair_planes(LT.d(), a0, a1, G.d(), Pp, prow_max, a0 * (a0 + 1) / 2, Pm, mrow_max,
+                         std::max<int64_t>(a0 * (a0 - 1) / 2, 0));
+        ladder_pm_block(T, nvec, Pp, prow_max, Pm, mrow_max, a0, a1, om2);
+    }
 }
 
 // Mixed precision keeps the ovvv integrals of the untransformed Cholesky vectors resident as split
@@ -763,6 +815,7 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     const int user_digits = ex.fp64_digits;
     const int fp64_digits = rdig > 0 ? rdig : (rdig < 0 ? 0 : user_digits);
     cudaStream_t s = ex.stream;
+    const auto trace_t0 = std::chrono::steady_clock::now();
     orbital_differences(ex, eps.d(), no, nv, epsdiff.d());
     DBuf omega_v = dalloc(namp, s);
     std::vector<DBuf> errs(dim), pars(dim);
@@ -825,7 +878,6 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     std::vector<double> norms;
     // CCSD_GPU_TRACE=1: one line per iteration on stderr with the refinement decisions
     const bool trace = std::getenv("CCSD_GPU_TRACE") && std::getenv("CCSD_GPU_TRACE")[0] == '1';
-    const auto trace_t0 = std::chrono::steady_clock::now();
     auto trace_ms = [&]() {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - trace_t0).count();
     };
@@ -842,6 +894,10 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     };
     double trace_moved = 0.0;
     const char *trace_why = "";
+    if (trace) {
+        CU_CHECK(cudaStreamSynchronize(s));
+        std::fprintf(stderr, "ccsd_gpu gs set-up (records allocated) t %.1f ms\n", trace_ms());
+    }
     // shift every stored DIIS error vector by v and rebuild their Gram matrix
     auto shift_diis = [&](const double *v) {
         const int n = (int)order.size();
@@ -981,6 +1037,10 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     }
     ex.prec = user;
     refresh();
+    if (trace) {
+        CU_CHECK(cudaStreamSynchronize(s));
+        std::fprintf(stderr, "ccsd_gpu gs done t %.1f ms\n", trace_ms());
+    }
     if (energy_out) *energy_out = e;
     if (iters) *iters = it;
     return conv ? CCSD_GPU_OK : CCSD_GPU_ENOCONV;

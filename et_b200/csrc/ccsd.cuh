@@ -55,7 +55,7 @@ struct Context {
     DBuf t;                  // [t1 | packed t2]
     DBuf epsdiff;            // orbital differences (n_amp)
     DBuf scal;               // scalar scratch
-    DBuf mbuf;               // split-bf16 ladder integrals M_ab[c,d] for all pairs (mixed precision)
+    DBuf mbuf;               // split-bf16 ladder integrals g+- of all pairs, P+ then P- (mixed precision)
     size_t mbuf_bytes = 0;
     DBuf gov;                  // g_iajb cache (g_ovov_const)
     bool have_gov = false;
@@ -163,11 +163,19 @@ struct Context {
     // n_t2); the integrals are formed once per call
     void ladder(const double *Lvv, const double *t2, double *om2, int64_t nvec = 1);
     void ladder_tc(const double *Lvv, const double *t2, double *om2, int64_t nvec, bool untransformed);
-    DBuf split_lvv_rows(const double *Lvv);
+    DBuf lvv_jca(const double *Lvv);
+    void form_pair_planes(const double *LT, int64_t a0, int64_t a1, double *G, __nv_bfloat16 *Pp, int64_t rows_p,
+                          int64_t rowp0, __nv_bfloat16 *Pm, int64_t rows_m, int64_t rowm0);
     bool ladder_pairs_resident();
     void ladder_tc_streamed(const double *Lvv, const double *t2, double *om2, int64_t nvec);
     void ladder_pairs(const double *Lvv, bool untransformed);
-    void ladder_tc_apply(const double *t2, double *om2, int64_t nvec);
+    struct TPlanes {
+        DBuf p, m;                   // t+ and t- planes
+        int64_t rows_p = 0, rows_m = 0;
+    };
+    TPlanes t_planes(const double *t2, int64_t nvec);
+    void ladder_pm_block(const TPlanes &T, int64_t nvec, const __nv_bfloat16 *Pp, int64_t prow, const __nv_bfloat16 *Pm,
+                         int64_t mrow, int64_t a0, int64_t a1, double *om2);
     // the residual's ladder in mixed precision from untransformed integrals plus t1 corrections
     void ladder_residual_mixed(const double *t1, const double *tf, const double *t2, double *om2);
     // om2 += pack(-(A + A^T) + T4) with A_aibj = sum_k t_ak Y0_kibj, T4 = sum_kl t_ak t_bl Q_kilj

@@ -1,5 +1,6 @@
 // Bandwidth kernels of the CCSD path: packed index algebra, A2 ladder +/- forms,
 // energy, MP2 guess, quasi-Newton update and DIIS (all FP64).
+#include <algorithm>
 #include <cmath>
 
 #include <cuda_bf16.h>
@@ -72,6 +73,84 @@ __global__ void form_gpm_kernel(const double *__restrict__ G, int64_t ldg, doubl
     }
 }
 
+// bf16 rounding planes of x: plane q holds the rounding of x minus the planes before it
+__device__ __forceinline__ void put_planes(double x, int np, size_t plane, __nv_bfloat16 *out) {
+    for (int q = 0; q < np; q++) {
+        const __nv_bfloat16 h = __double2bfloat16(x);
+        out[q * plane] = h;
+        x -= (double)__bfloat162float(h);
+    }
+}
+
+// t+ (plus) or t- rows of the +/- tensor-core ladder as np bf16 planes [np][rows_pad][kpad]: row
+// vec n_rows + ij (vector vec, ij over i >= j for t+, i > j for t-), column cd over c >= d (t+) or
+// c > d (t-), the values of build_tpm
+__global__ void build_tpm_planes_kernel(const double *__restrict__ t2s, int64_t nvec, int64_t no, int64_t nv,
+                                        int64_t rows_pad, int64_t kpad, int np, int plus,
+                                        __nv_bfloat16 *__restrict__ out) {
+    const int64_t nrow = plus ? no * (no + 1) / 2 : no * (no - 1) / 2;
+    const int64_t ncol = plus ? nv * (nv + 1) / 2 : nv * (nv - 1) / 2;
+    const int64_t nt2 = nv * no * (nv * no + 1) / 2;
+    const size_t plane = (size_t)rows_pad * kpad;
+    GRID_STRIDE(idx, rows_pad * kpad) {
+        const int64_t rr = idx / kpad, k = idx - rr * kpad;
+        const int64_t vec = nrow > 0 ? rr / nrow : nvec, row = nrow > 0 ? rr - vec * nrow : 0;
+        double val = 0.0;
+        if (vec < nvec && k < ncol) {
+            int64_t i, j, c, d;
+            untri(row, i, j);
+            untri(k, c, d);
+            if (!plus) {   // strict triangles: M(M-1)/2 + m maps to (M-1, m)
+                i += 1;
+                c += 1;
+            }
+            const double *t2 = t2s + vec * nt2;
+            const double x = t2[pk(c + nv * i, d + nv * j)], y = t2[pk(c + nv * j, d + nv * i)];
+            val = plus ? (c == d ? 0.5 : 1.0) * (i == j ? 0.5 : 1.0) * (x + y) : x - y;
+        }
+        put_planes(val, np, plane, out + idx);
+    }
+}
+
+// g+- of one block of a from G[(c + nv (a - a0)) + ldg (d + nv b)] = g_acbd (a in [a0, a1), b <= a):
+// g+ = g_acbd + g_adbc (c >= d) into P+ row a(a+1)/2 + b - rowp0, column c(c+1)/2 + d; g- = g_acbd -
+// g_adbc (a > b, c > d) into P- row a(a-1)/2 + b - rowm0, column c(c-1)/2 + d; each as np bf16
+// planes.  A block of threads takes one pair (a, b) and one 32 x 32 tile of (c, d) with its mirror
+// tile, staged in shared memory so that both reads run along c and the writes along d.
+__global__ void form_pm_planes_kernel(const double *__restrict__ G, int64_t ldg, int64_t nv, int64_t a0, int64_t a1,
+                                      int np, __nv_bfloat16 *__restrict__ Pp, int64_t kp, size_t plane_p,
+                                      int64_t rowp0, __nv_bfloat16 *__restrict__ Pm, int64_t km, size_t plane_m,
+                                      int64_t rowm0) {
+    __shared__ double sA[32][33], sB[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t abp0 = a0 * (a0 + 1) / 2, npairs = a1 * (a1 + 1) / 2 - abp0;
+    int64_t ct, dt;
+    untri(blockIdx.x, ct, dt);                       // tile pair ct >= dt
+    const int64_t c0 = 32 * ct, d0 = 32 * dt;
+    for (int64_t loc = blockIdx.y; loc < npairs; loc += gridDim.y) {
+        int64_t a, b;
+        untri(abp0 + loc, a, b);
+        const double *Gab = G + nv * (a - a0) + ldg * nv * b;   // Gab[c + ldg d] = g_acbd
+        for (int j = ty; j < 32; j += 8) {
+            const int64_t c = c0 + tx, d = d0 + j, cm = d0 + tx, dm = c0 + j;
+            sA[j][tx] = (c < nv && d < nv) ? Gab[c + ldg * d] : 0.0;       // g_acbd, c = c0 + tx
+            sB[j][tx] = (cm < nv && dm < nv) ? Gab[cm + ldg * dm] : 0.0;   // g_a(d0+tx)b(c0+j)
+        }
+        __syncthreads();
+        const int64_t d = d0 + tx;
+        for (int i = ty; i < 32; i += 8) {
+            const int64_t c = c0 + i;
+            if (c < nv && d <= c) {
+                const double x = sA[tx][i], y = sB[i][tx];      // g_acbd, g_adbc
+                put_planes(x + y, np, plane_p, Pp + (a * (a + 1) / 2 + b - rowp0) * kp + c * (c + 1) / 2 + d);
+                if (a > b && d < c)
+                    put_planes(x - y, np, plane_m, Pm + (a * (a - 1) / 2 + b - rowm0) * km + c * (c - 1) / 2 + d);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void add_omega_pm_kernel(double *__restrict__ om2, const double *__restrict__ wp,
                                     const double *__restrict__ wm, int64_t no, int64_t nv, int64_t a0, int64_t a1,
                                     int64_t ldwp, int64_t ldwm) {
@@ -87,64 +166,6 @@ __global__ void add_omega_pm_kernel(double *__restrict__ om2, const double *__re
         if (i != j && a != b) {
             int64_t ijm = i * (i - 1) / 2 + j, locm = a * (a - 1) / 2 + b - abm0;
             double m = wm[ijm + ldwm * locm];
-            x1 = p + m;
-            x2 = p - m;
-        }
-        int64_t P1 = pk(a + nv * i, b + nv * j), P2 = pk(a + nv * j, b + nv * i);
-        if (P1 == P2) {
-            om2[P1] += x1 + x2;
-        } else {
-            om2[P1] += x1;
-            om2[P2] += x2;
-        }
-    }
-}
-
-// T+ and T- of the full-(c,d) ladder as split bf16 rows: row ij_p (i >= j) carries
-// 1/2 (1 - d_ij/2)(t_cidj + t_cjdi), row n_o_p + ij_m (i > j) carries 1/2 (t_cidj - t_cjdi),
-// both at K position c + nv*d; padding rows/columns are zero.
-__global__ void build_T_kernel(const double *__restrict__ t2s, int64_t nvec, int64_t no, int64_t nv, int64_t rows_pad,
-                               int64_t Kq, int np, __nv_bfloat16 *__restrict__ out) {
-    const int64_t nop = no * (no + 1) / 2, nrow = no * no, nv2 = nv * nv, nt2 = nv * no * (nv * no + 1) / 2;
-    const size_t plane = (size_t)rows_pad * Kq;
-    GRID_STRIDE(idx, rows_pad * Kq) {
-        int64_t rr = idx / Kq, k = idx - (idx / Kq) * Kq;
-        const int64_t vec = rr / nrow, row = rr - vec * nrow;   // vector vec owns rows [vec nrow, (vec+1) nrow)
-        const double *t2 = t2s + vec * nt2;
-        double val = 0.0;
-        if (vec < nvec && k < nv2) {
-            int64_t c = k % nv, d = k / nv, i, j;
-            bool plus = row < nop;
-            if (plus) untri(row, i, j);
-            else {
-                untri(row - nop, i, j);   // strict: idx = M(M-1)/2 + m maps to (M-1, m)
-                i += 1;
-            }
-            double x = t2[pk(c + nv * i, d + nv * j)];
-            double y = t2[pk(c + nv * j, d + nv * i)];
-            val = plus ? 0.5 * (i == j ? 0.5 : 1.0) * (x + y) : 0.5 * (x - y);
-        }
-        for (int p = 0; p < np; p++) {
-            __nv_bfloat16 q = __double2bfloat16(val);
-            out[p * plane + idx] = q;
-            val -= (double)__bfloat162float(q);
-        }
-    }
-}
-
-// Omega contributions from W (nab x n_o^2, column-major, ldw): column ij_p holds omega+,
-// column n_o_p + ij_m holds omega- for the pair row ab = a(a+1)/2 + b.
-__global__ void add_omega_T_kernel(double *__restrict__ om2, const double *__restrict__ W, int64_t ldw, int64_t no,
-                                   int64_t nv) {
-    const int64_t nop = no * (no + 1) / 2, nab = nv * (nv + 1) / 2;
-    GRID_STRIDE(idx, nab * nop) {
-        int64_t ab = idx % nab, ij = idx / nab, a, b, i, j;
-        untri(ab, a, b);
-        untri(ij, i, j);
-        double p = W[ab + ldw * ij] * (a == b ? 0.5 : 1.0);
-        double x1 = p, x2 = p;
-        if (i != j && a != b) {
-            double m = W[ab + ldw * (nop + i * (i - 1) / 2 + j)];
             x1 = p + m;
             x2 = p - m;
         }
@@ -458,16 +479,21 @@ void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int
     CU_CHECK(cudaGetLastError());
 }
 
-void build_T(Exec &ex, const double *t2s, int64_t nvec, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
-             __nv_bfloat16 *out) {
-    build_T_kernel<<<grid_for(rows_pad * Kq, 256), 256, 0, ex.stream>>>(t2s, nvec, no, nv, rows_pad, Kq, np, out);
+void build_tpm_planes(Exec &ex, const double *t2s, int64_t nvec, int64_t no, int64_t nv, bool plus, int64_t rows_pad,
+                      int64_t kpad, int np, __nv_bfloat16 *out) {
+    build_tpm_planes_kernel<<<grid_for(rows_pad * kpad, 256), 256, 0, ex.stream>>>(t2s, nvec, no, nv, rows_pad, kpad,
+                                                                                  np, plus ? 1 : 0, out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }
 
-void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv) {
-    int64_t total = (nv * (nv + 1) / 2) * (no * (no + 1) / 2);
-    add_omega_T_kernel<<<grid_for(total, 256), 256, 0, ex.stream>>>(om2, W, ldw, no, nv);
+void form_pm_planes(Exec &ex, const double *G, int64_t ldg, int64_t nv, int64_t a0, int64_t a1, int np,
+                    __nv_bfloat16 *Pp, int64_t kp, size_t plane_p, int64_t rowp0, __nv_bfloat16 *Pm, int64_t km,
+                    size_t plane_m, int64_t rowm0) {
+    const int64_t nt = (nv + 31) / 32, npairs = a1 * (a1 + 1) / 2 - a0 * (a0 + 1) / 2;
+    dim3 grid((unsigned)(nt * (nt + 1) / 2), (unsigned)std::min<int64_t>(npairs, 65535));
+    form_pm_planes_kernel<<<grid, dim3(32, 8), 0, ex.stream>>>(G, ldg, nv, a0, a1, np, Pp, kp, plane_p, rowp0, Pm, km,
+                                                              plane_m, rowm0);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }

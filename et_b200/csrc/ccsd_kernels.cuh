@@ -22,11 +22,15 @@ void form_gpm(Exec &ex, const double *G, int64_t ldg, double *gp, double *gm, in
 void add_omega_pm(Exec &ex, double *om2, const double *wp, const double *wm, int64_t no, int64_t nv, int64_t a0,
                   int64_t a1, int64_t ldwp, int64_t ldwm);
 
-// T+/T- rows of the tensor-core ladder (np split-bf16 planes, [np][rows_pad][Kq]) for nvec packed
-// vectors (stride n_t2; vector v owns rows [v n_o^2, (v+1) n_o^2)) and the scatter of its result
-void build_T(Exec &ex, const double *t2s, int64_t nvec, int64_t no, int64_t nv, int64_t rows_pad, int64_t Kq, int np,
-             __nv_bfloat16 *out);
-void add_omega_T(Exec &ex, double *om2, const double *W, int64_t ldw, int64_t no, int64_t nv);
+// the +/- ladder on the tensor cores: t+ (plus) or t- of nvec packed vectors as np bf16 planes
+// [np][rows_pad][kpad] (rows: vector-major i >= j or i > j; columns: c >= d or c > d; build_tpm's
+// values), and g+- of the pairs a in [a0, a1) as planes of P+ [np][.][kp] (rows a(a+1)/2 + b - rowp0)
+// and P- [np][.][km] (rows a(a-1)/2 + b - rowm0) from G = g_acbd in form_gpm's layout
+void build_tpm_planes(Exec &ex, const double *t2s, int64_t nvec, int64_t no, int64_t nv, bool plus, int64_t rows_pad,
+                      int64_t kpad, int np, __nv_bfloat16 *out);
+void form_pm_planes(Exec &ex, const double *G, int64_t ldg, int64_t nv, int64_t a0, int64_t a1, int np,
+                    __nv_bfloat16 *Pp, int64_t kp, size_t plane_p, int64_t rowp0, __nv_bfloat16 *Pm, int64_t km,
+                    size_t plane_m, int64_t rowm0);
 
 // eta of the multiplier equation (construct_eta_ccsd, multiplier_equation_ccsd.F90:50-113) and the
 // initial multipliers (t1, packed contravariant t2; ccsd_class.F90:411-475)

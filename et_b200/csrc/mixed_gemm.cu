@@ -115,36 +115,6 @@ __device__ __forceinline__ void store_split_planes(__nv_bfloat16 *out, size_t pl
     if (np == 3) out[2 * plane + idx] = __float2bfloat16(r - __bfloat162float(mid));
 }
 
-// A2 ladder integrals: row (c, a) = c + nv*(a - a0), column (d, b) = d + nv*b of
-// G = L_vv^T L_vv is M_ab[c,d] = g_acbd; kept for b <= a and written as np bf16 planes at
-// pair row ab = a(a+1)/2 + b, K position c + nv*d.
-struct EpiPairs {
-    static constexpr bool kChunked = false;
-    __nv_bfloat16 *out;
-    size_t plane;
-    long long ldk;
-    long long row0;   // pair row of out's first row (a buffer holding a block of pair rows)
-    int nv, a0, M, N, np;
-    int a, c;
-    __device__ __forceinline__ void tile_setup(int) {}
-    __device__ __forceinline__ void row_setup(int row) {
-        a = a0 + row / nv;
-        c = row - (row / nv) * nv;
-    }
-    // the pair epilogue stores bf16 planes, so it takes the whole K range as one chunk
-    __device__ __forceinline__ void apply16(int row, int col0, const float (&v)[16], bool) const {
-#pragma unroll
-        for (int j = 0; j < 16; j++) store(row, col0 + j, v[j]);
-    }
-    __device__ __forceinline__ void store(int row, int col, float v) const {
-        if (row >= M || col >= N) return;
-        const int b = col / nv, d = col - b * nv;
-        if (b > a) return;
-        const size_t idx = (size_t)((long long)a * (a + 1) / 2 + b - row0) * ldk + c + (long long)nv * d;
-        store_split_planes(out, plane, idx, v, np);
-    }
-};
-
 // ovvv integrals of the untransformed Cholesky vectors for the ladder's Y intermediate: row
 // (c, k) = c + nv*k of L_ov, column (d, b) = d + nv*b of L_vv, so G = L_ov^T L_vv holds
 // g_kcbd; written as np bf16 planes at row k + no*b, K position c + nv*d (the 32 lanes of a warp
@@ -714,25 +684,6 @@ void tc_gemm_ovvv(Exec &ex, const __nv_bfloat16 *Lov, int64_t ov_rows, const __n
     epi.N = (int)(nv * nv);
     epi.np = check_planes(ex.planes);
     launch_tc(ex, epi.np, Lov, ov_rows, ov_rows * Kp, epi.M, Lvv, vv_rows, vv_rows * Kp, epi.N, Kp, epi,
-              double(epi.M) * double(epi.N) * double(k_true));
-}
-
-void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,
-                   __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld, int64_t k_true, int64_t row0) {
-    REQUIRE(row0 <= a0 * (a0 + 1) / 2 && a1 * (a1 + 1) / 2 - row0 <= out_rows_pad, CCSD_GPU_EINVAL,
-            "tc_gemm_pairs: pair rows outside the buffer");
-    EpiPairs epi{};
-    epi.out = out;
-    epi.row0 = row0;
-    epi.plane = (size_t)out_rows_pad * (size_t)out_ld;
-    epi.ldk = out_ld;
-    epi.nv = (int)nv;
-    epi.a0 = (int)a0;
-    epi.M = (int)(nv * (a1 - a0));
-    epi.N = (int)(nv * a1);
-    epi.np = check_planes(ex.planes);
-    const int64_t r0 = nv * a0;
-    launch_tc(ex, epi.np, L + r0 * Kp, l_rows - r0, l_rows * Kp, epi.M, L, l_rows, l_rows * Kp, epi.N, Kp, epi,
               double(epi.M) * double(epi.N) * double(k_true));
 }
 

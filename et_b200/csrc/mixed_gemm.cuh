@@ -61,13 +61,6 @@ void tc_gemm_ovvv(Exec &ex, const __nv_bfloat16 *Lov, int64_t ov_rows, const __n
                   int64_t Kp, int64_t no, int64_t nv, __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld,
                   int64_t k_true);
 
-// A2 ladder integrals for a in [a0,a1).  L holds split rows r = c + nv*a (l_rows rows per plane,
-// K = N_J padded to Kp): M_ab[c,d] = sum_J L[c + nv a] L[d + nv b] for b < a1; pairs b <= a are
-// written as split bf16 to out[plane][a(a+1)/2 + b - row0][c + nv*d] (row stride out_ld, plane
-// stride out_rows_pad * out_ld; row0 > 0 for a buffer that holds one block of pair rows).
-void tc_gemm_pairs(Exec &ex, const __nv_bfloat16 *L, int64_t l_rows, int64_t Kp, int64_t nv, int64_t a0, int64_t a1,
-                   __nv_bfloat16 *out, int64_t out_rows_pad, int64_t out_ld, int64_t k_true, int64_t row0 = 0);
-
 // The same GEMM with its split scratch in a fixed file-scope device array (no allocation);
 // synchronous, throws CCSD_GPU_ETIMEOUT when a bounded wait ran out.
 void mixed_gemm_noalloc(bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
