@@ -213,8 +213,11 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov, bool const_t1) {
         g.permute(D, "ckaj->ckaj", -1.0, C);
         g.contract(D, "Jai,Jkc->ckai", 2.0, Lt_vo, Lt_ov);
         g.contract(C, "kcld,djak->claj", -0.5, G4, tf);
-        g.contract(D, "lckd,dkaj->claj", 1.0, G4, u);
-        g.contract(D, "kcld,dkaj->claj", -0.5, G4, u);
+        // the two g_ovov terms of D share u: one contraction with H_lckd = g_lckd - 1/2 g_kcld
+        const int H = g.zeros("H_lckd", {no, nv, no, nv});
+        g.permute(H, "lckd->lckd", 1.0, G4);
+        g.permute(H, "kcld->lckd", -0.5, G4);
+        g.contract(D, "lckd,dkaj->claj", 1.0, H, u);
         const int x = g.zeros("x_c2", V4);
         g.contract(x, "akci,ckbj->aibj", -1.5, tf, C);
         g.contract(om, "aick,ckbj->aibj", 0.5, u, D);

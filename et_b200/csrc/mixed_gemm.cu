@@ -343,78 +343,81 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
     }
 }
 // FP64 operand (a strided gather: element (r, k) at p[roff(r) + koff(k)], the row and K indices
-// each spread over up to four tensor dimensions) -> np bf16 planes, K-major [plane][Rp][Kp], zero
-// padded: plane q holds the bf16 rounding of x minus the planes before it.  One pass reads the FP64
-// tensor in whatever order its dimensions lie and writes the planes, so an operand whose indices are
-// not in GEMM order needs no FP64 reordering copy first.  32 x 64 tiles staged in shared memory:
-// the reads run along the tensor's unit-stride index (rows or K), the writes along K as bf16 pairs.
-constexpr int GS_R = 32, GS_K = 64, GS_LD = GS_K + 2;   // row pitch: 16-byte aligned double pairs
+// each spread over up to four tensor dimensions) -> np bf16 planes, K-major [plane][Rp][Kp]: plane q
+// holds the bf16 rounding of x minus the planes before it.  One pass reads the FP64 tensor in
+// whatever order its dimensions lie and writes the planes, so an operand whose indices are not in
+// GEMM order needs no FP64 reordering copy first.
+//
+// The work is cut into boxes of 32 x 32 in the digits of two tensor dimensions: `a`, the first K
+// dimension (consecutive a are consecutive K positions, so the stores run along K), and `b`, the
+// tensor's unit-stride dimension where that is another one (so the loads run along it; otherwise the
+// first row dimension).  Every other digit is fixed per box.  Each warp takes boxes on its own: 8-byte
+// asynchronous copies (cp.async) along the unit-stride digit into its shared-memory tile, then bf16
+// planes stored along a.  Padding rows and K positions are cleared separately.
+constexpr int GS_WARPS = 4, GS_T = 32, GS_LD = GS_T + 1, GS_REST = 6;
 
-__global__ void __launch_bounds__(256) gather_split_kernel(SplitView v, int R, int K, int Rp, int Kp, int np,
-                                                            __nv_bfloat16 *__restrict__ out) {
-    __shared__ __align__(16) double tile[GS_R * GS_LD];
-    __shared__ long long roff[GS_R], koff[GS_K];
-    const int tid = threadIdx.x;
-    const int tiles_k = (Kp + GS_K - 1) / GS_K;
-    const long long ntiles = (long long)(Rp / GS_R) * tiles_k;
-    const bool row_fast = v.rs[0] == 1 && v.ks[0] != 1;
+struct GatherPlan {
+    const double *p;
+    long long na, nb;           // extents of the a and b digits
+    long long sa, sb;           // their memory strides
+    long long orb, okb;         // output row / K step of one b (a steps K by 1)
+    int lanes_on_a;             // the loads run along a (a has unit stride)
+    int nrest;
+    long long rn[GS_REST], rs[GS_REST], ror[GS_REST], rok[GS_REST];
+};
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+
+__global__ void __launch_bounds__(GS_WARPS * 32) gather_split_kernel(GatherPlan g, long long ntiles, int Rp, int Kp,
+                                                                      int np, __nv_bfloat16 *__restrict__ out) {
+    __shared__ __align__(16) double tiles[GS_WARPS][GS_T * GS_LD];   // element (i, j) at [j * GS_LD + i]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *tile = tiles[warp];
+    const long long ta = (g.na + GS_T - 1) / GS_T, tb = (g.nb + GS_T - 1) / GS_T;
     const size_t plane = (size_t)Rp * Kp;
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int r0 = (int)(t / tiles_k) * GS_R, k0 = (int)(t % tiles_k) * GS_K;
-        if (tid < GS_R) {
-            long long x = r0 + tid, off = -1;
-            if (x < R) {
-                off = 0;
-                for (int d = 0; d < v.nr; d++) {
-                    const long long q = x / v.rn[d];
-                    off += (x - q * v.rn[d]) * v.rs[d];
-                    x = q;
+    for (long long t = (long long)blockIdx.x * GS_WARPS + warp; t < ntiles; t += (long long)gridDim.x * GS_WARPS) {
+        const long long ca = t % ta, t1 = t / ta, cb = t1 % tb;
+        long long rest = t1 / tb, mem = 0, row = 0, kpos = 0;
+        for (int d = 0; d < g.nrest; d++) {
+            const long long q = rest / g.rn[d], x = rest - q * g.rn[d];
+            mem += x * g.rs[d];
+            row += x * g.ror[d];
+            kpos += x * g.rok[d];
+            rest = q;
+        }
+        const long long a0 = GS_T * ca, b0 = GS_T * cb;
+        const int na = (int)min(g.na - a0, (long long)GS_T), nb = (int)min(g.nb - b0, (long long)GS_T);
+        const double *base = g.p + mem + a0 * g.sa + b0 * g.sb;
+        if (g.lanes_on_a) {
+            const double *src = base + lane * g.sa;
+#pragma unroll 8
+            for (int j = 0; j < GS_T; j++) cp_async8(tile + j * GS_LD + lane, lane < na && j < nb ? src + j * g.sb : g.p,
+                                                     lane < na && j < nb);
+        } else {
+            const double *src = base + lane * g.sb;
+#pragma unroll 8
+            for (int i = 0; i < GS_T; i++) cp_async8(tile + lane * GS_LD + i, i < na && lane < nb ? src + i * g.sa : g.p,
+                                                     i < na && lane < nb);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncwarp();
+        if (lane < na) {
+            const long long r_base = row + b0 * g.orb, k_base = kpos + a0 + lane + b0 * g.okb;
+            for (int j = 0; j < nb; j++) {
+                double y = tile[j * GS_LD + lane];
+                __nv_bfloat16 *o = out + (size_t)(r_base + j * g.orb) * Kp + (k_base + j * g.okb);
+                for (int q = 0; q < np; q++) {
+                    const __nv_bfloat16 h = __double2bfloat16(y);
+                    o[q * plane] = h;
+                    y -= (double)__bfloat162float(h);
                 }
             }
-            roff[tid] = off;
-        } else if (tid < GS_R + GS_K) {
-            long long x = k0 + tid - GS_R, off = -1;
-            if (x < K) {
-                off = 0;
-                for (int d = 0; d < v.nk; d++) {
-                    const long long q = x / v.kn[d];
-                    off += (x - q * v.kn[d]) * v.ks[d];
-                    x = q;
-                }
-            }
-            koff[tid - GS_R] = off;
         }
-        __syncthreads();
-        double x[GS_R * GS_K / 256];
-#pragma unroll
-        for (int it = 0; it < GS_R * GS_K / 256; it++) {
-            const int e = tid + 256 * it;
-            const int i = row_fast ? e % GS_R : e / GS_K, j = row_fast ? e / GS_R : e % GS_K;
-            const long long ro = roff[i], ko = koff[j];
-            x[it] = (ro >= 0 && ko >= 0) ? __ldg(v.p + ro + ko) : 0.0;
-        }
-#pragma unroll
-        for (int it = 0; it < GS_R * GS_K / 256; it++) {
-            const int e = tid + 256 * it;
-            const int i = row_fast ? e % GS_R : e / GS_K, j = row_fast ? e / GS_R : e % GS_K;
-            tile[i * GS_LD + j] = x[it];
-        }
-        __syncthreads();
-        // warp w writes rows w, w + 8, ...; lane l the K pair (2l, 2l + 1) of every plane
-        const int warp = tid >> 5, lane = tid & 31, k = k0 + 2 * lane;
-        for (int i = warp; i < GS_R; i += 8) {
-            const int r = r0 + i;
-            if (r >= Rp || k >= Kp) continue;
-            double2 y = *reinterpret_cast<const double2 *>(&tile[i * GS_LD + 2 * lane]);
-            const size_t o = (size_t)r * Kp + k;
-            for (int q = 0; q < np; q++) {
-                const __nv_bfloat16 a = __double2bfloat16(y.x), b = __double2bfloat16(y.y);
-                *reinterpret_cast<__nv_bfloat162 *>(out + q * plane + o) = __halves2bfloat162(a, b);
-                y.x -= (double)__bfloat162float(a);
-                y.y -= (double)__bfloat162float(b);
-            }
-        }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -520,12 +523,73 @@ int n_tile(int planes) { return planes == 3 ? ModeX6::BN : ModeX3::BN; }
 
 void split_view(Exec &ex, const SplitView &v, int64_t R, int64_t K, int64_t Rp, int64_t Kp, int planes,
                 __nv_bfloat16 *out) {
-    REQUIRE(Rp % GS_R == 0 && Kp % 2 == 0 && R <= Rp && K <= Kp && Kp < (1ll << 31) && Rp < (1ll << 31),
-            CCSD_GPU_EINVAL, "operand split: bad padding");
+    REQUIRE(R >= 1 && K >= 1 && R <= Rp && K <= Kp && Kp < (1ll << 31) && Rp < (1ll << 31), CCSD_GPU_EINVAL,
+            "operand split: bad padding");
     REQUIRE(v.nr >= 1 && v.nr <= 4 && v.nk >= 1 && v.nk <= 4, CCSD_GPU_EINVAL, "operand split: 1 to 4 dims per group");
-    const int64_t tiles = (Rp / GS_R) * ((Kp + GS_K - 1) / GS_K);
-    const int blocks = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * 8);
-    gather_split_kernel<<<blocks, 256, 0, ex.stream>>>(v, (int)R, (int)K, (int)Rp, (int)Kp, planes, out);
+    // the digits: extent, memory stride, output row step, output K step
+    struct Digit {
+        long long n, s, orow, ok;
+    };
+    std::vector<Digit> dig;
+    long long step = 1, prod_r = 1, prod_k = 1;
+    for (int d = 0; d < v.nr; d++) {
+        REQUIRE(v.rn[d] >= 1, CCSD_GPU_EINVAL, "operand split: bad extent");
+        dig.push_back({v.rn[d], v.rs[d], step, 0});
+        step *= v.rn[d];
+    }
+    prod_r = step;
+    const int k_first = (int)dig.size();
+    step = 1;
+    for (int d = 0; d < v.nk; d++) {
+        REQUIRE(v.kn[d] >= 1, CCSD_GPU_EINVAL, "operand split: bad extent");
+        dig.push_back({v.kn[d], v.ks[d], 0, step});
+        step *= v.kn[d];
+    }
+    prod_k = step;
+    REQUIRE(prod_r == R && prod_k == K, CCSD_GPU_EINVAL, "operand split: view extents do not match the operand");
+    // a: the first K digit; b: the unit-stride digit if another one has it, else the first row digit
+    const int ia = k_first;
+    int ib = -1;
+    for (int d = 0; d < (int)dig.size(); d++)
+        if (d != ia && dig[d].n > 1 && dig[d].s == 1 && dig[ia].s != 1) ib = d;
+    if (ib < 0) {
+        for (int d = 0; d < (int)dig.size(); d++)
+            if (d != ia && dig[d].n > 1) {
+                ib = d;
+                break;
+            }
+    }
+    GatherPlan g{};
+    g.p = v.p;
+    g.na = dig[ia].n;
+    g.sa = dig[ia].s;
+    g.lanes_on_a = dig[ia].s == 1 || ib < 0 || dig[ib].s != 1;
+    if (ib >= 0) {
+        g.nb = dig[ib].n;
+        g.sb = dig[ib].s;
+        g.orb = dig[ib].orow;
+        g.okb = dig[ib].ok;
+    } else {
+        g.nb = 1;
+    }
+    for (int d = 0; d < (int)dig.size(); d++) {
+        if (d == ia || d == ib || dig[d].n == 1) continue;
+        REQUIRE(g.nrest < GS_REST, CCSD_GPU_EINVAL, "operand split: too many dims");
+        g.rn[g.nrest] = dig[d].n;
+        g.rs[g.nrest] = dig[d].s;
+        g.ror[g.nrest] = dig[d].orow;
+        g.rok[g.nrest] = dig[d].ok;
+        g.nrest++;
+    }
+    const long long ntiles = ((g.na + GS_T - 1) / GS_T) * ((g.nb + GS_T - 1) / GS_T) * (R * K / (g.na * g.nb));
+    // padding: the K positions [K, Kp) of every row of every plane, and the rows [R, Rp)
+    const size_t eb = sizeof(__nv_bfloat16);
+    if (Kp > K)
+        CU_CHECK(cudaMemset2DAsync(out + K, Kp * eb, 0, (Kp - K) * eb, (size_t)planes * Rp, ex.stream));
+    if (Rp > R)
+        CU_CHECK(cudaMemset2DAsync(out + R * Kp, Rp * Kp * eb, 0, (Rp - R) * Kp * eb, planes, ex.stream));
+    const int blocks = (int)std::min<long long>((ntiles + GS_WARPS - 1) / GS_WARPS, (long long)sm_count() * 6);
+    gather_split_kernel<<<blocks, GS_WARPS * 32, 0, ex.stream>>>(g, ntiles, (int)Rp, (int)Kp, planes, out);
     ex.launches++;
     CU_CHECK(cudaGetLastError());
 }
