@@ -273,8 +273,14 @@ class CCSD:
         self._check(self.lib.ccsd_gpu_energy(self.ctx, ctypes.byref(e)))
         return e.value
 
-    def construct_omega(self):
-        out = np.empty(self.n_amp)
+    def construct_omega(self, out=None):
+        """Omega at the current amplitudes into a host array: `out` (float64, contiguous, n_amp values,
+        e.g. pinned memory kept across iterations as eT keeps its omega array) or a new array."""
+        if out is None:
+            out = np.empty(self.n_amp)
+        elif not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                  and out.size == self.n_amp):
+            raise ValueError(f"out must be a contiguous float64 array of {self.n_amp} values")
         self._check(self.lib.ccsd_gpu_omega(self.ctx, _dp(out)))
         return out
 

@@ -176,7 +176,7 @@ struct Exec {
     int fp64_digits = 0;
     double fp64_digits_min_flops = 1e10;
     // digits of the first-order (FP64) terms inside a mixed-precision residual (0: cuBLAS DGEMM)
-    int mixed_fp64_digits = 7;
+    int mixed_fp64_digits = 6;
     // grow-only scratch of the digit GEMM (digit planes and exponents), owned by the context: the
     // multi-GB planes are neither allocated nor freed per product
     DBuf *digit_arena = nullptr;
