@@ -21,7 +21,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <mutex>
+#include <type_traits>
 
 #include "mixed_gemm.cuh"
 #include "tc_common.cuh"
@@ -152,6 +154,7 @@ namespace {
 // (instead of every wave streaming the whole of A or B from HBM again).
 struct TileMap {
     int num_mt, num_nt, nk_all, nks, group_m, bn;
+    int bm = BM;            // rows of one tile (256 for a CTA pair)
     int kc;   // K blocks accumulated in TMEM before the epilogue takes the partial sum (FP64)
     int *err;               // the caller's error word (device): a bounded wait that ran out writes its code
     long long wait_cycles;  // bound of every barrier wait
@@ -166,7 +169,7 @@ struct TileMap {
         const int first_m = grp * group_m;
         const int gsz = min(group_m, num_mt - first_m);
         const int mt = first_m + in % gsz, nt = in / gsz;
-        m0 = mt * BM;
+        m0 = mt * bm;
         n0 = nt * bn;
         kt0 = z * nks;
         nk = min(nks, nk_all - kt0);
@@ -342,6 +345,247 @@ split_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_con
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
     }
 }
+// The same GEMM on a pair of CTAs (a cluster of two on neighbouring SMs) sharing one tcgen05 MMA of
+// M = 256 (cta_group::2): each CTA stages its own 128 rows of A and half of the 256-wide B tile, so
+// a CTA moves 64 KB per K block instead of 96 KB and three stages fit in its shared memory (the
+// producer runs two K blocks ahead of the tensor cores instead of one).  CTA 0 of the pair issues
+// the MMAs and waits for both CTAs' loads on its own barriers (the loads of CTA 1 complete on CTA 0's
+// barrier); its commits arrive on the stage and accumulator barriers of both CTAs.  Each CTA's
+// epilogue drains its own TMEM rows and then signals CTA 0 that the accumulator is free.
+namespace {
+
+struct PairMode {
+    static constexpr int NP = 2, KB = 64, BN = 256, STAGES = 3;
+    static constexpr int A_TILE = BM * KB * 2;          // 128 rows of one plane
+    static constexpr int B_TILE = (BN / 2) * KB * 2;    // this CTA's half of the B tile
+    static constexpr int STAGE_BYTES = NP * (A_TILE + B_TILE);
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr uint32_t TMEM_COLS = 2 * BN;
+    static constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+};
+static_assert(PairMode::STAGE_BYTES == 64 * 1024, "pair stage size");
+
+constexpr uint32_t PEER_BIT_CLEAR = 0xFEFFFFFFu;   // shared::cluster address of the same offset in CTA 0
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// tile load into this CTA's shared memory whose bytes complete on CTA 0's barrier
+__device__ __forceinline__ void tma_load_3d_pair(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1,
+                                                 int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+        "%5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar) & PEER_BIT_CLEAR), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// arrives on the barrier at this offset in both CTAs once the pair's MMAs issued so far complete
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"((uint16_t)3)
+        : "memory");
+}
+
+__device__ __forceinline__ void arrive_cta0(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(smem_u32(bar) & PEER_BIT_CLEAR) : "memory");
+}
+
+template <class Epi>
+__global__ void __launch_bounds__(THREADS, 1)
+split_bf16_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TileMap map,
+                       int num_tiles, Epi epi) {
+    using MD = PairMode;
+    constexpr int A_TILE = MD::A_TILE, B_TILE = MD::B_TILE, STAGE_BYTES = MD::STAGE_BYTES, STAGES = MD::STAGES;
+    constexpr int KB = MD::KB, BN = MD::BN;
+    constexpr uint32_t TMEM_COLS = MD::TMEM_COLS;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *acc_full = empty + STAGES;    // [2]
+    uint64_t *acc_empty = acc_full + 2;     // [2], used on CTA 0
+    uint64_t *done = acc_empty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool lead = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 2 * (EPI_THREADS / 32));   // one arrival per epilogue warp of each CTA
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    cluster_sync();   // both CTAs' barriers exist before any load, commit or arrival crosses the pair
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer of this CTA: its A rows and its half of B; CTA 0 expects both CTAs' bytes
+            int g = 0;
+            int issued[STAGES] = {};
+            for (int t = pair; t < num_tiles && !*abort_flag; t += npairs) {
+                int m0, n0, z, kt0, nk;
+                map.decode(t, m0, n0, z, kt0, nk);
+                for (int i = 0; i < nk; i++, g++) {
+                    const int s = g % STAGES;
+                    if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1, map.wait_cycles) || *abort_flag) {
+                        record_error(map.err, ERR_PRODUCER);
+                        *abort_flag = 1;
+                        break;
+                    }
+                    if (map.stall_test && g == 0) continue;   // stage 0's first phase never completes
+                    issued[s]++;
+                    uint8_t *st = smem + s * STAGE_BYTES;
+                    if (lead) mbar_expect_tx(&full[s], 2 * STAGE_BYTES);
+                    const int k0 = (kt0 + i) * KB;
+#pragma unroll
+                    for (int p = 0; p < MD::NP; p++) {
+                        tma_load_3d_pair(&tmA, &full[s], st + p * A_TILE, k0, m0 + BM * (int)rank, p);
+                        tma_load_3d_pair(&tmB, &full[s], st + MD::NP * A_TILE + p * B_TILE, k0, n0 + (BN / 2) * (int)rank,
+                                         p);
+                    }
+                }
+            }
+            // CTA 0 waits for the last load of each stage (both CTAs' bytes land on its barrier); CTA 1
+            // keeps its shared memory until the final cluster barrier, which CTA 0 reaches after this
+            if (lead)
+                for (int s = 0; s < STAGES; s++)
+                    if (issued[s] && !mbar_wait(&full[s], (issued[s] - 1) & 1, map.wait_cycles))
+                        record_error(map.err, ERR_DRAIN);
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && lead) {
+            // MMA issuer of the pair
+            int g = 0, tc = 0;
+            for (int t = pair; t < num_tiles && !*abort_flag; t += npairs) {
+                int m0, n0, z, kt0, nk;
+                map.decode(t, m0, n0, z, kt0, nk);
+                for (int c0 = 0; c0 < nk && !*abort_flag; c0 += map.kc, tc++) {
+                    const int acc = tc & 1;
+                    if (!mbar_wait(&acc_empty[acc], ((tc >> 1) & 1) ^ 1, map.wait_cycles)) {
+                        record_error(map.err, ERR_MMA_ACC);
+                        *abort_flag = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t d = tmem + (uint32_t)(acc * BN);
+                    const int c1 = min(nk, c0 + map.kc);
+                    for (int i = c0; i < c1; i++, g++) {
+                        const int s = g % STAGES;
+                        if (!mbar_wait(&full[s], (g / STAGES) & 1, map.wait_cycles) || *abort_flag) {
+                            record_error(map.err, ERR_MMA_FULL);
+                            *abort_flag = 1;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const uint8_t *st = smem + s * STAGE_BYTES;
+#pragma unroll
+                        for (int kk = 0; kk < KB / 16; kk++) {
+                            const uint32_t ko = kk * 32;
+#pragma unroll
+                            for (int p = 0; p < 3; p++) {
+                                // hi*hi, hi*lo, lo*hi
+                                const uint8_t *ta = st + (p == 2 ? 1 : 0) * A_TILE;
+                                const uint8_t *tb = st + MD::NP * A_TILE + (p == 1 ? 1 : 0) * B_TILE;
+                                mma_bf16_pair(d, smem_desc_k<128>(ta, ko), smem_desc_k<128>(tb, ko), MD::IDESC,
+                                              (i > c0 || kk > 0 || p > 0) ? 1u : 0u);
+                            }
+                        }
+                        mma_commit_pair(&empty[s]);
+                    }
+                    mma_commit_pair(&acc_full[acc]);
+                }
+            }
+            mma_commit_pair(done);
+        }
+    } else {
+        // epilogue: this CTA's 128 rows; warp w reads TMEM lanes 32*(w % 4) .. +31
+        const int quarter = warp & 3;
+        int tc = 0;
+        bool aborted = false;
+        for (int t = pair; t < num_tiles && !aborted; t += npairs) {
+            int m0, n0, z, kt0, nk;
+            map.decode(t, m0, n0, z, kt0, nk);
+            for (int c0 = 0; c0 < nk; c0 += map.kc, tc++) {
+                const int acc = tc & 1;
+                bool ok = !*abort_flag && mbar_wait(&acc_full[acc], (tc >> 1) & 1, map.wait_cycles);
+                __syncwarp();
+                if (!ok || *abort_flag) {
+                    record_error(map.err, ERR_EPILOGUE);
+                    *abort_flag = 1;
+                    aborted = true;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const int row = m0 + BM * (int)rank + quarter * 32 + lane;
+                epi.tile_setup(z);
+                epi.row_setup(row);
+                const uint32_t base = tmem + (uint32_t)(acc * BN) + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll 1
+                for (int cc = 0; cc < BN; cc += 16) {
+                    float v[16];
+                    tmem_ld16(base + (uint32_t)cc, v);
+                    epi.apply16(row, n0 + cc, v, c0 == 0);
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) arrive_cta0(&acc_empty[acc]);
+            }
+        }
+    }
+    __syncthreads();
+    // every MMA of the pair complete before the TMEM is released (CTA 0's commit reaches both CTAs)
+    if (!mbar_wait(done, 0, map.wait_cycles)) record_error(map.err, ERR_DONE);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    cluster_sync();   // no arrival or load of either CTA is still headed for the other
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+}  // namespace
+
 // FP64 operand (a strided gather: element (r, k) at p[roff(r) + koff(k)], the row and K indices
 // each spread over up to four tensor dimensions) -> np bf16 planes, K-major [plane][Rp][Kp]: plane q
 // holds the bf16 rounding of x minus the planes before it.  One pass reads the FP64 tensor in
@@ -509,10 +753,92 @@ void launch_mode(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_pla
     }
 }
 
+// the two-plane GEMM on CTA pairs: tiles of 256 x 256, persistent over the pairs that can be resident
+template <class Epi>
+void launch_pair(Exec &ex, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t m_out,
+                 const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t n_out, int64_t Kp, const Epi &epi,
+                 double mnk, int splits) {
+    using MD = PairMode;
+    const int64_t Mp = round_up(m_out, 2 * BM), Np = round_up(n_out, MD::BN);
+    REQUIRE(Kp % BK == 0 && Kp > 0 && Mp > 0 && Np > 0, CCSD_GPU_EINVAL, "tc gemm: bad padding");
+    auto kernel = split_bf16_pair_kernel<Epi>;
+    CU_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MD::SMEM_BYTES));
+    // rows beyond a buffer's own rows (the second CTA of the last pair tile) read as zero
+    CUtensorMap ta = make_map(const_cast<__nv_bfloat16 *>(A), a_rows, Kp, BM, a_plane, MD::NP, MD::KB);
+    CUtensorMap tb = make_map(const_cast<__nv_bfloat16 *>(B), b_rows, Kp, MD::BN / 2, b_plane, MD::NP, MD::KB);
+    TileMap map;
+    map.bm = 2 * BM;
+    map.num_mt = (int)(Mp / (2 * BM));
+    map.num_nt = (int)(Np / MD::BN);
+    map.nk_all = (int)(Kp / MD::KB);
+    map.nks = (map.nk_all + splits - 1) / splits;
+    map.bn = MD::BN;
+    map.group_m = std::min(map.num_mt, 8);
+    map.kc = (Epi::kChunked && ex.k_chunk > 0) ? (int)std::max<int64_t>(1, ex.k_chunk / MD::KB) : map.nks;
+    REQUIRE(ex.gemm_err != nullptr, CCSD_GPU_EINVAL, "tc gemm: no error word");
+    map.err = ex.gemm_err;
+    map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : WAIT_CYCLES;
+    map.stall_test = ex.stall_test;
+    const int num_tiles = map.num_mt * map.num_nt * splits;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = MD::SMEM_BYTES;
+    cfg.stream = ex.stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    static int max_pairs[128] = {};
+    int dev = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    int &mp = max_pairs[dev & 127];
+    if (mp == 0) {
+        cfg.gridDim = dim3((unsigned)(2 * (sm_count() / 2)));
+        int n = 0;
+        CU_CHECK(cudaOccupancyMaxActiveClusters(&n, kernel, &cfg));
+        mp = std::max(1, n);
+    }
+    cfg.gridDim = dim3((unsigned)(2 * std::min(num_tiles, mp)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ex.prof && ex.prof->on) {
+        CU_CHECK(cudaEventCreate(&e0));
+        CU_CHECK(cudaEventCreate(&e1));
+        CU_CHECK(cudaEventRecord(e0, ex.stream));
+    }
+    CU_CHECK(cudaLaunchKernelEx(&cfg, kernel, ta, tb, map, num_tiles, epi));
+    ex.launches++;
+    if (e0) {
+        CU_CHECK(cudaEventRecord(e1, ex.stream));
+        ex.prof->events.emplace_back(e0, e1);
+        ex.prof->flops.push_back(2.0 * 3 * mnk);
+    }
+}
+
+// CTA pairs for two-plane FP64-output products with at least one full pair tile of rows, when
+// CCSD_GPU_PAIR_GEMM=1.  Off by default: at 10240^3 the pair runs at the single-CTA kernel's speed
+// (4.77 vs 4.75 ms, both near the power-capped bf16 rate), and the 256-row tiles pad the ladder's
+// 528-row operand further than 128-row tiles do.
+bool pair_gemm_on() {
+    static const bool on = [] {
+        const char *e = std::getenv("CCSD_GPU_PAIR_GEMM");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 template <class Epi>
 void launch_tc(Exec &ex, int planes, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t m_out,
                const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t n_out, int64_t Kp, const Epi &epi,
                double mnk, int splits = 1) {
+    if constexpr (std::is_same<Epi, EpiF64>::value) {
+        if (planes == 2 && m_out >= 2 * BM && pair_gemm_on()) {
+            launch_pair(ex, A, a_rows, a_plane, m_out, B, b_rows, b_plane, n_out, Kp, epi, mnk, splits);
+            return;
+        }
+    }
     if (planes == 3)
         launch_mode<ModeX6>(ex, A, a_rows, a_plane, m_out, B, b_rows, b_plane, n_out, Kp, epi, mnk, splits);
     else

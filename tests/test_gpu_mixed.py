@@ -263,3 +263,32 @@ def test_gathered_operands_equal_reordered_copies():
     assert tc_launches > 0
     assert np.array_equal(first, second) and np.array_equal(second, third)
     assert n2 - n1 == n1 - n0
+
+
+def test_cta_pair_gemm_matches_fp64():
+    """The two-plane GEMM on CTA pairs (cta_group::2, M = 256 per pair, CCSD_GPU_PAIR_GEMM=1, read once
+    per process) in a fresh process: the same tolerance against FP64 as the single-CTA kernel, with
+    transposes, a K split and row counts that leave the second CTA of the last pair without rows."""
+    import os
+    import subprocess
+    import sys
+    code = r"""
+import numpy as np
+from et_b200 import CCSD
+rng = np.random.default_rng(7)
+with CCSD(2, 3, 4) as c:
+    for (m, n, k, tA, tB) in [(256, 256, 64, False, False), (300, 1000, 777, True, False),
+                              (640, 512, 1200, False, True), (384, 300, 20000, True, True)]:
+        A = rng.standard_normal((k, m) if tA else (m, k))
+        B = rng.standard_normal((n, k) if tB else (k, n))
+        ref = (A.T if tA else A) @ (B.T if tB else B)
+        out = c.selftest_gemm(A, B, transA=tA, transB=tB, mixed=1)
+        scale = np.abs(A).max() * np.abs(B).max() * np.sqrt(k)
+        err = np.abs(out - ref).max() / scale
+        assert err < 1e-4, (m, n, k, tA, tB, err)
+print("ok")
+"""
+    env = dict(os.environ, CCSD_GPU_PAIR_GEMM="1")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]
