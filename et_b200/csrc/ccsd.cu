@@ -942,10 +942,13 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         have_corr = true;
         return nrm64;
     };
+    double t_norm_done = 0.0, t_energy = 0.0, t_update = 0.0;
     while (it < maxit) {
         it++;
+        const double t_start = trace ? trace_ms() : 0.0;
         refresh();
         e = energy();
+        if (trace) t_energy = trace_ms() - t_start;
         double nrm;
         bool exact = !mixed;
         if (!mixed || fp64_final) {
@@ -978,9 +981,15 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
         if (trace) {
             double pool_r, pool_u;
             trace_pool(pool_r, pool_u);
+            // phases (host time between the solver's synchronisation points): T1 transformation and
+            // energy, residual(s) and norm, and the previous iteration's update (quasi-Newton + DIIS)
+            const double now = trace_ms();
+            t_norm_done = now;
             std::fprintf(stderr,
-                         "ccsd_gpu gs %3d  E %.12f  |Omega| %.3e  %s  %-6s moved %.3e r_c %.3e  t %.1f ms  pool %.1f/%.1f GB%s\n",
-                         it, e, nrm, exact ? "fp64 " : "mixed", trace_why, trace_moved, r_c, trace_ms(), pool_u, pool_r,
+                         "ccsd_gpu gs %3d  E %.12f  |Omega| %.3e  %s  %-6s moved %.3e r_c %.3e  t %.1f ms  "
+                         "[T1+E %.1f  Omega %.1f  prev update %.1f]  pool %.1f/%.1f GB%s\n",
+                         it, e, nrm, exact ? "fp64 " : "mixed", trace_why, trace_moved, r_c, now, t_energy,
+                         now - t_start - t_energy, t_update, pool_u, pool_r,
                          fp64_final ? "  fp64 from here" : "");
         }
         if (!std::isfinite(nrm) || !std::isfinite(e)) {
@@ -1034,6 +1043,7 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
             throw Error(CCSD_GPU_ESINGULAR, "could not solve DIIS matrix equation");
         }
         prev = e;
+        if (trace) t_update = trace_ms() - t_norm_done;
     }
     ex.prec = user;
     refresh();

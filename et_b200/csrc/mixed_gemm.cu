@@ -366,28 +366,6 @@ struct PairMode {
 };
 static_assert(PairMode::STAGE_BYTES == 64 * 1024, "pair stage size");
 
-constexpr uint32_t PEER_BIT_CLEAR = 0xFEFFFFFFu;   // shared::cluster address of the same offset in CTA 0
-
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-__device__ __forceinline__ void cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-// tile load into this CTA's shared memory whose bytes complete on CTA 0's barrier
-__device__ __forceinline__ void tma_load_3d_pair(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1,
-                                                 int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
-        "%5}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar) & PEER_BIT_CLEAR), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
 __device__ __forceinline__ void mma_bf16_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                               uint32_t accumulate) {
     asm volatile(
@@ -395,19 +373,6 @@ __device__ __forceinline__ void mma_bf16_pair(uint32_t d_tmem, uint64_t adesc, u
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-// arrives on the barrier at this offset in both CTAs once the pair's MMAs issued so far complete
-__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-            smem_u32(bar)),
-        "h"((uint16_t)3)
-        : "memory");
-}
-
-__device__ __forceinline__ void arrive_cta0(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(smem_u32(bar) & PEER_BIT_CLEAR) : "memory");
 }
 
 template <class Epi>
@@ -829,12 +794,13 @@ bool pair_gemm_on() {
     return on;
 }
 
+// pair: the CTA-pair kernel for this launch (a route the autotuner measured), else the default
 template <class Epi>
 void launch_tc(Exec &ex, int planes, const __nv_bfloat16 *A, int64_t a_rows, int64_t a_plane, int64_t m_out,
                const __nv_bfloat16 *B, int64_t b_rows, int64_t b_plane, int64_t n_out, int64_t Kp, const Epi &epi,
-               double mnk, int splits = 1) {
+               double mnk, int splits = 1, bool pair = false) {
     if constexpr (std::is_same<Epi, EpiF64>::value) {
-        if (planes == 2 && m_out >= 2 * BM && pair_gemm_on()) {
+        if (planes == 2 && m_out >= 2 * BM && (pair || pair_gemm_on())) {
             launch_pair(ex, A, a_rows, a_plane, m_out, B, b_rows, b_plane, n_out, Kp, epi, mnk, splits);
             return;
         }
@@ -978,6 +944,11 @@ std::vector<int> tc_split_candidates(int64_t m, int64_t n, int64_t k, int planes
         // counts whose units fill about j waves of the persistent grid
         for (int j = 1; j <= 4; j++) add(j * nsm / tiles, 4);
     }
+    // the same K splits on CTA pairs (256 x 256 tiles) for products with a full pair tile of rows
+    if (planes == 2 && m >= 2 * BM) {
+        const size_t single = out.size();
+        for (size_t i = 0; i < single; i++) out.push_back(PAIR_ROUTE + out[i]);
+    }
     return out;
 }
 
@@ -989,18 +960,21 @@ void mixed_gemm_views(Exec &ex, const SplitView &A, const SplitView &B, int64_t 
     DBuf a(sizeof(__nv_bfloat16) * np * Mp * Kp, ex.stream), b(sizeof(__nv_bfloat16) * np * Np * Kp, ex.stream);
     split_view(ex, A, m, k, Mp, Kp, np, a.as<__nv_bfloat16>());
     split_view(ex, B, n, k, Np, Kp, np, b.as<__nv_bfloat16>());
+    const bool pair = splits >= PAIR_ROUTE;
+    if (pair) splits -= PAIR_ROUTE;
     if (splits <= 0) splits = tc_default_splits(m, n, k, np);
     splits = std::max(1, std::min<int>(splits, (int)(Kp / BK)));
     const double mnk = double(m) * double(n) * double(k);
     if (splits <= 1) {
         EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
-        launch_tc(ex, np, a.as<__nv_bfloat16>(), Mp, Mp * Kp, m, b.as<__nv_bfloat16>(), Np, Np * Kp, n, Kp, epi, mnk);
+        launch_tc(ex, np, a.as<__nv_bfloat16>(), Mp, Mp * Kp, m, b.as<__nv_bfloat16>(), Np, Np * Kp, n, Kp, epi, mnk, 1,
+                  pair);
         return;
     }
     DBuf part = dalloc((int64_t)splits * m * n, ex.stream);
     EpiF64 epi{part.d(), (long long)m, (int)m, (int)n, alpha, 0.0, (long long)m * n};
     launch_tc(ex, np, a.as<__nv_bfloat16>(), Mp, Mp * Kp, m, b.as<__nv_bfloat16>(), Np, Np * Kp, n, Kp, epi, mnk,
-              splits);
+              splits, pair);
     sum_splits_kernel<<<(unsigned)std::min<int64_t>((m * n + 255) / 256, 148 * 64), 256, 0, ex.stream>>>(
         part.d(), splits, m, n, beta, C, ldc);
     ex.launches++;
@@ -1043,16 +1017,18 @@ void tc_gemm_f64(Exec &ex, const __nv_bfloat16 *A, int64_t Mp, const __nv_bfloat
     REQUIRE(Mp >= round_up(m, BM) && Np >= round_up(n, B_ROW_PAD), CCSD_GPU_EINVAL, "tc_gemm_f64: bad padding");
     const int np = check_planes(ex.planes);
     const double mnk = double(m) * double(n) * double(k_true);
+    const bool pair = splits >= PAIR_ROUTE;
+    if (pair) splits -= PAIR_ROUTE;
     if (splits <= 0) splits = wave_splits(Mp / BM * (round_up(n, n_tile(np)) / n_tile(np)), Kp / BK);
     splits = std::max(1, std::min<int>(splits, (int)(Kp / BK)));
     if (splits == 1) {
         EpiF64 epi{C, (long long)ldc, (int)m, (int)n, alpha, beta};
-        launch_tc(ex, np, A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi, mnk);
+        launch_tc(ex, np, A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi, mnk, 1, pair);
         return;
     }
     DBuf part = dalloc((int64_t)splits * m * n, ex.stream);
     EpiF64 epi{part.d(), (long long)m, (int)m, (int)n, alpha, 0.0, (long long)m * n};
-    launch_tc(ex, np, A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi, mnk, splits);
+    launch_tc(ex, np, A, Mp, Mp * Kp, m, B, Np, Np * Kp, n, Kp, epi, mnk, splits, pair);
     sum_splits_kernel<<<(unsigned)std::min<int64_t>((m * n + 255) / 256, 148 * 64), 256, 0, ex.stream>>>(
         part.d(), splits, m, n, beta, C, ldc);
     ex.launches++;

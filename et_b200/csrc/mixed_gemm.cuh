@@ -32,10 +32,16 @@ SplitView matrix_view(const double *p, int64_t rows, int64_t sr, int64_t K, int6
 void mixed_gemm_views(Exec &ex, const SplitView &A, const SplitView &B, int64_t m, int64_t n, int64_t k, double alpha,
                       double beta, double *C, int64_t ldc, int splits = -1);
 
+// Routes (the `splits` argument of the GEMMs below and of mixed_gemm): s in 1..99 runs the
+// single-CTA kernel with s K splits, PAIR_ROUTE + s the CTA-pair kernel (cta_group::2, 256 x 256
+// tiles) with s K splits; 0 or less takes the fixed rule's count.
+constexpr int PAIR_ROUTE = 100;
+
 // K-split count of the fixed rule: split only when the output tiles cannot fill the SMs.
 int tc_default_splits(int64_t m, int64_t n, int64_t k, int planes);
 // K-split counts worth timing for an m x n x k product: 1, the fixed rule's count, and counts whose
-// tile units fill whole waves of the persistent grid.
+// tile units fill whole waves of the persistent grid; for products of at least 256 rows the same
+// counts again as CTA-pair routes.
 std::vector<int> tc_split_candidates(int64_t m, int64_t n, int64_t k, int planes);
 
 // Row / K padding of pre-split operands (A rows to 128, B rows to 256, K to 64).

@@ -75,12 +75,13 @@ struct OzMap {
     const int *ea, *eb;  // row exponents of op(A), column exponents of op(B)
     int *err;
     long long wait_cycles;
+    int bm = OBM;        // rows of one tile (256 for a CTA pair)
     __device__ __forceinline__ void tile(int t, int &m0, int &n0) const {
         const int per_group = group_m * num_nt;
         const int grp = t / per_group, in = t - grp * per_group;
         const int first_m = grp * group_m;
         const int gsz = min(group_m, num_mt - first_m);
-        m0 = (first_m + in % gsz) * OBM;
+        m0 = (first_m + in % gsz) * bm;
         n0 = (in / gsz) * OBN;
     }
     // diagonals [d0, d1) of pass p and the digits they need
@@ -96,7 +97,25 @@ struct OzMap {
 // field per 16 bytes, tiles of A_TILE / B_TILE bytes), so issuing an MMA costs a few integer adds.  An
 // int8 MMA of 128 x 128 x 32 lasts ~64 tensor cycles; rebuilding descriptors per MMA had the single
 // issuing thread, not the tensor pipe, set the pace.
-template <int S, int D0, int D1>
+// CTA-pair form of the int8 MMA (cta_group::2, M = 256 over the pair, N = 128): issued by CTA 0,
+// A rows from each CTA's own shared memory, the two 64-row halves of B from the two CTAs
+constexpr uint32_t IDESC_I8_PAIR = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OBN >> 3) << 17) |
+                                   ((uint32_t)(256 >> 4) << 24);
+
+template <bool PAIR>
+__device__ __forceinline__ void mma_i8_any(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    if constexpr (PAIR) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(IDESC_I8_PAIR), "r"(accumulate));
+    } else {
+        mma_i8(d_tmem, adesc, bdesc, accumulate);
+    }
+}
+
+template <int S, int D0, int D1, bool PAIR, int BT>
 __device__ __forceinline__ void issue_kblock(uint32_t tmem, uint64_t a0, uint64_t b0, bool first_kb) {
 #pragma unroll
     for (int kk = 0; kk < OBK / 32; kk++) {
@@ -106,19 +125,22 @@ __device__ __forceinline__ void issue_kblock(uint32_t tmem, uint64_t a0, uint64_
             for (int t = (d - S + 1 > 0 ? d - S + 1 : 0); t <= (d < S - 1 ? d : S - 1); t++) {
                 const int u = d - t;
                 const bool first = kk == 0 && t == (d - S + 1 > 0 ? d - S + 1 : 0);
-                mma_i8(tmem + (uint32_t)((d - D0) * OBN),
-                       a0 + (uint64_t)(t * (A_TILE >> 4) + kk * 2),
-                       b0 + (uint64_t)(u * (B_TILE >> 4) + kk * 2), (first_kb && first) ? 0u : 1u);
+                mma_i8_any<PAIR>(tmem + (uint32_t)((d - D0) * OBN),
+                                 a0 + (uint64_t)(t * (A_TILE >> 4) + kk * 2),
+                                 b0 + (uint64_t)(u * (BT >> 4) + kk * 2), (first_kb && first) ? 0u : 1u);
             }
         }
     }
 }
 
-template <int S>
+// BT: bytes of one digit tile of B in shared memory (128 rows, or the 64 of one CTA of a pair)
+template <int S, bool PAIR = false, int BT = B_TILE>
 __device__ __forceinline__ void issue_pass(int p, uint32_t tmem, const uint8_t *st, bool first_kb) {
     const uint64_t a0 = smem_desc_k<64>(st, 0), b0 = smem_desc_k<64>(st + SLOTS * A_TILE, 0);
-    if (p == 0) issue_kblock<S, 0, (S < MAX_DIAG_PER_PASS ? S : MAX_DIAG_PER_PASS)>(tmem, a0, b0, first_kb);
-    else if constexpr (S > MAX_DIAG_PER_PASS) issue_kblock<S, MAX_DIAG_PER_PASS, S>(tmem, a0, b0, first_kb);
+    if (p == 0)
+        issue_kblock<S, 0, (S < MAX_DIAG_PER_PASS ? S : MAX_DIAG_PER_PASS), PAIR, BT>(tmem, a0, b0, first_kb);
+    else if constexpr (S > MAX_DIAG_PER_PASS)
+        issue_kblock<S, MAX_DIAG_PER_PASS, S, PAIR, BT>(tmem, a0, b0, first_kb);
 }
 
 template <int S>
@@ -296,6 +318,194 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     }
 }
 
+// The digit GEMM on a pair of CTAs (a cluster of two): one cta_group::2 MMA of M = 256 (each CTA's
+// 128 rows of A) and N = 128 (64 rows of B staged by each CTA).  A 128 x 128 x 32 int8 MMA reads
+// 8 KB of operands per 64 tensor cycles, all a single SM's shared memory delivers beside the TMA
+// writes; in the pair each SM's shared memory serves its A rows and half of B, 6 KB.  CTA 0 issues
+// the MMAs and waits for both CTAs' loads on its own barriers; its commits arrive on both CTAs.
+constexpr int BP_TILE = (OBN / 2) * OBK;                         // one CTA's half of a B digit tile
+constexpr int OPSTAGE_BYTES = SLOTS * (A_TILE + BP_TILE);
+constexpr int OPSMEM = OSTAGES * OPSTAGE_BYTES + 1024 + 256;
+
+template <int S>
+__global__ void __launch_bounds__(OTHREADS, 1)
+ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzMap map,
+                  int num_tiles) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + OSTAGES * OPSTAGE_BYTES);
+    uint64_t *empty = full + OSTAGES;
+    uint64_t *acc_full = empty + OSTAGES;
+    uint64_t *acc_empty = acc_full + 1;   // used on CTA 0
+    uint64_t *done = acc_empty + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool lead = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < OSTAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, 2 * (OEPI / 32));   // one arrival per epilogue warp of each CTA
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(OTMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    cluster_sync();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int g = 0;
+            int issued[OSTAGES] = {};
+            for (int t = pair; t < num_tiles && !*abort_flag; t += npairs) {
+                int m0, n0;
+                map.tile(t, m0, n0);
+                for (int c = 0; c < map.nchunks && !*abort_flag; c++) {
+                    const int kb0 = c * map.kc, kb1 = min(map.nk_all, kb0 + map.kc);
+                    for (int p = 0; p < map.npass && !*abort_flag; p++) {
+                        int d0, d1, nd;
+                        map.pass(p, d0, d1, nd);
+                        for (int kb = kb0; kb < kb1; kb++, g++) {
+                            const int s = g % OSTAGES;
+                            if (!mbar_wait(&empty[s], ((g / OSTAGES) & 1) ^ 1, map.wait_cycles) || *abort_flag) {
+                                record_error(map.err, ERR_PRODUCER);
+                                *abort_flag = 1;
+                                break;
+                            }
+                            issued[s]++;
+                            uint8_t *st = smem + s * OPSTAGE_BYTES;
+                            if (lead) mbar_expect_tx(&full[s], 2u * (uint32_t)nd * (A_TILE + BP_TILE));
+                            for (int q = 0; q < nd; q++) {
+                                tma_load_3d_pair(&tmA, &full[s], st + q * A_TILE, kb * OBK, m0 + OBM * (int)rank, q);
+                                tma_load_3d_pair(&tmB, &full[s], st + SLOTS * A_TILE + q * BP_TILE, kb * OBK,
+                                                 n0 + (OBN / 2) * (int)rank, q);
+                            }
+                        }
+                    }
+                }
+            }
+            if (lead)
+                for (int s = 0; s < OSTAGES; s++)
+                    if (issued[s] && !mbar_wait(&full[s], (issued[s] - 1) & 1, map.wait_cycles))
+                        record_error(map.err, ERR_DRAIN);
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && lead) {
+            int g = 0, uc = 0;
+            for (int t = pair; t < num_tiles && !*abort_flag; t += npairs) {
+                for (int c = 0; c < map.nchunks && !*abort_flag; c++) {
+                    const int kb0 = c * map.kc, kb1 = min(map.nk_all, kb0 + map.kc);
+                    for (int p = 0; p < map.npass && !*abort_flag; p++, uc++) {
+                        if (!mbar_wait(acc_empty, (uc & 1) ^ 1, map.wait_cycles)) {
+                            record_error(map.err, ERR_MMA_ACC);
+                            *abort_flag = 1;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        for (int kb = kb0; kb < kb1; kb++, g++) {
+                            const int s = g % OSTAGES;
+                            if (!mbar_wait(&full[s], (g / OSTAGES) & 1, map.wait_cycles) || *abort_flag) {
+                                record_error(map.err, ERR_MMA_FULL);
+                                *abort_flag = 1;
+                                break;
+                            }
+                            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                            issue_pass<S, true, BP_TILE>(p, tmem, smem + s * OPSTAGE_BYTES, kb == kb0);
+                            mma_commit_pair(&empty[s]);
+                        }
+                        mma_commit_pair(acc_full);
+                    }
+                }
+            }
+            mma_commit_pair(done);
+        }
+    } else {
+        // epilogue: this CTA's 128 rows; warp w drains TMEM lanes 32 (w % 4) .. +31
+        const int quarter = warp & 3;
+        int uc = 0;
+        bool aborted = false;
+        for (int t = pair; t < num_tiles && !aborted; t += npairs) {
+            int m0, n0;
+            map.tile(t, m0, n0);
+            const int row = m0 + OBM * (int)rank + quarter * 32 + lane;
+            const double row_scale = row < map.M ? map.alpha * exp2((double)map.ea[row]) : 0.0;
+            for (int c = 0; c < map.nchunks && !aborted; c++) {
+                for (int p = 0; p < map.npass; p++, uc++) {
+                    int d0, d1, nd;
+                    map.pass(p, d0, d1, nd);
+                    bool ok = !*abort_flag && mbar_wait(acc_full, uc & 1, map.wait_cycles);
+                    __syncwarp();
+                    if (!ok || *abort_flag) {
+                        record_error(map.err, ERR_EPILOGUE);
+                        *abort_flag = 1;
+                        aborted = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const bool first = (c == 0 && p == 0);
+                    const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll 1
+                    for (int cc = 0; cc < OBN; cc += 16) {
+                        double v[16];
+#pragma unroll
+                        for (int j = 0; j < 16; j++) v[j] = 0.0;
+                        for (int d = d0; d < d1; d++) {
+                            uint32_t r[16];
+                            tmem_ld16u(base + (uint32_t)((d - d0) * OBN + cc), r);
+                            const double w = exp2(-7.0 * (double)(d + 2));
+#pragma unroll
+                            for (int j = 0; j < 16; j++) v[j] += w * (double)(int)r[j];
+                        }
+                        if (row < map.M) {
+                            double *out = map.C + (long long)(n0 + cc) * map.ldc + row;
+                            double old[16];
+#pragma unroll
+                            for (int j = 0; j < 16; j++) {
+                                const bool in = n0 + cc + j < map.N;
+                                old[j] = (in && (!first || map.beta != 0.0)) ? __ldcg(out + (long long)j * map.ldc) : 0.0;
+                            }
+#pragma unroll
+                            for (int j = 0; j < 16; j++) {
+                                const int col = n0 + cc + j;
+                                if (col < map.N) {
+                                    const double x = row_scale * exp2((double)map.eb[col]) * v[j];
+                                    out[(long long)j * map.ldc] = first ? x + map.beta * old[j] : x + old[j];
+                                }
+                            }
+                        }
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) arrive_cta0(acc_empty);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (!mbar_wait(done, 0, map.wait_cycles)) record_error(map.err, ERR_DONE);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    cluster_sync();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(OTMEM_COLS));
+    }
+}
+
 // Row exponents of a strided FP64 view (element (r, k) at src[r sr + k sk]): e[r] = the exponent of
 // the power of two just above max_k |x_rk| (frexp), by atomicMax over K slices of 32 x 32 tiles
 // (e must start below any exponent: all-zero rows keep the start value).
@@ -434,14 +644,15 @@ __global__ void oz_digits_kfast_kernel(const double *__restrict__ src, long long
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
-// digits x rows x Kp tensor of int8, box (64, 128, 1), 64-byte swizzle
-CUtensorMap make_i8_map(void *base, int64_t rows, int64_t Kp, int64_t plane_stride, int planes) {
+// digits x rows x Kp tensor of int8, box (64, box_rows, 1), 64-byte swizzle; rows beyond `rows` read
+// as zero
+CUtensorMap make_i8_map(void *base, int64_t rows, int64_t Kp, int64_t plane_stride, int planes, int box_rows = 128) {
     CUtensorMap m;
     REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, CCSD_GPU_EINVAL, "tensor map base must be 16-byte aligned");
     REQUIRE(Kp % 64 == 0 && plane_stride % 16 == 0, CCSD_GPU_EINVAL, "int8 digit planes: bad padding");
     cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)planes};
     cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)plane_stride};
-    cuuint32_t box[3] = {OBK, 128, 1};
+    cuuint32_t box[3] = {OBK, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
@@ -535,16 +746,54 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     auto kernel = digits == 7 ? ozaki_gemm_kernel<7> : digits == 6 ? ozaki_gemm_kernel<6>
                 : digits == 5 ? ozaki_gemm_kernel<5> : digits == 4 ? ozaki_gemm_kernel<4>
                 : digits == 3 ? ozaki_gemm_kernel<3> : ozaki_gemm_kernel<2>;
+    auto pkernel = digits == 7 ? ozaki_pair_kernel<7> : digits == 6 ? ozaki_pair_kernel<6>
+                 : digits == 5 ? ozaki_pair_kernel<5> : digits == 4 ? ozaki_pair_kernel<4>
+                 : digits == 3 ? ozaki_pair_kernel<3> : ozaki_pair_kernel<2>;
+    // CTA pairs where 256-row pair tiles pad op(A) no further than 128-row tiles do (10240^3 with 6
+    // digits: 18.47 against 18.72 ms; a 528-row operand would run a third of its pair rows empty);
+    // CCSD_GPU_PAIR_DIGITS=0 keeps single CTAs
+    static const bool pairs_on = [] {
+        const char *e = std::getenv("CCSD_GPU_PAIR_DIGITS");
+        return !(e && e[0] == '0');
+    }();
+    const bool pair = pairs_on && m >= 2 * OBM && round_up(m, (int64_t)(2 * OBM)) == Mp;
     CU_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OSMEM));
+    CU_CHECK(cudaFuncSetAttribute(pkernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OPSMEM));
     const int nsm = num_sms();
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(OTHREADS);
+    cfg.dynamicSmemBytes = OPSMEM;
+    cfg.stream = ex.stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int max_pairs = 1;
+    if (pair) {
+        static int cached[128] = {};
+        int dev = 0;
+        CU_CHECK(cudaGetDevice(&dev));
+        int &mp = cached[dev & 127];
+        if (mp == 0) {
+            cfg.gridDim = dim3((unsigned)(2 * (nsm / 2)));
+            int n = 0;
+            CU_CHECK(cudaOccupancyMaxActiveClusters(&n, pkernel, &cfg));
+            mp = std::max(1, n);
+        }
+        max_pairs = mp;
+    }
     for (int64_t k0 = 0; k0 < k; k0 += kslab) {
         const int64_t kk = std::min(kslab, k - k0), Kp = round_up(kk, OBK);
         slab_digits(ex, A + k0 * a_sk, a_sr, a_sk, m, kk, Mp, Kp, digits, ea, da);
         slab_digits(ex, B + k0 * b_sk, b_sr, b_sk, n, kk, Np, Kp, digits, eb, db);
         CUtensorMap ta = make_i8_map(da, Mp, Kp, Mp * Kp, digits);
-        CUtensorMap tb = make_i8_map(db, Np, Kp, Np * Kp, digits);
+        CUtensorMap tb = make_i8_map(db, Np, Kp, Np * Kp, digits, pair ? OBN / 2 : OBN);
         OzMap map{};
-        map.num_mt = (int)(Mp / OBM);
+        map.bm = pair ? 2 * OBM : OBM;
+        map.num_mt = (int)(pair ? round_up(Mp, (int64_t)(2 * OBM)) / (2 * OBM) : Mp / OBM);
         map.num_nt = (int)(Np / OBN);
         map.group_m = std::min(map.num_mt, 16);
         map.nk_all = (int)(Kp / OBK);
@@ -563,16 +812,21 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
         map.err = ex.gemm_err;
         map.wait_cycles = ex.wait_cycles > 0 ? ex.wait_cycles : OWAIT_CYCLES;
         const int num_tiles = map.num_mt * map.num_nt;
-        const int grid = std::min(num_tiles, nsm);
+        const int grid = std::min(num_tiles, pair ? max_pairs : nsm);
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ex.prof && ex.prof->on) {
             CU_CHECK(cudaEventCreate(&e0));
             CU_CHECK(cudaEventCreate(&e1));
             CU_CHECK(cudaEventRecord(e0, ex.stream));
         }
-        kernel<<<grid, OTHREADS, OSMEM, ex.stream>>>(ta, tb, map, num_tiles);
+        if (pair) {
+            cfg.gridDim = dim3((unsigned)(2 * grid));
+            CU_CHECK(cudaLaunchKernelEx(&cfg, pkernel, ta, tb, map, num_tiles));
+        } else {
+            kernel<<<grid, OTHREADS, OSMEM, ex.stream>>>(ta, tb, map, num_tiles);
+            CU_CHECK(cudaGetLastError());
+        }
         ex.launches++;
-        CU_CHECK(cudaGetLastError());
         if (e0) {
             CU_CHECK(cudaEventRecord(e1, ex.stream));
             ex.prof->oz_events.emplace_back(e0, e1);

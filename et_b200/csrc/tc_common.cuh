@@ -1,6 +1,7 @@
 // Device helpers shared by the tcgen05 GEMM kernels of libccsd_gpu (sm_100a): shared-memory
 // addresses, mbarriers with bounded waits, TMA tile loads, UMMA shared-memory descriptors,
-// tcgen05 commit and TMEM loads, and the driver entry point that encodes TMA tensor maps.
+// tcgen05 commit and TMEM loads, the CTA-pair (cta_group::2) forms of loads, commits and arrivals,
+// and the driver entry point that encodes TMA tensor maps.
 #pragma once
 
 #include <cuda.h>
@@ -113,6 +114,41 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// ---- CTA pairs (a cluster of two CTAs sharing cta_group::2 MMAs) ----
+constexpr uint32_t PEER_BIT_CLEAR = 0xFEFFFFFFu;   // shared::cluster address of the same offset in CTA 0
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// tile load into this CTA's shared memory whose bytes complete on CTA 0's barrier
+__device__ __forceinline__ void tma_load_3d_pair(const CUtensorMap *map, uint64_t *bar, void *dst, int c0, int c1,
+                                                 int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+        "%5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar) & PEER_BIT_CLEAR), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+// arrives on the barrier at this offset in both CTAs once the pair's MMAs issued so far complete
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"((uint16_t)3)
+        : "memory");
+}
+
+__device__ __forceinline__ void arrive_cta0(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(smem_u32(bar) & PEER_BIT_CLEAR) : "memory");
+}
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
