@@ -110,7 +110,7 @@ Context::~Context() {
     for (auto &G : rgraph) G.reset();
     if (ex.stream) cudaStreamSynchronize(ex.stream);
     if (graphs_captured) cudaDeviceGraphMemTrim(device);   // the physical memory the residual graphs held
-    for (DBuf *b : {&gov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
+    for (DBuf *b : {&gov, &hov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
                     &mbuf, &ybuf, &om_stage, &f64_gp, &f64_gm, &f64_ovvv, &hb_oo, &hb_ov, &hb_vo, &hb_vv,
                     &gemm_err, &digit_arena, &fb_oo, &fb_ov, &fb_vo, &fb_vv})
         b->release();
@@ -255,9 +255,27 @@ const double *Context::g_ovov_const() {
         gov = g_ovov();
         ex.prec = keep;
         have_gov = true;
+        gov_id++;
         cache_epoch++;
     }
     return gov.d();
+}
+
+// H_lckd = g_lckd - 1/2 g_kcld, the combination of g_ovov that the two u terms of omega_ccsd_d2
+// contract with (one product instead of two), kept beside g_ovov
+const double *Context::h_ovov_const() {
+    const double *g = g_ovov_const();
+    if (!hov || hov_id != gov_id) {
+        if (!hov) hov = dalloc(nov * nov, ex.stream);
+        const TV H = tv(hov.d(), {no, nv, no, nv});
+        permute_add(ex, 1.0, tv(g, {no, nv, no, nv}), 0.0, H);
+        TV gt = tv(g, {no, nv, no, nv});   // gt[l, c, k, d] = g[k, c, l, d]
+        std::swap(gt.s[0], gt.s[2]);
+        permute_add(ex, -0.5, gt, 1.0, H);
+        hov_id = gov_id;
+        cache_epoch++;
+    }
+    return hov.d();
 }
 
 // calculate_energy_ccsd (src/wavefunctions/ccsd/mean_value_ccsd.F90:36-99), FP64
@@ -697,24 +715,21 @@ void Context::ladder_residual_mixed(const double *t1, const double *tf, const do
 
 void Context::ladder_t1_corrections(const double *t1, const double *tf, const double *Y0, double *om2) {
     cudaStream_t s = ex.stream;
-    DBuf S = dalloc(nov * nov, s), A = dalloc(nov * nov, s);
+    // the terms below are A_aibj (not symmetric); omega gets pack(A + A^T) with the diagonal halved
+    DBuf A = dalloc(nov * nov, s);
     contract(ex, "ak,kibj->aibj", -1.0, tv(t1, {nv, no}), tv(Y0, {no, no, nv, no}), 0.0,
              tv(A.d(), {nv, no, nv, no}));
-    permute_add(ex, 1.0, tv(A.d(), {nv, no, nv, no}), 0.0, tv(S.d(), {nv, no, nv, no}));
-    TV At = tv(A.d(), {nv, no, nv, no});
-    std::swap(At.s[0], At.s[2]);
-    std::swap(At.s[1], At.s[3]);
-    permute_add(ex, 1.0, At, 1.0, tv(S.d(), {nv, no, nv, no}));
     {
         DBuf Q = dalloc(no * no * no * no, s), B = dalloc(nv * no * no * no, s);
         contract(ex, "kcld,cidj->kilj", 1.0, tv(g_ovov_const(), {no, nv, no, nv}), tv(tf, {nv, no, nv, no}), 0.0,
                  tv(Q.d(), {no, no, no, no}));
         contract(ex, "ak,kilj->ailj", 1.0, tv(t1, {nv, no}), tv(Q.d(), {no, no, no, no}), 0.0,
                  tv(B.d(), {nv, no, no, no}));
-        contract(ex, "bl,ailj->aibj", 1.0, tv(t1, {nv, no}), tv(B.d(), {nv, no, no, no}), 1.0,
-                 tv(S.d(), {nv, no, nv, no}));
+        // the symmetric term enters at half weight: pack(A + A^T) adds it twice
+        contract(ex, "bl,ailj->aibj", 0.5, tv(t1, {nv, no}), tv(B.d(), {nv, no, no, no}), 1.0,
+                 tv(A.d(), {nv, no, nv, no}));
     }
-    pack_half_diag_add(ex, 1.0, S.d(), om2, nov);
+    pack_sym_add(ex, A.d(), om2, nov);
 }
 
 // FP64 integrals of the untransformed vectors, resident while they fit in half of the free memory

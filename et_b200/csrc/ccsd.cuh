@@ -59,6 +59,9 @@ struct Context {
     size_t mbuf_bytes = 0;
     DBuf gov;                  // g_iajb cache (g_ovov_const)
     bool have_gov = false;
+    int64_t gov_id = 0;        // bumped whenever gov is formed again
+    DBuf hov;                  // g_lckd - 1/2 g_kcld (h_ovov_const), formed from gov number hov_id
+    int64_t hov_id = -1;
     int64_t l_version = 0;     // bumped whenever the Cholesky vectors change
     // what mbuf holds: 0 nothing, 1 untransformed L_vv pairs (valid for mbuf_version), 2 per call
     int mbuf_kind = 0, mbuf_planes = 0;
@@ -127,6 +130,7 @@ struct Context {
     // g_iajb = sum_J L_ia L_jb in FP64, kept until the Cholesky vectors change: the ov block is
     // unchanged by the T1 transformation, so every iteration shares it
     const double *g_ovov_const();
+    const double *h_ovov_const();
     double energy();
     void mp2_guess();
     void omega(double *d_omega);

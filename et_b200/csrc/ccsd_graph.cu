@@ -187,11 +187,13 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov, bool const_t1) {
         TermTimer tt(ex, "omega ccsd e2");
         const int Xbc = g.zeros("X_bc", {nv, nv}), Ykj = g.zeros("Y_kj", {no, no});
         g.contract(Xbc, "bkdl,ldkc->bc", -1.0, u, G4);
-        g.contract(om, "bc,cjai->bjai", 1.0, Xbc, tf);
         g.contract(Ykj, "kdlc,djcl->kj", 1.0, G4, u);
-        g.contract(om, "aibk,kj->aibj", -1.0, tf, Ykj);
-        g.contract(om, "bc,cjai->bjai", 1.0, F_vv, tf, true);
-        g.contract(om, "aibk,kj->aibj", -1.0, tf, F_oo, true);
+        // the Fock blocks join X and Y, so each side is one FP64 product with t (the Fock parts are
+        // first-order terms)
+        g.permute(Xbc, "bc->bc", 1.0, F_vv);
+        g.permute(Ykj, "kj->kj", 1.0, F_oo);
+        g.contract(om, "bc,cjai->bjai", 1.0, Xbc, tf, true);
+        g.contract(om, "aibk,kj->aibj", -1.0, tf, Ykj, true);
     }
     // om collects the terms that eT symmetrises (symmetric_sum, reordering.F90:416): the doubles
     // residual is pack(om + om^T) with the diagonal halved, formed in one pass at the end.  Terms
@@ -214,9 +216,14 @@ OmegaNodes Context::record_omega(Graph &g, bool const_ovov, bool const_t1) {
         g.contract(D, "Jai,Jkc->ckai", 2.0, Lt_vo, Lt_ov);
         g.contract(C, "kcld,djak->claj", -0.5, G4, tf);
         // the two g_ovov terms of D share u: one contraction with H_lckd = g_lckd - 1/2 g_kcld
-        const int H = g.zeros("H_lckd", {no, nv, no, nv});
-        g.permute(H, "lckd->lckd", 1.0, G4);
-        g.permute(H, "kcld->lckd", -0.5, G4);
+        int H;
+        if (const_ovov) {
+            H = g.input("H_lckd", {no, nv, no, nv}, h_ovov_const());
+        } else {
+            H = g.zeros("H_lckd", {no, nv, no, nv});
+            g.permute(H, "lckd->lckd", 1.0, G4);
+            g.permute(H, "kcld->lckd", -0.5, G4);
+        }
         g.contract(D, "lckd,dkaj->claj", 1.0, H, u);
         const int x = g.zeros("x_c2", V4);
         g.contract(x, "akci,ckbj->aibj", -1.5, tf, C);
@@ -297,16 +304,11 @@ void Context::record_ladder(Graph &g, int om2, int Lvv, int t2, int t1, int L_vv
             // d L~_ac = -sum_k c_ak L_kc: term -P(sum_k c_ak Y_kibj + (ai <-> bj))
             const double *Y = getY();
             const double *c1 = g.tangent(t1, nvec);
-            DBuf A = dalloc(nov * nov, ex.stream), S = dalloc(nov * nov, ex.stream);
+            DBuf A = dalloc(nov * nov, ex.stream);
             for (int n = 0; n < nvec; n++) {
                 contract(ex, "ak,kibj->aibj", -1.0, tv(c1 + n * nt1, {nv, no}), tv(Y, {no, no, nv, no}), 0.0,
                          tv(A.d(), {nv, no, nv, no}));
-                permute_add(ex, 1.0, tv(A.d(), {nv, no, nv, no}), 0.0, tv(S.d(), {nv, no, nv, no}));
-                TV At = tv(A.d(), {nv, no, nv, no});
-                std::swap(At.s[0], At.s[2]);
-                std::swap(At.s[1], At.s[3]);
-                permute_add(ex, 1.0, At, 1.0, tv(S.d(), {nv, no, nv, no}));
-                pack_half_diag_add(ex, 1.0, S.d(), out + n * nt2, nov);
+                pack_sym_add(ex, A.d(), out + n * nt2, nov);   // pack(A + A^T), diagonal halved
             }
         }
     };

@@ -80,14 +80,16 @@ __global__ void pack_sym_batch_kernel(const double *__restrict__ full, double *_
     }
 }
 
+// full (+)= the symmetric square of packed (accumulate = 0: overwrite)
 __global__ void squareup_batch_kernel(const double *__restrict__ packed, double *__restrict__ full, int64_t nov,
-                                      int64_t nbatch) {
+                                      int64_t nbatch, int accumulate) {
     const int64_t nf = nov * nov, np = nov * (nov + 1) / 2;
     GRID_STRIDE(idx, nf * nbatch) {
         int64_t n = idx / nf, r = idx - n * nf;
         int64_t x = r % nov, y = r / nov;
         int64_t M = x > y ? x : y, m = x > y ? y : x;
-        full[idx] += packed[n * np + M * (M + 1) / 2 + m];
+        const double v = packed[n * np + M * (M + 1) / 2 + m];
+        full[idx] = accumulate ? full[idx] + v : v;
     }
 }
 
@@ -148,9 +150,16 @@ int Graph::zeros(const std::string &name, std::vector<int64_t> dims) {
     for (int64_t d : n.dims) n.size *= d;
     n.own = dalloc(n.size, ex_.stream);
     n.v = n.own.d();
-    fill(ex_, n.v, n.size, 0.0);
+    n.zero = true;
     nodes_.push_back(std::move(n));
     return (int)nodes_.size() - 1;
+}
+
+void Graph::materialize(int i) {
+    GNode &n = nodes_[i];
+    if (!n.zero) return;
+    fill(ex_, n.v, n.size, 0.0);
+    n.zero = false;
 }
 
 int Graph::alias(int node) { return node; }
@@ -198,9 +207,20 @@ double *Graph::adjoint(int i, int nvec) {
 
 void Graph::run_forward(const GOp &op) {
     Fp64Scope fp64(ex_, op.fp64);
+    // inputs never written read as zero; an output never written is overwritten (beta = 0) by the
+    // ops that write every element of it, and zero-filled first for the others
+    if (op.a >= 0) materialize(op.a);
+    if (op.b >= 0) materialize(op.b);
+    if (op.kind == OpKind::Custom)
+        for (int i : custom_ins_[op.custom]) materialize(i);
+    const bool fresh = nodes_[op.out].zero &&
+                       (op.kind == OpKind::Contract || op.kind == OpKind::Permute || op.kind == OpKind::Squareup);
+    if (fresh) nodes_[op.out].zero = false;
+    else materialize(op.out);
+    const double beta = fresh ? 0.0 : 1.0;
     switch (op.kind) {
     case OpKind::Contract:
-        ccsd::contract(ex_, op.spec.c_str(), op.alpha, view(op.a), view(op.b), 1.0, view(op.out));
+        ccsd::contract(ex_, op.spec.c_str(), op.alpha, view(op.a), view(op.b), beta, view(op.out));
         break;
     case OpKind::Permute: {
         std::string s = op.spec;
@@ -215,12 +235,12 @@ void Graph::run_forward(const GOp &op) {
             pin.n[k] = in.n[pos];
             pin.s[k] = in.s[pos];
         }
-        permute_add(ex_, op.alpha, pin, 1.0, out);
+        permute_add(ex_, op.alpha, pin, beta, out);
         break;
     }
     case OpKind::Squareup:
         squareup_batch_kernel<<<grid_for(nov * nov, 256), 256, 0, ex_.stream>>>(nodes_[op.a].v, nodes_[op.out].v, nov,
-                                                                                1);
+                                                                                1, fresh ? 0 : 1);
         ex_.launches++;
         break;
     case OpKind::PackHalf:
@@ -393,7 +413,7 @@ void Graph::jvp(const std::vector<int> &inputs, const std::vector<const double *
         case OpKind::Squareup:
             if (!nodes_[op.a].active) break;
             squareup_batch_kernel<<<grid_for(nov * nov * nvec, 256), 256, 0, ex_.stream>>>(
-                tangent(op.a, nvec), tangent(op.out, nvec), nov, nvec);
+                tangent(op.a, nvec), tangent(op.out, nvec), nov, nvec, 1);
             ex_.launches++;
             break;
         case OpKind::PackHalf:
@@ -493,7 +513,7 @@ void Graph::vjp(const std::vector<int> &outputs, const std::vector<const double 
             // equal entries): the adjoint is the full symmetric square-up of the packed adjoint
             if (!nodes_[op.a].active) break;
             squareup_batch_kernel<<<grid_for(nov * nov * nvec, 256), 256, 0, ex_.stream>>>(
-                adjoint(op.out, nvec), adjoint(op.a, nvec), nov, nvec);
+                adjoint(op.out, nvec), adjoint(op.a, nvec), nov, nvec, 1);
             ex_.launches++;
             break;
         case OpKind::Trace: {
@@ -518,6 +538,12 @@ void Graph::vjp(const std::vector<int> &outputs, const std::vector<const double 
         else
             fill(ex_, results[k], n.size * nvec, 0.0);
     }
+}
+
+void pack_sym_add(Exec &ex, const double *full, double *packed, int64_t nov) {
+    pack_sym_batch_kernel<<<grid_for(nov * (nov + 1) / 2, 256), 256, 0, ex.stream>>>(full, packed, nov, 1);
+    ex.launches++;
+    CU_CHECK(cudaGetLastError());
 }
 
 }  // namespace ccsd

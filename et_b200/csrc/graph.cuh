@@ -21,6 +21,8 @@ struct GNode {
     DBuf own;                    // storage when the graph owns the primal
     DBuf tan, adj;               // [size x nvec]
     bool active = false;         // depends on a differentiated input
+    bool zero = false;           // allocated by zeros() and not written yet: reads as zero, and the
+                                 // first op writing it overwrites instead of accumulating
     int last_use = -1;           // index of the last op reading this node
 };
 
@@ -41,6 +43,10 @@ struct GOp {
     bool fp64 = false;           // force FP64 (first-order terms)
     int custom = -1;
 };
+
+// packed[(M, m)] += (full[M, m] + full[m, M]) * (1/2 if M == m) over M >= m: the symmetrised full
+// doubles array packed as eT's symmetric_sum + scale_diagonal(1/2) + packin do, in one pass
+void pack_sym_add(Exec &ex, const double *full, double *packed, int64_t nov);
 
 class Graph {
   public:
@@ -69,8 +75,14 @@ class Graph {
     // custom op over existing nodes
     int custom(CustomOp op, int out, std::vector<int> ins);
 
-    GNode &node(int i) { return nodes_[i]; }
-    const double *value(int i) const { return nodes_[i].v; }
+    GNode &node(int i) {
+        materialize(i);
+        return nodes_[i];
+    }
+    const double *value(int i) {
+        materialize(i);
+        return nodes_[i].v;
+    }
     int64_t nov = 0;               // for squareup / pack_half
 
     // derivative passes; seeds are [size x nvec] device arrays for the listed nodes.  Each pass
@@ -97,6 +109,8 @@ class Graph {
     std::vector<std::vector<int>> custom_ins_;
     void run_forward(const GOp &op);
     TV view(int node) const;
+    // fills a node that zeros() allocated and nothing has written yet
+    void materialize(int node);
     TV tview(int node, int nvec, bool adjoint);
 };
 
