@@ -133,10 +133,11 @@ __device__ __forceinline__ void issue_kblock(uint32_t tmem, uint64_t a0, uint64_
     }
 }
 
-// BT: bytes of one digit tile of B in shared memory (128 rows, or the 64 of one CTA of a pair)
-template <int S, bool PAIR = false, int BT = B_TILE>
+// BT: bytes of one digit tile of B in shared memory (128 rows, or the 64 of one CTA of a pair);
+// BOFF: offset of the B digit tiles in a stage (after the A digit tiles)
+template <int S, bool PAIR = false, int BT = B_TILE, int BOFF = SLOTS * A_TILE>
 __device__ __forceinline__ void issue_pass(int p, uint32_t tmem, const uint8_t *st, bool first_kb) {
-    const uint64_t a0 = smem_desc_k<64>(st, 0), b0 = smem_desc_k<64>(st + SLOTS * A_TILE, 0);
+    const uint64_t a0 = smem_desc_k<64>(st, 0), b0 = smem_desc_k<64>(st + BOFF, 0);
     if (p == 0)
         issue_kblock<S, 0, (S < MAX_DIAG_PER_PASS ? S : MAX_DIAG_PER_PASS), PAIR, BT>(tmem, a0, b0, first_kb);
     else if constexpr (S > MAX_DIAG_PER_PASS)
@@ -324,18 +325,28 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
 // writes; in the pair each SM's shared memory serves its A rows and half of B, 6 KB.  CTA 0 issues
 // the MMAs and waits for both CTAs' loads on its own barriers; its commits arrive on both CTAs.
 constexpr int BP_TILE = (OBN / 2) * OBK;                         // one CTA's half of a B digit tile
-constexpr int OPSTAGE_BYTES = SLOTS * (A_TILE + BP_TILE);
-constexpr int OPSMEM = OSTAGES * OPSTAGE_BYTES + 1024 + 256;
+
+// stages of S-digit operands: S digit tiles of A and S half tiles of B per K block; three stages where
+// they fit (up to six digits), which keeps the next two K blocks' loads in flight behind the MMAs
+template <int S>
+struct PairLayout {
+    static constexpr int STAGE = S * (A_TILE + BP_TILE);
+    static constexpr int STAGES = 3 * STAGE + 1024 + 256 <= 232448 ? 3 : 2;
+    static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+};
+static_assert(PairLayout<6>::STAGES == 3 && PairLayout<7>::STAGES == 2, "pair stages");
 
 template <int S>
 __global__ void __launch_bounds__(OTHREADS, 1)
 ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzMap map,
                   int num_tiles) {
+    using PL = PairLayout<S>;
+    constexpr int NST = PL::STAGES, STAGE = PL::STAGE, BOFF = S * A_TILE;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + OSTAGES * OPSTAGE_BYTES);
-    uint64_t *empty = full + OSTAGES;
-    uint64_t *acc_full = empty + OSTAGES;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + NST * STAGE);
+    uint64_t *empty = full + NST;
+    uint64_t *acc_full = empty + NST;
     uint64_t *acc_empty = acc_full + 1;   // used on CTA 0
     uint64_t *done = acc_empty + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
@@ -346,7 +357,7 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < OSTAGES; s++) {
+        for (int s = 0; s < NST; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -371,7 +382,7 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     if (warp == 0) {
         if (lane == 0) {
             int g = 0;
-            int issued[OSTAGES] = {};
+            int issued[NST] = {};
             for (int t = pair; t < num_tiles && !*abort_flag; t += npairs) {
                 int m0, n0;
                 map.tile(t, m0, n0);
@@ -381,18 +392,18 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         int d0, d1, nd;
                         map.pass(p, d0, d1, nd);
                         for (int kb = kb0; kb < kb1; kb++, g++) {
-                            const int s = g % OSTAGES;
-                            if (!mbar_wait(&empty[s], ((g / OSTAGES) & 1) ^ 1, map.wait_cycles) || *abort_flag) {
+                            const int s = g % NST;
+                            if (!mbar_wait(&empty[s], ((g / NST) & 1) ^ 1, map.wait_cycles) || *abort_flag) {
                                 record_error(map.err, ERR_PRODUCER);
                                 *abort_flag = 1;
                                 break;
                             }
                             issued[s]++;
-                            uint8_t *st = smem + s * OPSTAGE_BYTES;
+                            uint8_t *st = smem + s * STAGE;
                             if (lead) mbar_expect_tx(&full[s], 2u * (uint32_t)nd * (A_TILE + BP_TILE));
                             for (int q = 0; q < nd; q++) {
                                 tma_load_3d_pair(&tmA, &full[s], st + q * A_TILE, kb * OBK, m0 + OBM * (int)rank, q);
-                                tma_load_3d_pair(&tmB, &full[s], st + SLOTS * A_TILE + q * BP_TILE, kb * OBK,
+                                tma_load_3d_pair(&tmB, &full[s], st + BOFF + q * BP_TILE, kb * OBK,
                                                  n0 + (OBN / 2) * (int)rank, q);
                             }
                         }
@@ -400,7 +411,7 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 }
             }
             if (lead)
-                for (int s = 0; s < OSTAGES; s++)
+                for (int s = 0; s < NST; s++)
                     if (issued[s] && !mbar_wait(&full[s], (issued[s] - 1) & 1, map.wait_cycles))
                         record_error(map.err, ERR_DRAIN);
         }
@@ -418,14 +429,14 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         }
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                         for (int kb = kb0; kb < kb1; kb++, g++) {
-                            const int s = g % OSTAGES;
-                            if (!mbar_wait(&full[s], (g / OSTAGES) & 1, map.wait_cycles) || *abort_flag) {
+                            const int s = g % NST;
+                            if (!mbar_wait(&full[s], (g / NST) & 1, map.wait_cycles) || *abort_flag) {
                                 record_error(map.err, ERR_MMA_FULL);
                                 *abort_flag = 1;
                                 break;
                             }
                             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                            issue_pass<S, true, BP_TILE>(p, tmem, smem + s * OPSTAGE_BYTES, kb == kb0);
+                            issue_pass<S, true, BP_TILE, BOFF>(p, tmem, smem + s * STAGE, kb == kb0);
                             mma_commit_pair(&empty[s]);
                         }
                         mma_commit_pair(acc_full);
@@ -758,7 +769,10 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     }();
     const bool pair = pairs_on && m >= 2 * OBM && round_up(m, (int64_t)(2 * OBM)) == Mp;
     CU_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OSMEM));
-    CU_CHECK(cudaFuncSetAttribute(pkernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OPSMEM));
+    const int psmem = digits == 7 ? PairLayout<7>::SMEM : digits == 6 ? PairLayout<6>::SMEM
+                    : digits == 5 ? PairLayout<5>::SMEM : digits == 4 ? PairLayout<4>::SMEM
+                    : digits == 3 ? PairLayout<3>::SMEM : PairLayout<2>::SMEM;
+    CU_CHECK(cudaFuncSetAttribute(pkernel, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
     const int nsm = num_sms();
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -767,7 +781,7 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.blockDim = dim3(OTHREADS);
-    cfg.dynamicSmemBytes = OPSMEM;
+    cfg.dynamicSmemBytes = psmem;
     cfg.stream = ex.stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
