@@ -149,10 +149,14 @@ void Context::t1_transform_cholesky() {
     // vo: L_ai + sum_b L_ab t_bi - sum_j t_aj (L_ji + sum_b L_jb t_bi) (:293-440); the bracket is Lt_oo
     CU_CHECK(cudaMemcpyAsync(Lt_vo.d(), L_vo.d(), sizeof(double) * nJ * nv * no, cudaMemcpyDeviceToDevice, s));
     contract(ex, "Jab,bi->Jai", 1.0, tv(L_vv.d(), {nJ, nv, nv}), T1, 1.0, tv(Lt_vo.d(), {nJ, nv, no}));
-    contract(ex, "aj,Jji->Jai", -1.0, T1, tv(Lt_oo.d(), {nJ, no, no}), 1.0, tv(Lt_vo.d(), {nJ, nv, no}));
-    // vv: L_ab - sum_j t_aj L_jb                                  (:443-499)
+    // - sum_j Lt_oo[J, j, i] t_aj for each i: [J x j] times t1^T, written in place ((J, a) of one i is
+    // one contiguous block of Lt_vo, so no reordered copy of the output is needed)
+    gemm_batched_f64(ex, false, true, nJ, nv, no, -1.0, Lt_oo.d(), nJ, nJ * no, t1, nv, 0, 1.0, Lt_vo.d(), nJ,
+                     nJ * nv, no);
+    // vv: L_ab - sum_j t_aj L_jb                                  (:443-499), per b in place likewise
     CU_CHECK(cudaMemcpyAsync(Lt_vv.d(), L_vv.d(), sizeof(double) * nJ * nv * nv, cudaMemcpyDeviceToDevice, s));
-    contract(ex, "aj,Jjb->Jab", -1.0, T1, tv(L_ov.d(), {nJ, no, nv}), 1.0, tv(Lt_vv.d(), {nJ, nv, nv}));
+    gemm_batched_f64(ex, false, true, nJ, nv, no, -1.0, L_ov.d(), nJ, nJ * no, t1, nv, 0, 1.0, Lt_vv.d(), nJ,
+                     nJ * nv, nv);
 }
 
 // ---------------------------------------------------------------------------

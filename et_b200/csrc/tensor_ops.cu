@@ -293,6 +293,16 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
                               n, k, &alpha, A, lda, B, ldb, &beta, C, ldc));
 }
 
+void gemm_batched_f64(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha,
+                      const double *A, int64_t lda, int64_t strideA, const double *B, int64_t ldb, int64_t strideB,
+                      double beta, double *C, int64_t ldc, int64_t strideC, int64_t batch) {
+    if (m == 0 || n == 0 || batch == 0) return;
+    ex.flops += 2.0 * double(m) * double(n) * double(k) * double(batch);
+    BLAS_CHECK(cublasDgemmStridedBatched_64(ex.blas, transA ? CUBLAS_OP_T : CUBLAS_OP_N,
+                                            transB ? CUBLAS_OP_T : CUBLAS_OP_N, m, n, k, &alpha, A, lda, strideA, B,
+                                            ldb, strideB, &beta, C, ldc, strideC, batch));
+}
+
 // ---------------------------------------------------------------------------
 // contract()
 // ---------------------------------------------------------------------------

@@ -21,6 +21,12 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
           const double *A, int64_t lda, const double *B, int64_t ldb, double beta, double *C,
           int64_t ldc, bool allow_mixed = true);
 
+// C_z = alpha op(A_z) op(B_z) + beta C_z for z < batch, operand z at base + z * stride (FP64
+// DGEMM, strided batch): a product whose output index sits between two batch indices
+void gemm_batched_f64(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha,
+                      const double *A, int64_t lda, int64_t strideA, const double *B, int64_t ldb, int64_t strideB,
+                      double beta, double *C, int64_t ldc, int64_t strideC, int64_t batch);
+
 // packed doubles <-> full symmetric (v,o,v,o)
 void squareup(Exec &ex, const double *packed, double *full, int64_t nov);
 // packed += alpha * full(M,m) * (1/2 if M == m) over M >= m (eT's scale_diagonal(1/2) + packin);
