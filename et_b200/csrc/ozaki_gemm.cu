@@ -809,7 +809,9 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
         map.bm = pair ? 2 * OBM : OBM;
         map.num_mt = (int)(pair ? round_up(Mp, (int64_t)(2 * OBM)) / (2 * OBM) : Mp / OBM);
         map.num_nt = (int)(Np / OBN);
-        map.group_m = std::min(map.num_mt, 16);
+        // raster groups of 2048 rows: their A digit panels (2048 x K x digits bytes) stay in L2 while
+        // the group's N tiles stream past
+        map.group_m = std::min(map.num_mt, pair ? 8 : 16);
         map.nk_all = (int)(Kp / OBK);
         map.kc = OK_CHUNK / OBK;
         map.nchunks = (map.nk_all + map.kc - 1) / map.kc;
