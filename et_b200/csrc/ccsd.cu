@@ -110,6 +110,7 @@ Context::~Context() {
     for (auto &G : rgraph) G.reset();
     if (ex.stream) cudaStreamSynchronize(ex.stream);
     if (graphs_captured) cudaDeviceGraphMemTrim(device);   // the physical memory the residual graphs held
+    for (OzPlanes *p : {&f64_gp_dig, &f64_gm_dig, &f64_ovvv_dig}) p->buf.release();
     for (DBuf *b : {&gov, &hov, &L_oo, &L_ov, &L_vo, &L_vv, &Lt_oo, &Lt_ov, &Lt_vo, &Lt_vv, &h, &eps, &F, &t, &epsdiff, &scal,
                     &mbuf, &ybuf, &om_stage, &f64_gp, &f64_gm, &f64_ovvv, &hb_oo, &hb_ov, &hb_vo, &hb_vv,
                     &gemm_err, &digit_arena, &fb_oo, &fb_ov, &fb_vo, &fb_vv})
@@ -794,25 +795,81 @@ void Context::f64_integrals() {
     cache_epoch++;
 }
 
+int Context::f64_digit_planes(int digits) {
+    if (f64_dig_version == f64_version && f64_dig_digits == digits) return f64_dig_level;
+    const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
+    auto planes = [&](int64_t rows, int64_t k) {
+        return (double)digits * (double)((rows + 127) / 128 * 128) * (double)((k + 63) / 64 * 64);
+    };
+    const double ladder = planes(nvp, nvp) + (nvm > 0 ? planes(nvm, nvm) : 0.0), ovvv = planes(nov, nv * nv);
+    for (OzPlanes *p : {&f64_gp_dig, &f64_gm_dig, &f64_ovvv_dig}) p->buf.release();
+    size_t free_b = 0, total_b = 0;
+    CU_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    const double room = 0.6 * (double)free_b;
+    f64_dig_level = ladder + ovvv <= room ? 2 : ladder <= room ? 1 : 0;
+    if (f64_dig_level >= 1) {
+        ozaki_prepare(ex, true, nvp, nvp, f64_gp.d(), nvp, digits, f64_gp_dig);
+        if (nvm > 0) ozaki_prepare(ex, true, nvm, nvm, f64_gm.d(), nvm, digits, f64_gm_dig);
+    }
+    if (f64_dig_level == 2) ozaki_prepare(ex, false, nov, nv * nv, f64_ovvv.d(), nov, digits, f64_ovvv_dig);
+    f64_dig_version = f64_version;
+    f64_dig_digits = digits;
+    cache_epoch++;
+    return f64_dig_level;
+}
+
 void Context::ladder_residual_f64(const double *t1, const double *tf, const double *t2, double *om2) {
     f64_integrals();
     cudaStream_t s = ex.stream;
     const int64_t nop = no * (no + 1) / 2, nom = no * (no - 1) / 2;
     const int64_t nvp = nv * (nv + 1) / 2, nvm = nv * (nv - 1) / 2;
     const int64_t ldm = std::max<int64_t>(nom, 1);
+    // on the digit GEMM the constant operands come as digit planes kept per Cholesky set (products
+    // big enough for it, as gemm() decides)
+    const int digits = ex.fp64_digits;
+    const bool big = digits > 0 && 2.0 * double(nop) * double(nvp) * double(nvp) >= ex.fp64_digits_min_flops &&
+                     (ex.fp64_digits_min_flops <= 1 || (nop >= 256 && nvp >= 256));
+    const int level = big ? f64_digit_planes(digits) : 0;
     // X0 = sum_cd g_acbd t_cidj of the untransformed integrals, all pairs in two GEMMs
     {
         DBuf tp = dalloc(nop * nvp, s), tm = dalloc(ldm * std::max<int64_t>(nvm, 1), s);
         build_tpm(ex, t2, tp.d(), tm.d(), no, nv, nop, ldm);
         DBuf wp = dalloc(nop * nvp, s), wm = dalloc(ldm * std::max<int64_t>(nvm, 1), s);
-        gemm(ex, false, false, nop, nvp, nvp, 0.5, tp.d(), nop, f64_gp.d(), nvp, 0.0, wp.d(), nop, false);
-        if (nom > 0 && nvm > 0)
-            gemm(ex, false, false, nom, nvm, nvm, 0.5, tm.d(), ldm, f64_gm.d(), nvm, 0.0, wm.d(), ldm, false);
+        if (level >= 1) {
+            ozaki_gemm(ex, false, false, nop, nvp, nvp, 0.5, tp.d(), nop, f64_gp.d(), nvp, 0.0, wp.d(), nop, digits,
+                       nullptr, &f64_gp_dig);
+            if (nom > 0 && nvm > 0)
+                ozaki_gemm(ex, false, false, nom, nvm, nvm, 0.5, tm.d(), ldm, f64_gm.d(), nvm, 0.0, wm.d(), ldm,
+                           digits, nullptr, &f64_gm_dig);
+            ex.flops += 2.0 * (double(nop) * nvp * nvp + double(nom) * nvm * nvm);
+        } else {
+            gemm(ex, false, false, nop, nvp, nvp, 0.5, tp.d(), nop, f64_gp.d(), nvp, 0.0, wp.d(), nop, false);
+            if (nom > 0 && nvm > 0)
+                gemm(ex, false, false, nom, nvm, nvm, 0.5, tm.d(), ldm, f64_gm.d(), nvm, 0.0, wm.d(), ldm, false);
+        }
         add_omega_pm(ex, om2, wp.d(), wm.d(), no, nv, 0, nv, nop, ldm);
     }
     DBuf Y = dalloc(no * no * nv * no, s);
-    contract(ex, "kbcd,cidj->kibj", 1.0, tv(f64_ovvv.d(), {no, nv, nv, nv}), tv(tf, {nv, no, nv, no}), 0.0,
-             tv(Y.d(), {no, no, nv, no}));
+    if (level == 2) {
+        // Y_kibj = sum_cd g_kbcd t_cidj: t as [(c, d), (i, j)], the product [(k, b), (i, j)], then Y
+        DBuf TT = dalloc(nv * nv * no * no, s), W = dalloc(nov * no * no, s);
+        TV tt = tv(TT.d(), {nv, no, nv, no});   // (c, i, d, j) at c + nv d + nv^2 (i + no j)
+        tt.s[1] = nv * nv;
+        tt.s[2] = nv;
+        tt.s[3] = nv * nv * no;
+        permute_add(ex, 1.0, tv(tf, {nv, no, nv, no}), 0.0, tt);
+        ozaki_gemm(ex, false, false, nov, no * no, nv * nv, 1.0, f64_ovvv.d(), nov, TT.d(), nv * nv, 0.0, W.d(), nov,
+                   digits, &f64_ovvv_dig, nullptr);
+        ex.flops += 2.0 * double(nov) * double(no * no) * double(nv * nv);
+        TV w = tv(W.d(), {no, no, nv, no});     // (k, i, b, j) at k + no b + no nv (i + no j)
+        w.s[1] = no * nv;
+        w.s[2] = no;
+        w.s[3] = no * nv * no;
+        permute_add(ex, 1.0, w, 0.0, tv(Y.d(), {no, no, nv, no}));
+    } else {
+        contract(ex, "kbcd,cidj->kibj", 1.0, tv(f64_ovvv.d(), {no, nv, nv, nv}), tv(tf, {nv, no, nv, no}), 0.0,
+                 tv(Y.d(), {no, no, nv, no}));
+    }
     ladder_t1_corrections(t1, tf, Y.d(), om2);
 }
 

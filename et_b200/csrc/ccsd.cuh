@@ -5,6 +5,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "ozaki_gemm.cuh"
 #include "graph.cuh"
 
 namespace ccsd {
@@ -188,6 +189,13 @@ struct Context {
     bool f64_resident();
     void f64_integrals();
     void ladder_residual_f64(const double *t1, const double *tf, const double *t2, double *om2);
+    // digit planes of the resident FP64 integrals for FP64 evaluations on the int8 digit GEMM: the
+    // +/- ladder integrals (B operands) and g_kcbd (A operand of Y), kept per Cholesky set and digit
+    // count while they fit (levels: 2 all three, 1 the ladder pair only, 0 none)
+    int f64_digit_planes(int digits);
+    OzPlanes f64_gp_dig, f64_gm_dig, f64_ovvv_dig;
+    int64_t f64_dig_version = -1;
+    int f64_dig_digits = 0, f64_dig_level = 0;
     int davidson(int nstates, int side, const ccsd_gpu_davidson_options *o, double *omega_out, double *vectors_out,
                  int32_t *iters_out, const double *start = nullptr);
     void eta(double *out);

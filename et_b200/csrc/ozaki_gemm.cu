@@ -657,12 +657,15 @@ inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
 // digits x rows x Kp tensor of int8, box (64, box_rows, 1), 64-byte swizzle; rows beyond `rows` read
 // as zero
-CUtensorMap make_i8_map(void *base, int64_t rows, int64_t Kp, int64_t plane_stride, int planes, int box_rows = 128) {
+CUtensorMap make_i8_map(void *base, int64_t rows, int64_t Kp, int64_t plane_stride, int planes, int box_rows = 128,
+                        int64_t row_stride = 0) {
     CUtensorMap m;
+    if (row_stride == 0) row_stride = Kp;
     REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, CCSD_GPU_EINVAL, "tensor map base must be 16-byte aligned");
-    REQUIRE(Kp % 64 == 0 && plane_stride % 16 == 0, CCSD_GPU_EINVAL, "int8 digit planes: bad padding");
+    REQUIRE(Kp % 64 == 0 && row_stride % 16 == 0 && plane_stride % 16 == 0 && row_stride >= Kp, CCSD_GPU_EINVAL,
+            "int8 digit planes: bad padding");
     cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)planes};
-    cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)plane_stride};
+    cuuint64_t strides[2] = {(cuuint64_t)row_stride, (cuuint64_t)plane_stride};
     cuuint32_t box[3] = {OBK, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
@@ -721,9 +724,38 @@ void slab_digits(Exec &ex, const double *src, int64_t sr, int64_t sk, int64_t R,
 
 }  // namespace
 
+void ozaki_prepare(Exec &ex, bool trans, int64_t rows, int64_t k, const double *X, int64_t ldx, int digits,
+                   OzPlanes &out) {
+    REQUIRE(rows > 0 && k > 0 && rows < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "ozaki_prepare: bad size");
+    REQUIRE(digits >= 2 && digits <= SLOTS, CCSD_GPU_EINVAL, "ozaki_prepare: 2 to 7 digits");
+    // rows of op(X): X[r + ldx kk] (N) or X[kk + ldx r] (T), padded to 128 (either operand's tiles)
+    const int64_t sr = trans ? ldx : 1, sk = trans ? 1 : ldx;
+    const int64_t Rp = round_up(rows, (int64_t)OBM), Kp = round_up(k, (int64_t)OBK);
+    const size_t exp_bytes = round_up(sizeof(int) * (size_t)Rp, (size_t)256);
+    const size_t need = exp_bytes + (size_t)digits * Rp * Kp;
+    if (out.buf.bytes() < need) {
+        out.buf.release();
+        out.buf.alloc(need, ex.stream);
+    }
+    out.rows = rows;
+    out.k = k;
+    out.Rp = Rp;
+    out.Kp = Kp;
+    out.digits = digits;
+    out.exp_bytes = exp_bytes;
+    int *e = out.buf.as<int>();
+    row_exponents(ex, X, sr, sk, rows, k, Rp, e);
+    slab_digits(ex, X, sr, sk, rows, k, Rp, Kp, digits, e, reinterpret_cast<int8_t *>(out.buf.as<uint8_t>() + exp_bytes));
+}
+
 void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double alpha, const double *A,
-                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, int digits) {
+                int64_t lda, const double *B, int64_t ldb, double beta, double *C, int64_t ldc, int digits,
+                const OzPlanes *pa, const OzPlanes *pb) {
     REQUIRE(m > 0 && n > 0 && k > 0, CCSD_GPU_EINVAL, "ozaki_gemm: empty product");
+    REQUIRE(!pa || (pa->digits == digits && pa->rows == m && pa->k == k), CCSD_GPU_EINVAL,
+            "ozaki_gemm: prepared A does not match");
+    REQUIRE(!pb || (pb->digits == digits && pb->rows == n && pb->k == k), CCSD_GPU_EINVAL,
+            "ozaki_gemm: prepared B does not match");
     REQUIRE(m < (1ll << 31) && n < (1ll << 31) && k < (1ll << 31), CCSD_GPU_EINVAL, "ozaki_gemm: size too large");
     REQUIRE(digits >= 2 && digits <= SLOTS, CCSD_GPU_EINVAL, "ozaki_gemm: 2 to 7 digits");
     REQUIRE(ex.gemm_err != nullptr, CCSD_GPU_EINVAL, "ozaki_gemm: no error word");
@@ -736,12 +768,13 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     // the digit planes of K slabs of whole 16384-wide chunks, at most ~4 GB of them at a time (a
     // 21 GB operand would otherwise need 18 GB of planes at once); each slab's launch adds its chunks
     // to C in the order one launch over all K would, so the result does not depend on the slabs
-    const int64_t per_chunk = (int64_t)digits * (Mp + Np) * OK_CHUNK;
+    const int64_t per_chunk = (int64_t)digits * std::max<int64_t>(OBM, (pa ? 0 : Mp) + (pb ? 0 : Np)) * OK_CHUNK;
     int64_t budget = 4ll << 30;
     if (const char *mb = std::getenv("CCSD_GPU_DIGIT_SLAB_MB")) budget = std::max<int64_t>(1, std::atoll(mb)) << 20;
     const int64_t chunks_per_slab = std::max<int64_t>(1, budget / per_chunk);
     const int64_t kslab = std::min<int64_t>(round_up(k, OBK), chunks_per_slab * OK_CHUNK);
-    const size_t a_bytes = round_up((size_t)digits * Mp * kslab, 1024), b_bytes = (size_t)digits * Np * kslab;
+    const size_t a_bytes = pa ? 0 : round_up((size_t)digits * Mp * kslab, (size_t)1024);
+    const size_t b_bytes = pb ? 0 : (size_t)digits * Np * kslab;
     const size_t need = exp_bytes + a_bytes + b_bytes;
     DBuf local;
     DBuf *arena = ex.digit_arena ? ex.digit_arena : &local;
@@ -752,8 +785,11 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     uint8_t *base = arena->as<uint8_t>();
     int *ea = reinterpret_cast<int *>(base), *eb = ea + Mp;
     int8_t *da = reinterpret_cast<int8_t *>(base + exp_bytes), *db = da + a_bytes;
-    row_exponents(ex, A, a_sr, a_sk, m, k, Mp, ea);
-    row_exponents(ex, B, b_sr, b_sk, n, k, Np, eb);
+    // a prepared operand brings its exponents and the digit planes of all of K (no conversion here)
+    if (pa) ea = pa->buf.as<int>();
+    else row_exponents(ex, A, a_sr, a_sk, m, k, Mp, ea);
+    if (pb) eb = pb->buf.as<int>();
+    else row_exponents(ex, B, b_sr, b_sk, n, k, Np, eb);
     auto kernel = digits == 7 ? ozaki_gemm_kernel<7> : digits == 6 ? ozaki_gemm_kernel<6>
                 : digits == 5 ? ozaki_gemm_kernel<5> : digits == 4 ? ozaki_gemm_kernel<4>
                 : digits == 3 ? ozaki_gemm_kernel<3> : ozaki_gemm_kernel<2>;
@@ -801,10 +837,15 @@ void ozaki_gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_
     }
     for (int64_t k0 = 0; k0 < k; k0 += kslab) {
         const int64_t kk = std::min(kslab, k - k0), Kp = round_up(kk, OBK);
-        slab_digits(ex, A + k0 * a_sk, a_sr, a_sk, m, kk, Mp, Kp, digits, ea, da);
-        slab_digits(ex, B + k0 * b_sk, b_sr, b_sk, n, kk, Np, Kp, digits, eb, db);
-        CUtensorMap ta = make_i8_map(da, Mp, Kp, Mp * Kp, digits);
-        CUtensorMap tb = make_i8_map(db, Np, Kp, Np * Kp, digits, pair ? OBN / 2 : OBN);
+        if (!pa) slab_digits(ex, A + k0 * a_sk, a_sr, a_sk, m, kk, Mp, Kp, digits, ea, da);
+        if (!pb) slab_digits(ex, B + k0 * b_sk, b_sr, b_sk, n, kk, Np, Kp, digits, eb, db);
+        // prepared planes: the slab starts k0 bytes into each row of the whole-K planes (k0 is a
+        // multiple of 16384, so the tensor map base stays 16-byte aligned)
+        CUtensorMap ta = pa ? make_i8_map(pa->digits_base() + k0, Mp, Kp, pa->Rp * pa->Kp, digits, OBM, pa->Kp)
+                            : make_i8_map(da, Mp, Kp, Mp * Kp, digits);
+        CUtensorMap tb = pb ? make_i8_map(pb->digits_base() + k0, Np, Kp, pb->Rp * pb->Kp, digits,
+                                          pair ? OBN / 2 : OBN, pb->Kp)
+                            : make_i8_map(db, Np, Kp, Np * Kp, digits, pair ? OBN / 2 : OBN);
         OzMap map{};
         map.bm = pair ? 2 * OBM : OBM;
         map.num_mt = (int)(pair ? round_up(Mp, (int64_t)(2 * OBM)) / (2 * OBM) : Mp / OBM);
