@@ -400,7 +400,7 @@ def run_gpu(args):
             result["workloads"][name]["wall_s"] = round(time.perf_counter() - t0, 1)
     if rank == 0:
         if args.cpu_baseline and world == 1:
-            result["cpu_baseline"] = cpu_sample(args)
+            result["cpu_baseline"] = cpu_sample_isolated(args)
         print(json.dumps(result), flush=True)
 
 
@@ -771,14 +771,45 @@ def cpu_sample(args, iterations=None):
                       f"cores) at the benchmark's own shape o={n_o} v={n_v} N_J={n_J}"}
 
 
+def cpu_sample_isolated(args, iterations=None, timeout_s=900):
+    """cpu_sample in a child process of its own: one OpenMP/OpenBLAS pool sized to the CPUs this
+    process may run on (no CUDA runtime, torch threads or GPU-side work beside it), threads that
+    sleep instead of spinning when idle, and a bound on the wall time.  A sample that runs out of
+    time is reported as such instead of holding the benchmark."""
+    try:
+        ncpu = len(os.sched_getaffinity(0))
+    except AttributeError:
+        ncpu = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(ncpu), OPENBLAS_NUM_THREADS=str(ncpu), OMP_WAIT_POLICY="PASSIVE")
+    spec = {"n_o": args.n_o, "n_v": args.n_v, "n_J": args.n_J, "cpu_iterations": args.cpu_iterations,
+            "iterations": iterations}
+    code = ("import json, sys, types; sys.path.insert(0, '.'); import bench; "
+            "a = json.loads(sys.argv[1]); it = a.pop('iterations'); "
+            "print(json.dumps(bench.cpu_sample(types.SimpleNamespace(**a), it)))")
+    root = os.path.dirname(os.path.abspath(__file__))
+    try:
+        r = subprocess.run([sys.executable, "-c", code, json.dumps(spec)], env=env, cwd=root, capture_output=True,
+                           text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        cores, model = host_cpu()
+        return {"value": None, "unit": "s/iter", "cores": cores, "kind": "port", "cpu_model": model,
+                "iterations_timed": 0, "sample": f"timed out after {timeout_s} s (one iteration of the CPU "
+                                                   f"restatement at o={args.n_o} v={args.n_v} N_J={args.n_J})"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        raise RuntimeError("CPU baseline failed: " + r.stderr[-2000:])
+    return json.loads(lines[-1])
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cb = cpu_sample(args)
+    cb = cpu_sample_isolated(args)
     line = {"metric": METRIC, "value": cb["value"], "unit": "s/iter", "n_gpus": 0,
             "steps": cb["iterations_timed"], "warmup": 0, "requested_steps": args.steps,
-            "requested_warmup": args.warmup, "ms_per_step": round(cb["value"] * 1e3, 1),
+            "requested_warmup": args.warmup,
+            "ms_per_step": round(cb["value"] * 1e3, 1) if cb["value"] is not None else None,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": f"CCSD ground-state iteration, synthetic Cholesky system o={args.n_o} "
