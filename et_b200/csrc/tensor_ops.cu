@@ -222,6 +222,14 @@ struct Route {
     std::string key;
 };
 
+// fixed rule: the tensor-core tile is 128 x 256 x 64, so skinny products stay on the FP64 pipe
+Route fixed_route(const Exec &ex, int64_t m, int64_t n, int64_t k, double fl, bool allow_mixed) {
+    Route r;
+    const bool tc_ok = allow_mixed && ex.prec == Prec::MIXED && k >= 16;
+    r.mixed = tc_ok && fl >= ex.mixed_min_flops && (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64));
+    return r;
+}
+
 Route lookup_route(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, double fl, bool allow_mixed) {
     Route r;
     const bool tc_ok = allow_mixed && ex.prec == Prec::MIXED && k >= 16;
@@ -242,9 +250,7 @@ Route lookup_route(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int
         r.splits = route;
         return r;
     }
-    // fixed rule: the tensor-core tile is 128 x 256 x 64, so skinny products stay on the FP64 pipe
-    r.mixed = tc_ok && fl >= ex.mixed_min_flops && (ex.mixed_min_flops <= 1 || (m >= 64 && n >= 64 && k >= 64));
-    return r;
+    return fixed_route(ex, m, n, k, fl, allow_mixed);
 }
 
 }  // namespace
@@ -270,9 +276,14 @@ void gemm(Exec &ex, bool transA, bool transB, int64_t m, int64_t n, int64_t k, d
                 mixed_gemm(ex, transA, transB, m, n, k, alpha, A, lda, B, ldb, 0.0, scratch.d(), m, r);
             }
         });
-        rt.known = true;
-        rt.mixed = route > 0;
-        rt.splits = route;
+        if (route < 0) {
+            // not timed now (another thread is timing, or the stream is being captured): the fixed rule
+            rt = fixed_route(ex, m, n, k, fl, allow_mixed);
+        } else {
+            rt.known = true;
+            rt.mixed = route > 0;
+            rt.splits = route;
+        }
     }
     const bool mixed = rt.mixed;
     const int route = rt.splits;
