@@ -730,8 +730,10 @@ void Context::ladder_t1_corrections(const double *t1, const double *tf, const do
                  tv(Q.d(), {no, no, no, no}));
         contract(ex, "ak,kilj->ailj", 1.0, tv(t1, {nv, no}), tv(Q.d(), {no, no, no, no}), 0.0,
                  tv(B.d(), {nv, no, no, no}));
-        // the symmetric term enters at half weight: pack(A + A^T) adds it twice
-        contract(ex, "bl,ailj->aibj", 0.5, tv(t1, {nv, no}), tv(B.d(), {nv, no, no, no}), 1.0,
+        // the symmetric term sum_l t_bl B_ailj enters at half weight (pack(A + A^T) adds it twice), in
+        // its mirrored form sum_l t_al B_bjli, whose output index order (a | i, b, j) lies in A's own
+        // layout, so the product writes A in place instead of through a reordered copy
+        contract(ex, "al,bjli->aibj", 0.5, tv(t1, {nv, no}), tv(B.d(), {nv, no, no, no}), 1.0,
                  tv(A.d(), {nv, no, nv, no}));
     }
     pack_sym_add(ex, A.d(), om2, nov);
