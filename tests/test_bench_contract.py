@@ -56,3 +56,14 @@ def test_synthetic_cholesky_vectors_in_et_layout():
     assert np.abs(a.L_mo - a.L_mo.transpose(0, 2, 1)).max() == 0.0
     flat = a.L_mo.reshape(-1, order="F")
     assert np.shares_memory(flat, a.L_mo)
+
+
+def test_cpu_baseline_is_bounded():
+    """The CPU restatement runs in a child process with a wall-time bound: a sample that runs out of
+    time is reported (no value, the reason in `sample`) instead of holding the benchmark."""
+    import types
+    bench = _bench()
+    args = types.SimpleNamespace(n_o=32, n_v=320, n_J=1200, cpu_iterations=1)
+    cb = bench.cpu_sample_isolated(args, timeout_s=1)
+    assert cb["value"] is None and cb["iterations_timed"] == 0 and "timed out" in cb["sample"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1
