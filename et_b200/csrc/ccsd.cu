@@ -955,7 +955,7 @@ int Context::solve_gs(const ccsd_gpu_solver_options *o, double *energy_out, int3
     int last_check = 0;
     std::vector<double> norms;
     // CCSD_GPU_TRACE=1: one line per iteration on stderr with the refinement decisions
-    const bool trace = std::getenv("CCSD_GPU_TRACE") && std::getenv("CCSD_GPU_TRACE")[0] == '1';
+    const bool trace = std::getenv("CCSD_GPU_TRACE") && std::atoi(std::getenv("CCSD_GPU_TRACE")) >= 1;
     auto trace_ms = [&]() {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - trace_t0).count();
     };
